@@ -1,0 +1,269 @@
+"""a2afft_b200: B200-native drop-in for the a2afft pencil-decomposed 3D FFT of
+humz2k/3D-FFTs-MPI.
+
+Host-side mirror of the reference's two classes over the C ABI of
+``liba2afft_b200.so`` (``include/a2afft_b200.h``):
+
+* ``a2aDistribution`` -- ``src/a2afft/distribution/a2adistribution.h:5-41``:
+  brick decomposition of an ``Ng^3`` grid over ``world_size`` ranks and the six
+  pencil transpose steps.  The ranks are virtual: one device buffer holds every
+  rank's brick, rank-major, each brick in the reference's ``[x][y][z]``
+  layout.
+* ``a2adfft`` -- ``src/a2afft/dfft/a2adfft.h:9-30``: ``make_plans`` /
+  ``forward`` / ``inverse`` in place on such a buffer.
+
+plus the 1D helpers of ``src/a2afft/dfft/kernels/kernels.h:5-11``
+(``forward_1d_fft``, ``inverse_1d_fft``, ``scale_fft``, ``fast_copy_fft``).
+
+Buffers are CUDA tensors (``complex128`` for ``precision="c128"``, the
+reference's ``fftPrecision double``; ``complex64`` for ``"c64"``) with
+``world_size * nlocal`` elements, or raw device pointers (``int``).  Every call
+goes to the CUDA library; errors raise ``A2AError`` with the library's status
+and message.
+"""
+from __future__ import annotations
+
+import ctypes
+
+from ._lib import (  # noqa: F401
+    A2AError,
+    C64,
+    C128,
+    Desc,
+    LIB_PATH,
+    METHOD_PLAIN,
+    METHOD_SPLIT_BF16,
+    METHOD_SPLIT_FP16,
+    bufptr,
+    call,
+    lib,
+)
+
+__all__ = [
+    "A2AError",
+    "a2aDistribution",
+    "a2adfft",
+    "forward_1d_fft",
+    "inverse_1d_fft",
+    "scale_fft",
+    "fast_copy_fft",
+    "version",
+]
+
+_PREC = {"c128": C128, "complex128": C128, "double": C128, "c64": C64, "complex64": C64, "float": C64}
+_METHODS = {"plain": METHOD_PLAIN, "split_bf16": METHOD_SPLIT_BF16, "split_fp16": METHOD_SPLIT_FP16}
+
+
+def version() -> int:
+    return lib().a2a_version()
+
+
+def _torch_dtype(prec: int):
+    import torch
+
+    return torch.complex128 if prec == C128 else torch.complex64
+
+
+class a2aDistribution:
+    """``a2aDistribution(MPI_Comm, int Ng, int blockSize)``
+    (``a2adistribution.cpp:85-154``) over ``world_size`` virtual ranks.
+
+    ``Ng`` may be a 3-tuple ``(nx, ny, nz)`` for a box (an extension the
+    reference does not have; only ``a2adfft`` accepts boxes)."""
+
+    def __init__(self, world_size: int, Ng, blockSize: int = 64, precision: str = "c128"):
+        if precision not in _PREC:
+            raise ValueError(f"precision must be one of {sorted(_PREC)}")
+        self.precision = _PREC[precision]
+        h = ctypes.c_void_p()
+        if isinstance(Ng, (tuple, list)):
+            nx, ny, nz = (int(v) for v in Ng)
+            call("a2a_distribution_create_box", nx, ny, nz, int(world_size), int(blockSize), self.precision,
+                 ctypes.byref(h))
+        else:
+            call("a2a_distribution_create", int(Ng), int(world_size), int(blockSize), self.precision, ctypes.byref(h))
+        self._h = h
+        d = Desc()
+        call("a2a_distribution_describe", self._h, ctypes.byref(d))
+        self.ndims = d.ndims
+        self.ng = tuple(d.ng)
+        self.Ng = self.ng[0]
+        self.world_size = d.world_size
+        self.dims = list(d.dims)
+        self.local_grid_size = list(d.local_grid_size)
+        self.nlocal = int(d.nlocal)
+        self.nsends = int(d.nsends)
+        self.blockSize = d.block_size
+        self.element_bytes = int(d.element_bytes)
+        self.buffer_bytes = int(d.buffer_bytes)
+        self._stream = None
+
+    # -- reference public fields per rank (a2adistribution.h:8-17) ----------
+    def coords(self, rank: int) -> list[int]:
+        c, s = (ctypes.c_int * 3)(), (ctypes.c_int * 3)()
+        call("a2a_rank_coords", self._h, int(rank), c, s)
+        return list(c)
+
+    def local_coordinates_start(self, rank: int) -> list[int]:
+        c, s = (ctypes.c_int * 3)(), (ctypes.c_int * 3)()
+        call("a2a_rank_coords", self._h, int(rank), c, s)
+        return list(s)
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def dtype(self):
+        return _torch_dtype(self.precision)
+
+    def empty(self, device="cuda"):
+        """A device buffer of ``world_size * nlocal`` elements."""
+        import torch
+
+        return torch.empty(self.world_size * self.nlocal, dtype=self.dtype, device=device)
+
+    def set_stream(self, stream) -> None:
+        """CUDA stream for the calls that take none (a ``torch.cuda.Stream``,
+        a raw handle or ``None`` for the default stream)."""
+        self._stream = stream
+        handle = getattr(stream, "cuda_stream", stream)
+        call("a2a_distribution_set_stream", self._h, ctypes.c_void_p(handle or 0))
+
+    def _buf(self, t):
+        if isinstance(t, int):
+            return bufptr(t)
+        if not t.is_cuda:
+            raise ValueError("buffers must be CUDA tensors (or raw device pointers)")
+        if t.dtype != self.dtype:
+            raise TypeError(f"buffer dtype {t.dtype} does not match the distribution's {self.dtype}")
+        if not t.is_contiguous() or t.numel() != self.world_size * self.nlocal:
+            raise ValueError(f"buffer must be contiguous with world_size*nlocal = {self.world_size * self.nlocal} "
+                             "elements")
+        return bufptr(t.data_ptr())
+
+    # -- the six steps (a2adistribution.cpp:156-256) -------------------------
+    def getZPencils(self, d_Buff1, d_Buff2):
+        call("a2a_get_z_pencils", self._h, self._buf(d_Buff1), self._buf(d_Buff2))
+
+    def returnZPencils(self, d_Buff1, d_Buff2):
+        call("a2a_return_z_pencils", self._h, self._buf(d_Buff1), self._buf(d_Buff2))
+
+    def getXPencils(self, d_Buff1, d_Buff2):
+        call("a2a_get_x_pencils", self._h, self._buf(d_Buff1), self._buf(d_Buff2))
+
+    def returnXPencils(self, d_Buff1, d_Buff2):
+        call("a2a_return_x_pencils", self._h, self._buf(d_Buff1), self._buf(d_Buff2))
+
+    def getYPencils(self, d_Buff1, d_Buff2):
+        call("a2a_get_y_pencils", self._h, self._buf(d_Buff1), self._buf(d_Buff2))
+
+    def returnYPencils(self, d_Buff1, d_Buff2):
+        call("a2a_return_y_pencils", self._h, self._buf(d_Buff1), self._buf(d_Buff2))
+
+    def finalize(self) -> None:
+        """``a2aDistribution::finalize`` (``a2adistribution.cpp:258-265``)."""
+        if self._h:
+            call("a2a_distribution_finalize", self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.finalize()
+        except Exception:
+            pass
+
+
+# -- dfft/kernels/kernels.h:5-11 --------------------------------------------
+
+
+def forward_1d_fft(dist: a2aDistribution, data) -> None:
+    """Forward 1D transform of every contiguous length-Ng line
+    (``a2affts.cu:7-40``)."""
+    call("a2a_forward_1d_fft", dist.handle, dist._buf(data))
+
+
+def inverse_1d_fft(dist: a2aDistribution, data) -> None:
+    """Inverse, unnormalised (``a2affts.cu:42-76``)."""
+    call("a2a_inverse_1d_fft", dist.handle, dist._buf(data))
+
+
+def scale_fft(dist: a2aDistribution, out, data) -> None:
+    """``out = data / Ng^3`` (``a2affts.cu:78-92``)."""
+    call("a2a_scale_fft", dist.handle, dist._buf(out), dist._buf(data))
+
+
+def fast_copy_fft(dist: a2aDistribution, out, data) -> None:
+    """``out = data`` (``a2affts.cu:94-106``)."""
+    call("a2a_fast_copy_fft", dist.handle, dist._buf(out), dist._buf(data))
+
+
+class a2adfft:
+    """``a2adfft(a2aDistribution&)`` (``dfft/a2adfft.cpp:7-16``)."""
+
+    def __init__(self, dist: a2aDistribution, method: str = "plain"):
+        self.distribution = dist
+        self.Ng = dist.Ng
+        self.nlocal = dist.nlocal
+        self.world_size = dist.world_size
+        self.blockSize = dist.blockSize
+        h = ctypes.c_void_p()
+        call("a2a_dfft_create", dist.handle, ctypes.byref(h))
+        self._h = h
+        self.plans_made = 0
+        self.d_scratch = None
+        if method != "plain":
+            self.set_method(method)
+
+    def set_method(self, method: str) -> None:
+        call("a2a_dfft_set_method", self._h, _METHODS[method])
+        self.plans_made = 0
+
+    def make_plans(self, d_scratch=None) -> None:
+        """``a2adfft::make_plans`` (``a2adfft.cpp:18-24``); the scratch buffer
+        is optional because the fused transform runs in place."""
+        self.d_scratch = d_scratch
+        call("a2a_dfft_make_plans", self._h, None if d_scratch is None else self.distribution._buf(d_scratch))
+        self.plans_made = 1
+
+    def forward(self, d_data, stream=None) -> None:
+        """``a2adfft::forward`` (``a2adfft.cpp:26-91``).  Synchronous unless a
+        stream is given."""
+        if stream is None:
+            call("a2a_dfft_forward", self._h, self.distribution._buf(d_data))
+        else:
+            handle = getattr(stream, "cuda_stream", stream)
+            call("a2a_dfft_forward_async", self._h, self.distribution._buf(d_data), ctypes.c_void_p(handle))
+
+    def inverse(self, d_data, stream=None) -> None:
+        """``a2adfft::inverse`` (``a2adfft.cpp:93-158``), scaled by 1/Ng^3."""
+        if stream is None:
+            call("a2a_dfft_inverse", self._h, self.distribution._buf(d_data))
+        else:
+            handle = getattr(stream, "cuda_stream", stream)
+            call("a2a_dfft_inverse_async", self._h, self.distribution._buf(d_data), ctypes.c_void_p(handle))
+
+    backward = inverse
+
+    def execute_pass(self, d_data, pass_index: int, inverse: bool, stream) -> None:
+        """Enqueue one of the three fused passes (0 = Z, 1 = X, 2 = Y)."""
+        handle = getattr(stream, "cuda_stream", stream)
+        call("a2a_dfft_execute_pass_async", self._h, self.distribution._buf(d_data), int(pass_index), int(inverse),
+             ctypes.c_void_p(handle))
+
+    @property
+    def launches_per_transform(self) -> int:
+        n = ctypes.c_int()
+        call("a2a_dfft_launches_per_transform", self._h, ctypes.byref(n))
+        return n.value
+
+    def destroy(self) -> None:
+        if self._h:
+            call("a2a_dfft_destroy", self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass

@@ -1,0 +1,563 @@
+// C ABI of liba2afft_b200: a2aDistribution / a2adfft over virtual ranks.
+//
+// Reference interfaces replaced (paths inside humz2k/3D-FFTs-MPI):
+//   src/a2afft/distribution/a2adistribution.{h,cpp}  -> a2a_distribution_*, a2a_get/return_*_pencils
+//   src/a2afft/dfft/a2adfft.{h,cpp}                  -> a2a_dfft_*
+//   src/a2afft/dfft/kernels/a2affts.cu               -> a2a_forward/inverse_1d_fft, a2a_scale_fft, a2a_fast_copy_fft
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+using a2a::Dist;
+using a2a::PassKernel;
+
+struct a2a_distribution {
+    Dist d;
+};
+
+struct a2a_dfft {
+    a2a_distribution* dist = nullptr;
+    void* scratch = nullptr;
+    bool plans_made = false;
+    a2a_method method = A2A_METHOD_PLAIN;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+a2a_status fail(a2a_status s, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return s;
+}
+
+a2a_status cuda_fail(cudaError_t e, const char* what) {
+    return fail(A2A_ERROR_CUDA, "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
+}
+
+#define A2A_CUDA(call, what)                              \
+    do {                                                  \
+        cudaError_t e_ = (call);                          \
+        if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+    } while (0)
+
+// MPI_Dims_create(n, 3) for all-zero input dims: prime factors, largest
+// first, each to the dimension with the smallest running product, then sorted
+// non-increasing (the balanced factorisation the MPI standard asks for).
+void dims_create(int n, int dims[3]) {
+    std::vector<int> f;
+    int m = n;
+    for (int p = 2; (long)p * p <= m; ++p)
+        while (m % p == 0) {
+            f.push_back(p);
+            m /= p;
+        }
+    if (m > 1) f.push_back(m);
+    std::sort(f.rbegin(), f.rend());
+    int d[3] = {1, 1, 1};
+    for (int p : f) {
+        int i = 0;
+        for (int k = 1; k < 3; ++k)
+            if (d[k] < d[i]) i = k;
+        d[i] *= p;
+    }
+    std::sort(d, d + 3, [](int a, int b) { return a > b; });
+    for (int k = 0; k < 3; ++k) dims[k] = d[k];
+}
+
+bool find_kernel(a2a_precision prec, int n, int mode, bool inv, PassKernel* k) {
+    return prec == A2A_C128 ? a2a::find_pass_kernel_f64(n, mode, inv, k)
+                            : a2a::find_pass_kernel_f32(n, mode, inv, k);
+}
+
+// Stage twiddles W_{Ns R}^{r m} (forward sign), laid out as RadixPlan::twoff,
+// generated in long double with the exponent reduced exactly.
+void gen_twiddles(const PassKernel& k, std::vector<long double>& re, std::vector<long double>& im) {
+    const long double pi = acosl(-1.0L);
+    re.clear();
+    im.clear();
+    int ns = k.radix[0];
+    for (int s = 1; s < k.nstages; ++s) {
+        const int R = k.radix[s];
+        const long long M = (long long)ns * R;
+        for (int r = 1; r < R; ++r)
+            for (int m = 0; m < ns; ++m) {
+                const long long e = ((long long)r * m) % M;
+                const long double ang = 2.0L * pi * (long double)e / (long double)M;
+                re.push_back(cosl(ang));
+                im.push_back(-sinl(ang));
+            }
+        ns *= R;
+    }
+}
+
+a2a_status check_buf(void** p, const char* name) {
+    if (!p || !p[0]) return fail(A2A_ERROR_INVALID_VALUE, "%s is NULL", name);
+    if (reinterpret_cast<uintptr_t>(p[0]) % 16)
+        return fail(A2A_ERROR_MISALIGNED, "%s[0] is not 16-byte aligned", name);
+    return A2A_SUCCESS;
+}
+
+a2a_status finish(const Dist& d, cudaStream_t st, bool sync) {
+    A2A_CUDA(cudaGetLastError(), "kernel launch");
+    if (sync) A2A_CUDA(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+    return A2A_SUCCESS;
+}
+
+template <typename T>
+cudaError_t launch_pass_t(const PassKernel& k, const void* src, void* dst, const uint32_t* offA, const uint32_t* offU,
+                          const uint32_t* offV, const void* tw, int NU, int NV, double scale, cudaStream_t st) {
+    a2a::PassArgs<T> a;
+    a.src = static_cast<const a2a::cx<T>*>(src);
+    a.dst = static_cast<a2a::cx<T>*>(dst);
+    a.offA = offA;
+    a.offU = offU;
+    a.offV = offV;
+    a.tw = static_cast<const a2a::cx<T>*>(tw);
+    a.NU = NU;
+    a.NV = NV;
+    a.scale = T(scale);
+    void* args[] = {&a};
+    const unsigned grid = unsigned((uint64_t)NU * (NV / k.lines));
+    return cudaLaunchKernel(k.fn, dim3(grid), dim3(k.threads), args, k.smem, st);
+}
+
+cudaError_t launch_pass(const Dist& d, const PassKernel& k, const void* src, void* dst, const uint32_t* offA,
+                        const uint32_t* offU, const uint32_t* offV, const void* tw, int NU, int NV, double scale,
+                        cudaStream_t st) {
+    if (d.prec == A2A_C128) return launch_pass_t<double>(k, src, dst, offA, offU, offV, tw, NU, NV, scale, st);
+    return launch_pass_t<float>(k, src, dst, offA, offU, offV, tw, NU, NV, scale, st);
+}
+
+a2a_status setup_distribution(Dist& d, int nx, int ny, int nz, int P, int block_size, a2a_precision prec) {
+    if (nx < 1 || ny < 1 || nz < 1 || P < 1)
+        return fail(A2A_ERROR_INVALID_VALUE, "grid sizes and world_size must be >= 1");
+    if (block_size < 1 || block_size > 1024) return fail(A2A_ERROR_INVALID_VALUE, "block_size must be in [1, 1024]");
+    if (prec != A2A_C128 && prec != A2A_C64) return fail(A2A_ERROR_INVALID_VALUE, "unknown precision %d", (int)prec);
+    d.ng[0] = nx;
+    d.ng[1] = ny;
+    d.ng[2] = nz;
+    d.P = P;
+    d.block_size = block_size;
+    d.prec = prec;
+    d.elem_bytes = prec == A2A_C128 ? 16 : 8;
+    d.cube = (nx == ny && ny == nz);
+    dims_create(P, d.dims);
+    for (int a = 0; a < 3; ++a)  // a2adistribution.cpp:102-104
+        if (d.ng[a] % d.dims[a])
+            return fail(A2A_ERROR_DECOMPOSITION, "N[%d]=%d is not divisible by dims[%d]=%d", a, d.ng[a], a, d.dims[a]);
+    for (int a = 0; a < 3; ++a) d.local[a] = d.ng[a] / d.dims[a];
+    for (int a = 0; a < 3; ++a)  // :115-117
+        if (P % d.dims[a])
+            return fail(A2A_ERROR_DECOMPOSITION, "world_size=%d is not divisible by dims[%d]=%d", P, a, d.dims[a]);
+    const long long lx = d.local[0], ly = d.local[1], lz = d.local[2];
+    if ((lx * ly) % P || (lx * lz) % P || (ly * lz) % P)  // :119-121
+        return fail(A2A_ERROR_DECOMPOSITION, "a face of the %lldx%lldx%lld brick is not divisible by world_size=%d",
+                    lx, ly, lz, P);
+    d.nlocal = (uint64_t)lx * ly * lz;
+    d.chunk = d.nlocal / P;
+    const uint64_t total = d.nlocal * (uint64_t)P;
+    if (total >= (uint64_t(1) << 32))
+        return fail(A2A_ERROR_UNSUPPORTED, "grids of 2^32 or more elements are not supported");
+
+    A2A_CUDA(cudaGetDevice(&d.device), "cudaGetDevice");
+    A2A_CUDA(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, d.device), "cudaDeviceGetAttribute");
+
+    // kernels and twiddles per axis
+    for (int a = 0; a < 3; ++a)
+        for (int inv = 0; inv < 2; ++inv) {
+            if (!find_kernel(prec, d.ng[a], a2a::MODE_LINE, inv, &d.kline[a][inv]) ||
+                !find_kernel(prec, d.ng[a], a2a::MODE_BATCH, inv, &d.kbatch[a][inv]))
+                return fail(A2A_ERROR_UNSUPPORTED,
+                            "no compiled transform of length %d (supported: 4 8 12 16 24 32 48 64 96 128 192 256 "
+                            "384 512 768 1024)",
+                            d.ng[a]);
+            for (const PassKernel* k : {&d.kline[a][inv], &d.kbatch[a][inv]})
+                A2A_CUDA(cudaFuncSetAttribute(k->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k->smem),
+                         "cudaFuncSetAttribute");
+        }
+
+    // offset tables: brick offsets per axis (global (x,y,z) lives at
+    // off[0][x] + off[1][y] + off[2][z]), identity, pencil-buffer line bases
+    const int maxn = std::max(nx, std::max(ny, nz));
+    std::vector<uint32_t> h;
+    size_t pos[6];
+    const uint64_t nl = d.nlocal;
+    const uint64_t d1 = d.dims[1], d2 = d.dims[2];
+    pos[0] = h.size();
+    for (int x = 0; x < nx; ++x) h.push_back(uint32_t((x / lx) * d1 * d2 * nl + (x % lx) * ly * lz));
+    pos[1] = h.size();
+    for (int y = 0; y < ny; ++y) h.push_back(uint32_t((y / ly) * d2 * nl + (y % ly) * lz));
+    pos[2] = h.size();
+    for (int z = 0; z < nz; ++z) h.push_back(uint32_t((z / lz) * nl + (z % lz)));
+    pos[3] = h.size();
+    for (int i = 0; i < maxn; ++i) h.push_back(uint32_t(i));
+    pos[4] = h.size();
+    for (int u = 0; u < nx; ++u) h.push_back(uint32_t((uint64_t)u * nx * nx));
+    pos[5] = h.size();
+    for (int v = 0; v < nx; ++v) h.push_back(uint32_t((uint64_t)v * nx));
+    A2A_CUDA(cudaMalloc(&d.d_tables, h.size() * sizeof(uint32_t)), "cudaMalloc(tables)");
+    A2A_CUDA(cudaMemcpy(d.d_tables, h.data(), h.size() * sizeof(uint32_t), cudaMemcpyHostToDevice), "cudaMemcpy");
+    for (int a = 0; a < 3; ++a) d.off[a] = d.d_tables + pos[a];
+    d.iota = d.d_tables + pos[3];
+    d.pen_u = d.d_tables + pos[4];
+    d.pen_v = d.d_tables + pos[5];
+
+    std::vector<long double> re, im;
+    size_t twpos[3], twtotal = 0;
+    for (int a = 0; a < 3; ++a) {
+        twpos[a] = twtotal;
+        twtotal += (size_t)d.kline[a][0].twtotal;
+    }
+    if (twtotal == 0) twtotal = 1;
+    A2A_CUDA(cudaMalloc(&d.d_tw, twtotal * d.elem_bytes), "cudaMalloc(twiddles)");
+    std::vector<double> hd;
+    std::vector<float> hf;
+    for (int a = 0; a < 3; ++a) {
+        gen_twiddles(d.kline[a][0], re, im);
+        for (size_t i = 0; i < re.size(); ++i) {
+            hd.push_back((double)re[i]);
+            hd.push_back((double)im[i]);
+            hf.push_back((float)re[i]);
+            hf.push_back((float)im[i]);
+        }
+    }
+    if (!hd.empty()) {
+        if (prec == A2A_C128)
+            A2A_CUDA(cudaMemcpy(d.d_tw, hd.data(), hd.size() * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy");
+        else
+            A2A_CUDA(cudaMemcpy(d.d_tw, hf.data(), hf.size() * sizeof(float), cudaMemcpyHostToDevice), "cudaMemcpy");
+    }
+    for (int a = 0; a < 3; ++a) d.tw[a] = static_cast<const char*>(d.d_tw) + twpos[a] * d.elem_bytes;
+    return A2A_SUCCESS;
+}
+
+void release(Dist& d) {
+    if (d.d_tables) cudaFree(d.d_tables);
+    if (d.d_tw) cudaFree(d.d_tw);
+    d.d_tables = nullptr;
+    d.d_tw = nullptr;
+}
+
+a2a_status create_common(int nx, int ny, int nz, int P, int bs, a2a_precision prec, a2a_distribution** out) {
+    if (!out) return fail(A2A_ERROR_INVALID_VALUE, "out is NULL");
+    *out = nullptr;
+    auto* h = new (std::nothrow) a2a_distribution();
+    if (!h) return fail(A2A_ERROR_OUT_OF_MEMORY, "host allocation failed");
+    const a2a_status s = setup_distribution(h->d, nx, ny, nz, P, bs, prec);
+    if (s != A2A_SUCCESS) {
+        release(h->d);
+        delete h;
+        return s;
+    }
+    *out = h;
+    return A2A_SUCCESS;
+}
+
+a2a_status need_cube(const Dist& d, const char* what) {
+    if (!d.cube) return fail(A2A_ERROR_NOT_IMPLEMENTED, "%s needs a cube (the reference API takes one Ng)", what);
+    return A2A_SUCCESS;
+}
+
+// 1D transforms of the contiguous length-Ng lines of a pencil buffer.
+a2a_status lines_1d(a2a_distribution* h, void** data, bool inv) {
+    if (!h) return fail(A2A_ERROR_INVALID_VALUE, "distribution is NULL");
+    Dist& d = h->d;
+    a2a_status s;
+    if ((s = need_cube(d, "1D pencil transforms")) != A2A_SUCCESS) return s;
+    if ((s = check_buf(data, "d_data")) != A2A_SUCCESS) return s;
+    const int n = d.ng[0];
+    A2A_CUDA(launch_pass(d, d.kline[0][inv], data[0], data[0], d.iota, d.pen_u, d.pen_v, d.tw[0], n, n, 1.0,
+                         d.stream),
+             "1D pass launch");
+    return finish(d, d.stream, true);
+}
+
+// One of the three in-place axis passes over the rank-major bricks.  Each
+// pass's gather/scatter addresses come from the brick offset tables, i.e. the
+// alltoall + unpack (and pack + alltoall) composites of the reference steps.
+cudaError_t run_pass(const Dist& d, int pass, bool inv, void* p, cudaStream_t st) {
+    const int i = inv ? 1 : 0;
+    switch (pass) {
+        case 0:  // Z pencils: lines (x, y), element z
+            return launch_pass(d, d.kline[2][i], p, p, d.off[2], d.off[0], d.off[1], d.tw[2], d.ng[0], d.ng[1], 1.0,
+                               st);
+        case 1:  // X pencils: lines (y, z), element x
+            return launch_pass(d, d.kbatch[0][i], p, p, d.off[0], d.off[1], d.off[2], d.tw[0], d.ng[1], d.ng[2],
+                               1.0, st);
+        default: {  // Y pencils: lines (x, z), element y; carries the inverse's 1/(nx ny nz)
+            const double scale = inv ? 1.0 / ((double)d.ng[0] * d.ng[1] * d.ng[2]) : 1.0;
+            return launch_pass(d, d.kbatch[1][i], p, p, d.off[1], d.off[0], d.off[2], d.tw[1], d.ng[0], d.ng[2],
+                               scale, st);
+        }
+    }
+}
+
+a2a_status check_dfft(a2a_dfft* f, void** data) {
+    if (!f) return fail(A2A_ERROR_INVALID_VALUE, "dfft is NULL");
+    if (!f->plans_made) return fail(A2A_ERROR_NO_PLANS, "make_plans has not been called");
+    return check_buf(data, "d_data");
+}
+
+// The fused transform: Z, X then Y pass.
+a2a_status fused(a2a_dfft* f, void** data, bool inv, cudaStream_t st, bool sync) {
+    a2a_status s;
+    if ((s = check_dfft(f, data)) != A2A_SUCCESS) return s;
+    const Dist& d = f->dist->d;
+    for (int pass = 0; pass < 3; ++pass) A2A_CUDA(run_pass(d, pass, inv, data[0], st), "axis pass launch");
+    return finish(d, st, sync);
+}
+
+template <typename F> a2a_status step(a2a_distribution* h, void** b1, void** b2, F&& body) {
+    if (!h) return fail(A2A_ERROR_INVALID_VALUE, "distribution is NULL");
+    Dist& d = h->d;
+    a2a_status s;
+    if ((s = need_cube(d, "the pencil steps")) != A2A_SUCCESS) return s;
+    if ((s = check_buf(b1, "d_buff1")) != A2A_SUCCESS) return s;
+    if ((s = check_buf(b2, "d_buff2")) != A2A_SUCCESS) return s;
+    if (b1[0] == b2[0]) return fail(A2A_ERROR_INVALID_VALUE, "d_buff1 and d_buff2 must be distinct buffers");
+    cudaError_t e = body(d, b1[0], b2[0]);
+    if (e != cudaSuccess) return cuda_fail(e, "pencil step launch");
+    return finish(d, d.stream, true);
+}
+
+}  // namespace
+
+extern "C" {
+
+a2a_status a2a_distribution_create(int ng, int world_size, int block_size, a2a_precision precision,
+                                   a2a_distribution** out) {
+    return create_common(ng, ng, ng, world_size, block_size, precision, out);
+}
+
+a2a_status a2a_distribution_create_box(int nx, int ny, int nz, int world_size, int block_size,
+                                       a2a_precision precision, a2a_distribution** out) {
+    return create_common(nx, ny, nz, world_size, block_size, precision, out);
+}
+
+a2a_status a2a_distribution_describe(const a2a_distribution* h, a2a_distribution_desc* o) {
+    if (!h || !o) return fail(A2A_ERROR_INVALID_VALUE, "NULL argument");
+    const Dist& d = h->d;
+    o->ndims = 3;
+    for (int a = 0; a < 3; ++a) {
+        o->ng[a] = d.ng[a];
+        o->dims[a] = d.dims[a];
+        o->local_grid_size[a] = d.local[a];
+    }
+    o->world_size = d.P;
+    o->nlocal = (int64_t)d.nlocal;
+    o->nsends = (int64_t)d.chunk;
+    o->block_size = d.block_size;
+    o->precision = (int)d.prec;
+    o->element_bytes = d.elem_bytes;
+    o->buffer_bytes = (size_t)d.P * d.nlocal * d.elem_bytes;
+    return A2A_SUCCESS;
+}
+
+a2a_status a2a_rank_coords(const a2a_distribution* h, int rank, int coords[3], int local_start[3]) {
+    if (!h || !coords) return fail(A2A_ERROR_INVALID_VALUE, "NULL argument");
+    const Dist& d = h->d;
+    if (rank < 0 || rank >= d.P) return fail(A2A_ERROR_INVALID_VALUE, "rank %d outside [0, %d)", rank, d.P);
+    coords[0] = rank / (d.dims[1] * d.dims[2]);
+    coords[1] = (rank / d.dims[2]) % d.dims[1];
+    coords[2] = rank % d.dims[2];
+    if (local_start)
+        for (int a = 0; a < 3; ++a) local_start[a] = d.local[a] * coords[a];
+    return A2A_SUCCESS;
+}
+
+a2a_status a2a_distribution_set_stream(a2a_distribution* h, void* stream) {
+    if (!h) return fail(A2A_ERROR_INVALID_VALUE, "distribution is NULL");
+    h->d.stream = static_cast<cudaStream_t>(stream);
+    return A2A_SUCCESS;
+}
+
+a2a_status a2a_get_z_pencils(a2a_distribution* h, void** b1, void** b2) {
+    return step(h, b1, b2, [](Dist& d, void* p1, void* p2) {
+        cudaError_t e = a2a::launch_alltoall(d, p1, p2, d.stream);
+        if (e == cudaSuccess) e = a2a::launch_pencil_remap(d, 2, true, p2, p1, d.stream);
+        return e;
+    });
+}
+
+a2a_status a2a_return_z_pencils(a2a_distribution* h, void** b1, void** b2) {
+    return step(h, b1, b2, [](Dist& d, void* p1, void* p2) {
+        cudaError_t e = a2a::launch_pencil_remap(d, 2, false, p1, p2, d.stream);
+        if (e == cudaSuccess) e = a2a::launch_alltoall(d, p2, p1, d.stream);
+        return e;
+    });
+}
+
+a2a_status a2a_get_x_pencils(a2a_distribution* h, void** b1, void** b2) {
+    return step(h, b1, b2, [](Dist& d, void* p1, void* p2) {
+        cudaError_t e = a2a::launch_fast_axis(d, 0, p1, p2, d.stream);
+        if (e == cudaSuccess) e = a2a::launch_alltoall(d, p2, p1, d.stream);
+        if (e == cudaSuccess) e = a2a::launch_pencil_remap(d, 0, true, p1, p2, d.stream);
+        return e;
+    });
+}
+
+a2a_status a2a_return_x_pencils(a2a_distribution* h, void** b1, void** b2) {
+    return step(h, b1, b2, [](Dist& d, void* p1, void* p2) {
+        cudaError_t e = a2a::launch_pencil_remap(d, 0, false, p2, p1, d.stream);
+        if (e == cudaSuccess) e = a2a::launch_alltoall(d, p1, p2, d.stream);
+        return e;
+    });
+}
+
+a2a_status a2a_get_y_pencils(a2a_distribution* h, void** b1, void** b2) {
+    return step(h, b1, b2, [](Dist& d, void* p1, void* p2) {
+        cudaError_t e = a2a::launch_fast_axis(d, 1, p2, p1, d.stream);
+        if (e == cudaSuccess) e = a2a::launch_alltoall(d, p1, p2, d.stream);
+        if (e == cudaSuccess) e = a2a::launch_pencil_remap(d, 1, true, p2, p1, d.stream);
+        return e;
+    });
+}
+
+a2a_status a2a_return_y_pencils(a2a_distribution* h, void** b1, void** b2) {
+    return step(h, b1, b2, [](Dist& d, void* p1, void* p2) {
+        cudaError_t e = a2a::launch_pencil_remap(d, 1, false, p2, p1, d.stream);
+        if (e == cudaSuccess) e = a2a::launch_alltoall(d, p1, p2, d.stream);
+        if (e == cudaSuccess) e = a2a::launch_fast_axis(d, 2, p2, p1, d.stream);
+        return e;
+    });
+}
+
+a2a_status a2a_distribution_finalize(a2a_distribution* h) {
+    if (!h) return A2A_SUCCESS;
+    release(h->d);
+    delete h;
+    return A2A_SUCCESS;
+}
+
+a2a_status a2a_forward_1d_fft(a2a_distribution* h, void** d_data) { return lines_1d(h, d_data, false); }
+a2a_status a2a_inverse_1d_fft(a2a_distribution* h, void** d_data) { return lines_1d(h, d_data, true); }
+
+a2a_status a2a_scale_fft(a2a_distribution* h, void** d_out, void** d_data) {
+    if (!h) return fail(A2A_ERROR_INVALID_VALUE, "distribution is NULL");
+    Dist& d = h->d;
+    a2a_status s;
+    if ((s = need_cube(d, "scale_fft")) != A2A_SUCCESS) return s;
+    if ((s = check_buf(d_out, "d_out")) != A2A_SUCCESS) return s;
+    if ((s = check_buf(d_data, "d_data")) != A2A_SUCCESS) return s;
+    const double ng = d.ng[0];
+    A2A_CUDA(a2a::launch_scale(d, d_data[0], d_out[0], ng * ng * ng, d.stream), "scale launch");
+    return finish(d, d.stream, true);
+}
+
+a2a_status a2a_fast_copy_fft(a2a_distribution* h, void** d_out, void** d_data) {
+    if (!h) return fail(A2A_ERROR_INVALID_VALUE, "distribution is NULL");
+    Dist& d = h->d;
+    a2a_status s;
+    if ((s = check_buf(d_out, "d_out")) != A2A_SUCCESS) return s;
+    if ((s = check_buf(d_data, "d_data")) != A2A_SUCCESS) return s;
+    A2A_CUDA(cudaMemcpyAsync(d_out[0], d_data[0], (size_t)d.P * d.nlocal * d.elem_bytes, cudaMemcpyDeviceToDevice,
+                             d.stream),
+             "cudaMemcpyAsync");
+    return finish(d, d.stream, true);
+}
+
+a2a_status a2a_dfft_create(a2a_distribution* dist, a2a_dfft** out) {
+    if (!dist || !out) return fail(A2A_ERROR_INVALID_VALUE, "NULL argument");
+    auto* f = new (std::nothrow) a2a_dfft();
+    if (!f) return fail(A2A_ERROR_OUT_OF_MEMORY, "host allocation failed");
+    f->dist = dist;
+    *out = f;
+    return A2A_SUCCESS;
+}
+
+a2a_status a2a_dfft_set_method(a2a_dfft* f, a2a_method m) {
+    if (!f) return fail(A2A_ERROR_INVALID_VALUE, "dfft is NULL");
+    if (m != A2A_METHOD_PLAIN && m != A2A_METHOD_SPLIT_BF16 && m != A2A_METHOD_SPLIT_FP16)
+        return fail(A2A_ERROR_INVALID_VALUE, "unknown method %d", (int)m);
+    if (m != A2A_METHOD_PLAIN) return fail(A2A_ERROR_NOT_IMPLEMENTED, "split tensor-core methods are not built yet");
+    f->method = m;
+    f->plans_made = false;
+    return A2A_SUCCESS;
+}
+
+a2a_status a2a_dfft_make_plans(a2a_dfft* f, void** d_scratch) {
+    if (!f) return fail(A2A_ERROR_INVALID_VALUE, "dfft is NULL");
+    const Dist& d = f->dist->d;
+    f->scratch = d_scratch ? d_scratch[0] : nullptr;
+    // every pass's inner batch extent must split into whole tiles
+    const struct {
+        const PassKernel* k;
+        int nv;
+        const char* name;
+    } passes[3] = {{&d.kline[2][0], d.ng[1], "Z"}, {&d.kbatch[0][0], d.ng[2], "X"}, {&d.kbatch[1][0], d.ng[2], "Y"}};
+    for (const auto& p : passes)
+        if (p.nv % p.k->lines)
+            return fail(A2A_ERROR_UNSUPPORTED, "%s pass: %d lines are not a multiple of the %d-line tile", p.name,
+                        p.nv, p.k->lines);
+    f->plans_made = true;
+    return A2A_SUCCESS;
+}
+
+a2a_status a2a_dfft_forward(a2a_dfft* f, void** d_data) {
+    return fused(f, d_data, false, f ? f->dist->d.stream : nullptr, true);
+}
+a2a_status a2a_dfft_inverse(a2a_dfft* f, void** d_data) {
+    return fused(f, d_data, true, f ? f->dist->d.stream : nullptr, true);
+}
+a2a_status a2a_dfft_backward(a2a_dfft* f, void** d_data) { return a2a_dfft_inverse(f, d_data); }
+a2a_status a2a_dfft_forward_async(a2a_dfft* f, void** d_data, void* stream) {
+    return fused(f, d_data, false, static_cast<cudaStream_t>(stream), false);
+}
+a2a_status a2a_dfft_inverse_async(a2a_dfft* f, void** d_data, void* stream) {
+    return fused(f, d_data, true, static_cast<cudaStream_t>(stream), false);
+}
+
+a2a_status a2a_dfft_execute_pass_async(a2a_dfft* f, void** d_data, int pass, int inverse, void* stream) {
+    a2a_status s;
+    if ((s = check_dfft(f, d_data)) != A2A_SUCCESS) return s;
+    if (pass < 0 || pass > 2) return fail(A2A_ERROR_INVALID_VALUE, "pass must be 0 (Z), 1 (X) or 2 (Y)");
+    A2A_CUDA(run_pass(f->dist->d, pass, inverse != 0, d_data[0], static_cast<cudaStream_t>(stream)),
+             "axis pass launch");
+    return A2A_SUCCESS;
+}
+
+a2a_status a2a_dfft_launches_per_transform(const a2a_dfft* f, int* out) {
+    if (!f || !out) return fail(A2A_ERROR_INVALID_VALUE, "NULL argument");
+    *out = 3;
+    return A2A_SUCCESS;
+}
+
+a2a_status a2a_dfft_destroy(a2a_dfft* f) {
+    delete f;
+    return A2A_SUCCESS;
+}
+
+const char* a2a_status_string(a2a_status s) {
+    switch (s) {
+        case A2A_SUCCESS: return "success";
+        case A2A_ERROR_INVALID_VALUE: return "invalid value";
+        case A2A_ERROR_DECOMPOSITION: return "decomposition rejected";
+        case A2A_ERROR_UNSUPPORTED: return "unsupported size";
+        case A2A_ERROR_NO_PLANS: return "make_plans not called";
+        case A2A_ERROR_MISALIGNED: return "misaligned buffer";
+        case A2A_ERROR_CUDA: return "CUDA error";
+        case A2A_ERROR_OUT_OF_MEMORY: return "out of memory";
+        case A2A_ERROR_TIMEOUT: return "device wait timed out";
+        case A2A_ERROR_NOT_IMPLEMENTED: return "not implemented";
+    }
+    return "unknown status";
+}
+
+const char* a2a_last_error(void) { return g_last_error.c_str(); }
+
+int a2a_version(void) { return A2AFFT_B200_VERSION; }
+
+}  // extern "C"

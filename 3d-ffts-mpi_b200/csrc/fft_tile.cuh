@@ -1,0 +1,396 @@
+// Batched 1D FFT tile engine for sm_100a: Stockham auto-sort, mixed radix
+// 2/3/4/8/16, one tile of B lines of length N per CTA, staged through shared
+// memory, global traffic fused with the pencil gather/scatter.
+//
+// This replaces the batched cuFFT calls of the reference
+// (src/a2afft/dfft/kernels/a2affts.cu:7-76, cufftPlan1d + cufftExecZ2Z/C2C on
+// nlocal/Ng contiguous pencils) AND the pack/unpack remaps around them
+// (src/a2afft/distribution/kernels/a2apencils.cu): a line's element n lives at
+// `base[line] + offA[n]`, where the tables encode the alltoall + unpack
+// composite for the virtual-rank brick layout, so the gather happens inside
+// the first stage's loads and the scatter inside the last stage's stores.
+//
+// Stockham stage s (radix R, Ns = product of the radices before s):
+//   butterfly j in [0, N/R):  x_r = in[j + r N/R] * W_{Ns R}^{r (j mod Ns)}
+//                             y   = DFT_R(x)
+//                             out[(j/Ns) Ns R + (j mod Ns) + r Ns] = y_r
+// Stage 0 has no twiddles and reads global memory straight into registers;
+// the last stage (Ns R = N) writes global memory straight from registers.
+// Shared memory holds one tile, updated in place (every thread reads its
+// butterfly inputs, the block synchronises, then writes).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace a2a {
+
+// --------------------------------------------------------------------------
+// complex helpers
+// --------------------------------------------------------------------------
+template <typename T> struct CxOf;
+template <> struct CxOf<float> { using type = float2; };
+template <> struct CxOf<double> { using type = double2; };
+template <typename T> using cx = typename CxOf<T>::type;
+
+template <typename V> struct RealOf;
+template <> struct RealOf<float2> { using type = float; };
+template <> struct RealOf<double2> { using type = double; };
+
+template <typename V>
+__host__ __device__ __forceinline__ V mk(typename RealOf<V>::type re, typename RealOf<V>::type im) {
+    V v;
+    v.x = re;
+    v.y = im;
+    return v;
+}
+template <typename V> __device__ __forceinline__ V add(V a, V b) { return mk<V>(a.x + b.x, a.y + b.y); }
+template <typename V> __device__ __forceinline__ V sub(V a, V b) { return mk<V>(a.x - b.x, a.y - b.y); }
+template <typename V> __device__ __forceinline__ V neg(V a) { return mk<V>(-a.x, -a.y); }
+// a * (+i) and a * (-i)
+template <typename V> __device__ __forceinline__ V mul_pi(V a) { return mk<V>(-a.y, a.x); }
+template <typename V> __device__ __forceinline__ V mul_mi(V a) { return mk<V>(a.y, -a.x); }
+template <typename V> __device__ __forceinline__ V scl(V a, typename RealOf<V>::type s) {
+    return mk<V>(a.x * s, a.y * s);
+}
+// a * (c + i s)
+template <typename V>
+__device__ __forceinline__ V cmul(V a, typename RealOf<V>::type c, typename RealOf<V>::type s) {
+    return mk<V>(a.x * c - a.y * s, a.x * s + a.y * c);
+}
+// a * w, or a * conj(w)
+template <bool CONJ, typename V> __device__ __forceinline__ V cmulw(V a, V w) {
+    return CONJ ? cmul(a, w.x, -w.y) : cmul(a, w.x, w.y);
+}
+
+// cos(2 pi m / 16) and sin(2 pi m / 16), m = 0..15: the sixteenth roots of
+// unity, to 21 significant digits.
+__host__ __device__ constexpr double root16_cos(int m) {
+    switch (m & 15) {
+        case 0: return 1.0;
+        case 1: case 15: return 0.923879532511286756128;
+        case 2: case 14: return 0.707106781186547524401;
+        case 3: case 13: return 0.382683432365089771728;
+        case 4: case 12: return 0.0;
+        case 5: case 11: return -0.382683432365089771728;
+        case 6: case 10: return -0.707106781186547524401;
+        case 7: case 9: return -0.923879532511286756128;
+        default: return -1.0;
+    }
+}
+__host__ __device__ constexpr double root16_sin(int m) { return root16_cos((m + 12) & 15); }
+// sin(2 pi / 3)
+constexpr double kSin60 = 0.866025403784438646763723170753;
+
+// v * W_R^k with W_R = exp(-2 pi i / R) (forward) or its conjugate (INV).
+// R divides 16; k is a compile-time constant once the caller's loops unroll,
+// so the switch folds to one case.
+template <int R, bool INV, typename V> __device__ __forceinline__ V twc(V v, int k) {
+    static_assert(16 % R == 0, "in-register twiddles are sixteenth roots of unity");
+    using T = typename RealOf<V>::type;
+    const int m = ((k % R) + R) % R * (16 / R);
+    switch (m) {
+        case 0: return v;
+        case 4: return INV ? mul_pi(v) : mul_mi(v);
+        case 8: return neg(v);
+        case 12: return INV ? mul_mi(v) : mul_pi(v);
+        default: {
+            const T c = (T)root16_cos(m);
+            const T s = (T)root16_sin(m);
+            return cmul(v, c, INV ? s : -s);
+        }
+    }
+}
+
+// --------------------------------------------------------------------------
+// small DFTs in registers, natural order in and out:
+//   y_k = sum_n x_n exp(-+ 2 pi i n k / R)
+// --------------------------------------------------------------------------
+template <int R, bool INV, typename V> struct Dft;
+
+template <bool INV, typename V> struct Dft<1, INV, V> {
+    static __device__ __forceinline__ void run(V*) {}
+};
+
+template <bool INV, typename V> struct Dft<2, INV, V> {
+    static __device__ __forceinline__ void run(V* v) {
+        const V a = v[0];
+        v[0] = add(a, v[1]);
+        v[1] = sub(a, v[1]);
+    }
+};
+
+template <bool INV, typename V> struct Dft<3, INV, V> {
+    static __device__ __forceinline__ void run(V* v) {
+        using T = typename RealOf<V>::type;
+        const V t = add(v[1], v[2]);
+        const V d = scl(sub(v[1], v[2]), (T)kSin60);
+        const V m = sub(v[0], scl(t, (T)0.5));
+        const V rot = INV ? mul_pi(d) : mul_mi(d);  // -+ i sin60 (x1 - x2)
+        v[0] = add(v[0], t);
+        v[1] = add(m, rot);
+        v[2] = sub(m, rot);
+    }
+};
+
+template <bool INV, typename V> struct Dft<4, INV, V> {
+    static __device__ __forceinline__ void run(V* v) {
+        const V a = add(v[0], v[2]);
+        const V b = sub(v[0], v[2]);
+        const V c = add(v[1], v[3]);
+        V d = sub(v[1], v[3]);
+        d = INV ? mul_pi(d) : mul_mi(d);
+        v[0] = add(a, c);
+        v[2] = sub(a, c);
+        v[1] = add(b, d);
+        v[3] = sub(b, d);
+    }
+};
+
+// R = R1 * R2 split: n = R2 m + p, k = k1 + R1 k2,
+// y[k1 + R1 k2] = sum_p W_R2^{p k2} ( W_R^{p k1} sum_m x[R2 m + p] W_R1^{m k1} )
+template <int R1, int R2, bool INV, typename V> __device__ __forceinline__ void dft_split(V* v) {
+    constexpr int R = R1 * R2;
+    V a[R];
+#pragma unroll
+    for (int p = 0; p < R2; ++p) {
+        V col[R1];
+#pragma unroll
+        for (int m = 0; m < R1; ++m) col[m] = v[R2 * m + p];
+        Dft<R1, INV, V>::run(col);
+#pragma unroll
+        for (int k1 = 0; k1 < R1; ++k1) a[p * R1 + k1] = twc<R, INV>(col[k1], p * k1);
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) {
+        V row[R2];
+#pragma unroll
+        for (int p = 0; p < R2; ++p) row[p] = a[p * R1 + k1];
+        Dft<R2, INV, V>::run(row);
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) v[k1 + R1 * k2] = row[k2];
+    }
+}
+
+template <bool INV, typename V> struct Dft<8, INV, V> {
+    static __device__ __forceinline__ void run(V* v) { dft_split<4, 2, INV>(v); }
+};
+template <bool INV, typename V> struct Dft<16, INV, V> {
+    static __device__ __forceinline__ void run(V* v) { dft_split<4, 4, INV>(v); }
+};
+
+// --------------------------------------------------------------------------
+// radix plans
+// --------------------------------------------------------------------------
+template <int... Rs> struct RadixPlan {
+    static constexpr int S = sizeof...(Rs);
+    static constexpr int r[S] = {Rs...};
+    static constexpr int N = (Rs * ...);
+    // Ns before stage s
+    __host__ __device__ static constexpr int ns(int s) {
+        int x = 1;
+        for (int i = 0; i < s; ++i) x *= r[i];
+        return x;
+    }
+    // offset of stage s's twiddle table (stages >= 1; (R-1)*Ns entries each,
+    // laid out [r-1][j mod Ns])
+    __host__ __device__ static constexpr int twoff(int s) {
+        int o = 0;
+        for (int i = 1; i < s; ++i) o += (r[i] - 1) * ns(i);
+        return o;
+    }
+    __host__ __device__ static constexpr int twtotal() { return twoff(S); }
+};
+
+enum PassMode : int {
+    // line elements are contiguous in memory (runs of the brick's l_axis):
+    // threads walk along a line (the reference's Z pencils, and every 1D
+    // call on pencil buffers)
+    MODE_LINE = 0,
+    // consecutive lines are contiguous in memory: threads walk across lines
+    // (X and Y passes over z-fastest bricks)
+    MODE_BATCH = 1
+};
+
+template <typename T> struct PassArgs {
+    const cx<T>* src;      // may alias dst (in-place pass)
+    cx<T>* dst;
+    const uint32_t* offA;  // element offset of index n along the transform axis (N entries)
+    const uint32_t* offU;  // line offset, outer batch coordinate (NU entries)
+    const uint32_t* offV;  // line offset, inner batch coordinate (NV entries)
+    const cx<T>* tw;       // stage twiddles, forward sign, RadixPlan::twoff layout
+    int NU;
+    int NV;                // multiple of B
+    T scale;               // multiplies every stored element
+};
+
+// Line/butterfly index mapping: butterfly q of a stage with Nb = N/R
+// butterflies per line.
+template <int MODE, int B, int NB> __device__ __forceinline__ void bf_map(int q, int& b, int& j) {
+    if constexpr (MODE == MODE_BATCH) {
+        b = q % B;
+        j = q / B;
+    } else {
+        j = q % NB;
+        b = q / NB;
+    }
+}
+
+// shared-memory slot of element n of tile line b
+template <int MODE, int B, int N> __device__ __forceinline__ int sidx(int b, int n) {
+    if constexpr (MODE == MODE_BATCH) {
+        return n * B + b;
+    } else {
+        return b * (N + N / 32) + n + (n >> 5);
+    }
+}
+
+template <int MODE, int B, int N> struct TileGeom {
+    static constexpr int elems = (MODE == MODE_BATCH) ? N * B : B * (N + N / 32);
+};
+
+// streaming loads/stores: each element is touched once per pass
+template <typename V> __device__ __forceinline__ V ld_stream(const V* p) { return __ldcs(p); }
+template <typename V> __device__ __forceinline__ void st_stream(V* p, V v) { __stcs(p, v); }
+
+template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV, int s>
+__device__ __forceinline__ void run_stage(const PassArgs<T>& a, cx<T>* tile, const cx<T>* tw,
+                                          const uint32_t* offA_s, const size_t* base_s, int tid) {
+    using V = cx<T>;
+    constexpr int N = PLAN::N;
+    constexpr int R = PLAN::r[s];
+    constexpr int NS = PLAN::ns(s);
+    constexpr int NBL = N / R;             // butterflies per line
+    constexpr int NBT = B * NBL;           // butterflies per tile
+    constexpr int K = (NBT + THREADS - 1) / THREADS;
+    constexpr bool EXACT = (NBT % THREADS) == 0;
+    constexpr bool LAST = (s == PLAN::S - 1);
+    constexpr int TWO = PLAN::twoff(s);
+
+    V x[K][R];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const int q = tid + k * THREADS;
+        if (EXACT || q < NBT) {
+            int b, j;
+            bf_map<MODE, B, NBL>(q, b, j);
+#pragma unroll
+            for (int r = 0; r < R; ++r) x[k][r] = tile[sidx<MODE, B, N>(b, j + r * NBL)];
+        }
+    }
+    __syncthreads();  // the tile is updated in place
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const int q = tid + k * THREADS;
+        if (EXACT || q < NBT) {
+            int b, j;
+            bf_map<MODE, B, NBL>(q, b, j);
+            const int m = j % NS;
+#pragma unroll
+            for (int r = 1; r < R; ++r) x[k][r] = cmulw<INV>(x[k][r], tw[TWO + (r - 1) * NS + m]);
+            Dft<R, INV, V>::run(x[k]);
+            if constexpr (LAST) {
+                const size_t lb = base_s[b];
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    st_stream(a.dst + lb + offA_s[j + r * NBL], scl(x[k][r], a.scale));
+            } else {
+                const int jd = (j / NS) * NS * R + m;
+#pragma unroll
+                for (int r = 0; r < R; ++r) tile[sidx<MODE, B, N>(b, jd + r * NS)] = x[k][r];
+            }
+        }
+    }
+    if constexpr (!LAST) {
+        __syncthreads();
+        run_stage<T, PLAN, B, THREADS, MODE, INV, s + 1>(a, tile, tw, offA_s, base_s, tid);
+    }
+}
+
+template <typename T, class PLAN, int B, int MODE>
+constexpr size_t pass_smem_bytes() {
+    constexpr int N = PLAN::N;
+    size_t bytes = sizeof(cx<T>) * (size_t)(TileGeom<MODE, B, N>::elems + PLAN::twtotal());
+    bytes += sizeof(uint32_t) * (size_t)N;
+    bytes = (bytes + 15) & ~size_t(15);
+    bytes += sizeof(size_t) * (size_t)B;
+    return bytes;
+}
+
+// One CTA = one tile of B lines: lines (u, v0 .. v0+B-1).
+template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV>
+__global__ void __launch_bounds__(THREADS) fft_pass_kernel(const PassArgs<T> a) {
+    using V = cx<T>;
+    constexpr int N = PLAN::N;
+    constexpr int R0 = PLAN::r[0];
+    constexpr int NBL = N / R0;
+    constexpr int NBT = B * NBL;
+    constexpr int K = (NBT + THREADS - 1) / THREADS;
+    constexpr bool EXACT = (NBT % THREADS) == 0;
+    constexpr int TWN = PLAN::twtotal();
+    static_assert(MODE != MODE_BATCH || THREADS % B == 0, "batch mode needs THREADS % B == 0");
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* tile = reinterpret_cast<V*>(smem_raw);
+    V* tw = tile + TileGeom<MODE, B, N>::elems;
+    uint32_t* offA_s = reinterpret_cast<uint32_t*>(tw + TWN);
+    size_t* base_s = reinterpret_cast<size_t*>(
+        smem_raw + ((sizeof(V) * (size_t)(TileGeom<MODE, B, N>::elems + TWN) + sizeof(uint32_t) * N + 15) &
+                    ~size_t(15)));
+
+    const int tid = threadIdx.x;
+    const int tilesV = a.NV / B;
+    const int u = blockIdx.x / tilesV;
+    const int v0 = (blockIdx.x - u * tilesV) * B;
+    const size_t ubase = a.offU[u];
+
+    // stage 0: global -> registers, gather addresses straight from the tables
+    V x[K][R0];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const int q = tid + k * THREADS;
+        if (EXACT || q < NBT) {
+            int b, j;
+            bf_map<MODE, B, NBL>(q, b, j);
+            const size_t lb = ubase + __ldg(a.offV + v0 + b);
+#pragma unroll
+            for (int r = 0; r < R0; ++r) x[k][r] = ld_stream(a.src + lb + __ldg(a.offA + j + r * NBL));
+        }
+    }
+    // tables for the later stages (overlaps the loads in flight)
+    for (int i = tid; i < TWN; i += THREADS) tw[i] = a.tw[i];
+    for (int i = tid; i < N; i += THREADS) offA_s[i] = a.offA[i];
+    for (int i = tid; i < B; i += THREADS) base_s[i] = ubase + a.offV[v0 + i];
+
+    if constexpr (PLAN::S == 1) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int q = tid + k * THREADS;
+            if (EXACT || q < NBT) {
+                int b, j;
+                bf_map<MODE, B, NBL>(q, b, j);
+                Dft<R0, INV, V>::run(x[k]);
+                const size_t lb = ubase + __ldg(a.offV + v0 + b);
+#pragma unroll
+                for (int r = 0; r < R0; ++r)
+                    st_stream(a.dst + lb + __ldg(a.offA + j + r * NBL), scl(x[k][r], a.scale));
+            }
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int q = tid + k * THREADS;
+            if (EXACT || q < NBT) {
+                int b, j;
+                bf_map<MODE, B, NBL>(q, b, j);
+                Dft<R0, INV, V>::run(x[k]);
+#pragma unroll
+                for (int r = 0; r < R0; ++r) tile[sidx<MODE, B, N>(b, j * R0 + r)] = x[k][r];
+            }
+        }
+        __syncthreads();
+        run_stage<T, PLAN, B, THREADS, MODE, INV, 1>(a, tile, tw, offA_s, base_s, tid);
+    }
+}
+
+}  // namespace a2a

@@ -1,0 +1,50 @@
+// Host-side state shared by the translation units of liba2afft_b200.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/a2afft_b200.h"
+#include "fft_registry.cuh"
+
+namespace a2a {
+
+// Everything an a2aDistribution carries, for all virtual ranks at once.
+struct Dist {
+    int ng[3] = {0, 0, 0};
+    int P = 0;
+    int dims[3] = {0, 0, 0};
+    int local[3] = {0, 0, 0};
+    uint64_t nlocal = 0;
+    uint64_t chunk = 0;  // nsends = nlocal / P
+    int block_size = 0;
+    a2a_precision prec = A2A_C128;
+    size_t elem_bytes = 16;
+    bool cube = true;
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    int sms = 148;
+
+    // device tables (one allocation): brick offsets per axis, identity
+    // offsets and the pencil-buffer line bases (cubes only)
+    uint32_t* d_tables = nullptr;
+    const uint32_t* off[3] = {nullptr, nullptr, nullptr};
+    const uint32_t* iota = nullptr;
+    const uint32_t* pen_u = nullptr;
+    const uint32_t* pen_v = nullptr;
+    // FP64-generated stage twiddles per axis (forward sign), in the
+    // precision of the plan
+    void* d_tw = nullptr;
+    const void* tw[3] = {nullptr, nullptr, nullptr};
+    // pass kernels per axis: [axis][inverse]
+    PassKernel kline[3][2];
+    PassKernel kbatch[3][2];
+};
+
+// remap.cu
+cudaError_t launch_alltoall(const Dist& d, const void* src, void* dst, cudaStream_t st);
+cudaError_t launch_pencil_remap(const Dist& d, int axis, bool unpack, const void* src, void* dst, cudaStream_t st);
+cudaError_t launch_fast_axis(const Dist& d, int which, const void* src, void* dst, cudaStream_t st);
+cudaError_t launch_scale(const Dist& d, const void* src, void* dst, double divisor, cudaStream_t st);
+
+}  // namespace a2a

@@ -1,0 +1,409 @@
+#!/usr/bin/env python
+"""Benchmark of the a2afft_b200 pencil-decomposed 3D FFT on B200.
+
+Workload: 512^3 complex64 C2C forward + inverse on a 64-rank virtual grid
+(dims [4,4,4], 128^3 bricks), input U[-1,1) real/imag plus 3 pure tones of
+amplitude 100 (seed 2) -- the precision-form configuration the headline metric
+is quoted on.  One step = one forward + one inverse of the whole cube, in
+place.  The 1 GiB buffer is larger than the 126 MB L2, so no flush is needed
+between steps.
+
+Printed (rank 0, one JSON line):
+  value         ms per forward+inverse, device-resident data, CUDA events on the
+                launching stream (max over ranks; with N ranks, N independent
+                replicas run and value = max time / N)
+  e2e           the same through the public API with pinned HOST buffers: the
+                H2D copy of the input and the D2H copy of the result are inside
+                every timed step
+  roofline      the dominant pass kernel: algorithmic bytes (2 x Ng^3 x 8 B per
+                launch) / its mean CUDA-event duration, against the measured HBM
+                copy bandwidth
+  cpu_baseline  the reference's step sequence on the host cores (oracle port:
+                numpy remaps + scipy pocketfft), on a 256^3 sample scaled to
+                512^3 by N log N
+
+``--impl reference`` times only that CPU pipeline (rank 0) on the same
+workload and prints its line with "impl": "reference".
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "512^3 C2C fwd+inv ms & %HBM peak: split-TC vs plain FP32 at L2 err<=1e-6"
+NG = 512
+RANKS = 64
+SEED = 2
+FALLBACK_HBM_GBS = 6650.0
+CPU_SAMPLE_NG = 256
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--method", choices=["plain", "split_bf16", "split_fp16"], default="plain")
+    ap.add_argument("--ng", type=int, default=NG)
+    ap.add_argument("--ranks", type=int, default=RANKS)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg")
+    ap.add_argument("--no-check", action="store_true", help="skip the accuracy check (profiling runs)")
+    return ap.parse_args()
+
+
+def workload_name(ng, ranks, dims):
+    return (f"{ng}^3 complex64 C2C forward+inverse, {ranks} virtual ranks (dims {dims}), "
+            f"U[-1,1)+3 tones x100 seed {SEED}")
+
+
+def cpu_pipeline_ms(ng_sample, ranks, ng_target, reps=1):
+    """The reference's host step sequence (oracle port) on one cube of
+    ng_sample^3, best of `reps`, scaled to ng_target^3 by N log N."""
+    import numpy as np
+
+    import __graft_entry__ as entry
+
+    O = entry.load_oracle()
+    cores = os.cpu_count() or 1
+    d = O.Decomp(ng_sample, ranks)
+    g = O.make_input("uniform", (ng_sample,) * 3, seed=SEED, dtype=np.complex64, tones=3)
+    b = O.global_to_bricks(g, d)
+    lines = O.scipy_lines(cores)
+    best = float("inf")
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        f = O.forward(b, d, lines, np.complex64)
+        O.inverse(f, d, lines, np.complex64)
+        best = min(best, time.perf_counter() - t0)
+    n_s, n_t = float(ng_sample) ** 3, float(ng_target) ** 3
+    scale = (n_t * math.log2(n_t)) / (n_s * math.log2(n_s))
+    sample = (f"one forward+inverse of a {ng_sample}^3 complex64 cube on {ranks} virtual ranks "
+              f"(dims {d.dims}), best of {reps}, x{scale:.3f} (N log N) to {ng_target}^3")
+    return best * 1e3 * scale, cores, sample, best
+
+
+class ClockSampler:
+    """Samples SM clock and clock-event reasons through NVML while running."""
+
+    REASONS = {0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+               0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+               0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting"}
+
+    def __init__(self, torch_device_index):
+        self.samples, self.reasons, self.max_mhz = [], 0, None
+        self._stop = threading.Event()
+        self._h = None
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            self._nv = pynvml
+            import torch
+
+            props = torch.cuda.get_device_properties(torch_device_index)
+            h = None
+            for attr in ("pci_bus_id",):
+                bus = getattr(props, attr, None)
+                if bus is not None:
+                    try:
+                        h = pynvml.nvmlDeviceGetHandleByPciBusId(f"{int(props.pci_domain_id):08x}:{int(bus):02x}:"
+                                                                 f"{int(props.pci_device_id):02x}.0")
+                    except Exception:
+                        h = None
+            if h is None:
+                vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+                idx = int(vis.split(",")[torch_device_index]) if vis else torch_device_index
+                h = pynvml.nvmlDeviceGetHandleByIndex(idx)
+            self._h = h
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+        except Exception as e:  # no NVML: clocks reported as unavailable
+            self.error = str(e)
+
+    def _run(self):
+        nv = self._nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
+                self.reasons |= int(nv.nvmlDeviceGetCurrentClocksEventReasons(self._h))
+            except Exception:
+                pass
+            time.sleep(0.005)
+
+    def __enter__(self):
+        if self._h is not None:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._h is not None:
+            self._t.join()
+
+    def summary(self):
+        if self._h is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvml unavailable"]}
+        names = [n for bit, n in self.REASONS.items() if self.reasons & bit and n != "gpu_idle"]
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None, "sm_max_mhz": self.max_mhz,
+                "reasons": names, "samples": len(self.samples)}
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic(kernel_key):
+    """DRAM bytes per launch from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic.txt")
+    try:
+        with open(path) as fh:
+            for line in fh:
+                parts = line.split()
+                if len(parts) >= 2 and parts[0] == kernel_key:
+                    return float(parts[1])
+    except OSError:
+        pass
+    return None
+
+
+def synth_bricks(torch, ng, dims, seed, device):
+    """Seeded U[-1,1) re/im + 3 tones of amplitude 100, generated on the GPU,
+    returned in the rank-major brick layout."""
+    gen = torch.Generator(device=device).manual_seed(seed)
+    shape = (ng, ng, ng)
+    re = torch.rand(shape, generator=gen, device=device, dtype=torch.float32) * 2 - 1
+    im = torch.rand(shape, generator=gen, device=device, dtype=torch.float32) * 2 - 1
+    g = torch.complex(re, im)
+    del re, im
+    ks = torch.randint(0, ng, (3, 3), generator=gen, device=device)
+    idx = torch.arange(ng, device=device, dtype=torch.int64)
+    for kx, ky, kz in ks.tolist():
+        ph = ((kx * idx)[:, None, None] + (ky * idx)[None, :, None] + (kz * idx)[None, None, :]) % ng
+        g += 100.0 * torch.polar(torch.ones((), device=device), ph.to(torch.float32) * (2 * math.pi / ng))
+        del ph
+    d0, d1, d2 = dims
+    lx, ly, lz = ng // d0, ng // d1, ng // d2
+    b = g.reshape(d0, lx, d1, ly, d2, lz).permute(0, 2, 4, 1, 3, 5).contiguous().reshape(-1)
+    del g
+    return b
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    ng_target = args.ng
+    # calibrate the sample size so the whole run stays within a few minutes
+    est_ms, cores, _, wall = cpu_pipeline_ms(128, args.ranks, ng_target)
+    sample_ng = CPU_SAMPLE_NG if wall * 8.5 * (args.steps + args.warmup) < 240 else 128
+    times = []
+    for i in range(args.warmup + args.steps):
+        ms, cores, sample, _ = cpu_pipeline_ms(sample_ng, args.ranks, ng_target)
+        if i >= args.warmup:
+            times.append(ms)
+    value = statistics.mean(times)
+    import __graft_entry__ as entry
+
+    dims = entry.load_oracle().dims_create(args.ranks, 3)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "ms", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(value, 3), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": workload_name(ng_target, args.ranks, dims), "ng": ng_target,
+                   "world_size": args.ranks, "precision": "c64", "sample_ng": sample_ng},
+        "cpu_baseline": {"value": round(value, 3), "unit": "ms", "cores": cores, "kind": "port",
+                         "sample": sample + "; remaps single-threaded numpy, 1D transforms scipy.fft workers=cores"},
+        "e2e": {"value": round(value, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    import __graft_entry__ as entry
+
+    pkg = entry.load_package()
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    ng, ranks = args.ng, args.ranks
+    dist = pkg.a2aDistribution(ranks, ng, 64, precision="c64")
+    dfft = pkg.a2adfft(dist, method=args.method)
+    dfft.make_plans()
+    x = synth_bricks(torch, ng, dist.dims, SEED, dev)
+    x0 = x.clone()
+    stream = torch.cuda.Stream(device=dev)
+    nbytes_buf = x.numel() * x.element_size()
+
+    def step():
+        for inv in (0, 1):
+            for p in range(3):
+                dfft.execute_pass(x, p, inv, stream)
+
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        for _ in range(max(args.warmup, 3)):
+            step()
+    torch.cuda.synchronize()
+
+    # accuracy (outside the timed region): forward vs our FP64 path, round trip
+    rel_err = None
+    rt_err = None
+    if (world == 1 or rank == 0) and not args.no_check:
+        x.copy_(x0)
+        dfft.forward(x)
+        d64 = pkg.a2aDistribution(ranks, ng, 64, precision="c128")
+        f64 = pkg.a2adfft(d64)
+        f64.make_plans()
+        y = x0.to(torch.complex128)
+        f64.forward(y)
+        rel_err = float(torch.linalg.vector_norm(x.to(torch.complex128) - y) / torch.linalg.vector_norm(y))
+        del y, f64, d64
+        dfft.inverse(x)
+        rt_err = float(torch.linalg.vector_norm((x - x0).to(torch.complex128)) /
+                       torch.linalg.vector_norm(x0.to(torch.complex128)))
+        torch.cuda.empty_cache()
+    x.copy_(x0)
+
+    # timed region: K steps, an event between every pass launch
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(6 * args.steps + 1)]
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        with torch.cuda.stream(stream):
+            evs[0].record(stream)
+            k = 1
+            for _ in range(args.steps):
+                for inv in (0, 1):
+                    for p in range(3):
+                        dfft.execute_pass(x, p, inv, stream)
+                        evs[k].record(stream)
+                        k += 1
+        torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    total_ms = evs[0].elapsed_time(evs[-1])
+    per_pass = [[] for _ in range(6)]
+    for i in range(6 * args.steps):
+        per_pass[i % 6].append(evs[i].elapsed_time(evs[i + 1]))
+    step_ms = total_ms / args.steps
+    if world > 1:
+        t = torch.tensor([step_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        step_ms = float(t.item())
+
+    # e2e through the public API with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        hin = x0.cpu().pin_memory()
+        hout = torch.empty_like(hin).pin_memory()
+        ke = max(1, min(args.steps, 10))
+        with torch.cuda.stream(stream):
+            for _ in range(2):
+                x.copy_(hin, non_blocking=True)
+                dfft.forward(x, stream)
+                dfft.inverse(x, stream)
+                hout.copy_(x, non_blocking=True)
+            stream.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(ke):
+                x.copy_(hin, non_blocking=True)
+                dfft.forward(x, stream)
+                dfft.inverse(x, stream)
+                hout.copy_(x, non_blocking=True)
+            e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = e0.elapsed_time(e1) / ke
+        if world > 1:
+            t = torch.tensor([e2e_ms], device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        e2e = {"value": round(e2e_ms / world, 3), "unit": "ms", "h2d_bytes_per_step": nbytes_buf,
+               "d2h_bytes_per_step": nbytes_buf, "steps": ke}
+        del hin, hout
+
+    if rank != 0:
+        return
+    peak, peak_kind = measured_peak()
+    names = ["Z_fwd", "X_fwd", "Y_fwd", "Z_inv", "X_inv", "Y_inv"]
+    means = [statistics.mean(v) for v in per_pass]
+    dom = max(range(6), key=lambda i: means[i])
+    alg_bytes = 2.0 * float(ng) ** 3 * 8  # one read + one write of the cube per pass
+    achieved = alg_bytes / (means[dom] * 1e-3) / 1e9
+    key = ["line", "batch", "batch"][dom % 3] + f"_{ng}_c64"
+    traffic = profiled_traffic(key)
+    alg_total = 6 * alg_bytes
+    value = step_ms / world
+    line = {
+        "metric": METRIC, "value": round(value, 4), "unit": "ms", "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": round(step_ms, 4), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "impl": "a2afft_b200",
+        "config": {"workload": workload_name(ng, ranks, dist.dims), "ng": ng, "world_size": ranks,
+                   "dims": dist.dims, "precision": "c64", "method": args.method,
+                   "l2": "inputs 1 GiB > 126 MB L2 (no flush)",
+                   "replicas": world},
+        "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": round(achieved, 1), "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "traffic": traffic, "algorithmic_bytes": alg_bytes},
+        "per_pass_ms": {n: round(m, 4) for n, m in zip(names, means)},
+        "effective_gbs": round(alg_total / (step_ms * 1e-3) / 1e9, 1),
+        "hbm_frac": round(alg_total / (step_ms * 1e-3) / 1e9 / peak, 4),
+        "transforms_per_s": round(2 * 1e3 / step_ms, 2),
+        "gflops": round(2 * 5 * float(ng) ** 3 * math.log2(float(ng) ** 3) / (step_ms * 1e-3) / 1e9, 1),
+        "rel_l2_vs_fp64": rel_err, "roundtrip_rel_l2": rt_err,
+        "clocks": clk.summary(),
+        "gpu_launches": 6 * args.steps,
+        "e2e": e2e,
+    }
+    if world == 1 and not args.no_cpu:
+        ms, cores, sample, _ = cpu_pipeline_ms(CPU_SAMPLE_NG, ranks, ng)
+        line["cpu_baseline"] = {"value": round(ms, 1), "unit": "ms", "cores": cores, "kind": "port",
+                                "sample": sample + "; remaps single-threaded numpy, 1D transforms scipy.fft "
+                                "workers=cores"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,188 @@
+/*
+ * a2afft_b200 -- C ABI of a B200 (sm_100a) pencil-decomposed 3D FFT that is a
+ * drop-in for the a2afft library of humz2k/3D-FFTs-MPI (src/a2afft).
+ *
+ * The reference runs one MPI rank per GPU: rank r owns a brick of the global
+ * Ng^3 grid (brick grid dims = MPI_Dims_create(P, 3)) stored [x][y][z]
+ * row-major, and a 3D transform is three rounds of
+ * alltoall + pack/unpack + batched 1D cuFFT.  Here the P ranks are VIRTUAL:
+ * every rank's brick lives in one device buffer, rank-major -- rank r's brick
+ * starts at element r * nlocal and has exactly the reference's per-rank
+ * layout.  A "buffer" below is therefore world_size * nlocal complex elements
+ * (interleaved re/im; double for A2A_C128, float for A2A_C64).
+ *
+ * Buffers are passed as `void**` exactly like the reference passes
+ * `fftPrecision**` (the library reads buf[0]; it never writes the pointer).
+ * Every entry point returns an a2a_status; nothing aborts or prints.
+ * Calls without a stream argument run on the object's stream (default: the
+ * legacy default stream) and synchronise it before returning, which is the
+ * reference's behaviour (every step there ends in cudaDeviceSynchronize).
+ * `_async` variants only enqueue work.
+ */
+#ifndef A2AFFT_B200_H
+#define A2AFFT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define A2AFFT_B200_VERSION 100 /* 1.0.0 */
+
+typedef enum a2a_status {
+    A2A_SUCCESS = 0,
+    A2A_ERROR_INVALID_VALUE = 1,   /* null pointer, bad enum, non-positive size */
+    A2A_ERROR_DECOMPOSITION = 2,   /* a grid the reference asserts on
+                                      (distribution/a2adistribution.cpp:102-121) */
+    A2A_ERROR_UNSUPPORTED = 3,     /* a transform length with no compiled kernel */
+    A2A_ERROR_NO_PLANS = 4,        /* forward/inverse before make_plans */
+    A2A_ERROR_MISALIGNED = 5,      /* a device buffer not 16-byte aligned */
+    A2A_ERROR_CUDA = 6,            /* a CUDA runtime call failed */
+    A2A_ERROR_OUT_OF_MEMORY = 7,   /* the plan's own tables could not be allocated */
+    A2A_ERROR_TIMEOUT = 8,         /* a bounded device-side wait gave up */
+    A2A_ERROR_NOT_IMPLEMENTED = 9  /* a method not available for this plan */
+} a2a_status;
+
+/* Element type.  The reference compiles `#define fftPrecision double`
+ * (dfft/a2adfft.h:1) with an FP32 variant (dfft/kernels/a2affts.cu:25-35,
+ * src/fft_demo). */
+typedef enum a2a_precision {
+    A2A_C128 = 0, /* complex double, 16 bytes (reference default) */
+    A2A_C64 = 1   /* complex float, 8 bytes */
+} a2a_precision;
+
+/* How the 1D butterflies are computed (no reference counterpart: the
+ * reference always calls cuFFT). */
+typedef enum a2a_method {
+    A2A_METHOD_PLAIN = 0,      /* CUDA-core Stockham mixed radix 2/3/4/8/16 */
+    A2A_METHOD_SPLIT_BF16 = 1, /* radix-16 stages on tensor cores, split bf16 */
+    A2A_METHOD_SPLIT_FP16 = 2  /* radix-16 stages on tensor cores, split fp16 */
+} a2a_method;
+
+/* Public fields of a2aDistribution (distribution/a2adistribution.h:8-17). */
+typedef struct a2a_distribution_desc {
+    int ndims;              /* always 3 */
+    int ng[3];              /* global grid; ng[0]==ng[1]==ng[2]==Ng for cubes */
+    int world_size;         /* number of (virtual) ranks P */
+    int dims[3];            /* MPI_Dims_create(P, 3) */
+    int local_grid_size[3]; /* ng[a] / dims[a] */
+    int64_t nlocal;         /* complexes per rank */
+    int64_t nsends;         /* nlocal / P: complexes per peer per alltoall */
+    int block_size;         /* the reference's CUDA block size argument */
+    int precision;          /* a2a_precision */
+    size_t element_bytes;   /* 16 (C128) or 8 (C64) */
+    size_t buffer_bytes;    /* world_size * nlocal * element_bytes */
+} a2a_distribution_desc;
+
+typedef struct a2a_distribution a2a_distribution; /* a2aDistribution */
+typedef struct a2a_dfft a2a_dfft;                 /* a2adfft */
+
+/* ---- a2aDistribution ---------------------------------------------------- */
+
+/* a2aDistribution(MPI_Comm, int Ng, int blockSize)
+ * (distribution/a2adistribution.cpp:85-154).  The communicator is replaced by
+ * the number of virtual ranks.  Returns A2A_ERROR_DECOMPOSITION where the
+ * reference asserts.  Allocates only small device tables on the current
+ * device. */
+a2a_status a2a_distribution_create(int ng, int world_size, int block_size,
+                                   a2a_precision precision, a2a_distribution** out);
+
+/* Extension with no reference counterpart: an nx x ny x nz box with the same
+ * brick rules applied per axis.  Only the fused transform (a2a_dfft_*)
+ * accepts boxes; the pencil steps and 1D calls need a cube. */
+a2a_status a2a_distribution_create_box(int nx, int ny, int nz, int world_size, int block_size,
+                                       a2a_precision precision, a2a_distribution** out);
+
+a2a_status a2a_distribution_describe(const a2a_distribution* dist, a2a_distribution_desc* out);
+
+/* rank2coords + get_local_grid_start (a2adistribution.cpp:55-83). */
+a2a_status a2a_rank_coords(const a2a_distribution* dist, int rank, int coords[3], int local_start[3]);
+
+/* Stream used by the calls below that take no stream (NULL = default). */
+a2a_status a2a_distribution_set_stream(a2a_distribution* dist, void* cuda_stream);
+
+/* The six transpose steps of a2aDistribution (a2adistribution.cpp:156-256),
+ * over all virtual ranks at once.  On return BOTH buffers hold what the
+ * reference leaves in them (the alltoall becomes a rank-major chunk
+ * permutation in device memory).  One deliberate difference: the Y return
+ * packs with the true inverse of the Y unpack; the reference's
+ * d_y_pencils_to_y_a2a (distribution/kernels/a2apencils.cu:189-208) is not a
+ * permutation unless dims[1]==2 or dims[0]==1, and the two agree wherever it
+ * is. */
+a2a_status a2a_get_z_pencils(a2a_distribution* dist, void** d_buff1, void** d_buff2);    /* :156-170 */
+a2a_status a2a_return_z_pencils(a2a_distribution* dist, void** d_buff1, void** d_buff2); /* :172-186 */
+a2a_status a2a_get_x_pencils(a2a_distribution* dist, void** d_buff1, void** d_buff2);    /* :188-204 */
+a2a_status a2a_return_x_pencils(a2a_distribution* dist, void** d_buff1, void** d_buff2); /* :206-220 */
+a2a_status a2a_get_y_pencils(a2a_distribution* dist, void** d_buff1, void** d_buff2);    /* :222-238 */
+a2a_status a2a_return_y_pencils(a2a_distribution* dist, void** d_buff1, void** d_buff2); /* :240-256 */
+
+/* a2aDistribution::finalize (a2adistribution.cpp:258-265); also frees the
+ * object.  NULL is accepted. */
+a2a_status a2a_distribution_finalize(a2a_distribution* dist);
+
+/* ---- 1D kernels (dfft/kernels/kernels.h:5-11) --------------------------- */
+
+/* forward_1d_fft / inverse_1d_fft (dfft/kernels/a2affts.cu:7-76): in place,
+ * unnormalised, every contiguous length-Ng line of the buffer (the pencils a
+ * get_*_pencils step produced). */
+a2a_status a2a_forward_1d_fft(a2a_distribution* dist, void** d_data);
+a2a_status a2a_inverse_1d_fft(a2a_distribution* dist, void** d_data);
+
+/* launch_scale_fft (a2affts.cu:78-92, 108-116): out = data / Ng^3. */
+a2a_status a2a_scale_fft(a2a_distribution* dist, void** d_out, void** d_data);
+/* launch_fast_copy_fft (a2affts.cu:94-106, 118-125): out = data. */
+a2a_status a2a_fast_copy_fft(a2a_distribution* dist, void** d_out, void** d_data);
+
+/* ---- a2adfft ------------------------------------------------------------ */
+
+/* a2adfft(a2aDistribution&) (dfft/a2adfft.cpp:7-16).  The distribution must
+ * outlive the dfft object. */
+a2a_status a2a_dfft_create(a2a_distribution* dist, a2a_dfft** out);
+
+/* Selects the butterfly method (default A2A_METHOD_PLAIN); call before
+ * make_plans.  The split tensor-core methods need A2A_C64. */
+a2a_status a2a_dfft_set_method(a2a_dfft* dfft, a2a_method method);
+
+/* a2adfft::make_plans(fftPrecision** d_scratch) (dfft/a2adfft.cpp:18-24).
+ * The scratch buffer is borrowed as in the reference (same size as a data
+ * buffer; NULL is accepted because the fused transform runs in place).
+ * Kernel choice and twiddle tables (FP64-generated) are fixed here. */
+a2a_status a2a_dfft_make_plans(a2a_dfft* dfft, void** d_scratch);
+
+/* a2adfft::forward / inverse (dfft/a2adfft.cpp:26-158): in place on
+ * d_data[0], rank-major bricks in, rank-major bricks out, natural frequency
+ * order, forward unnormalised, inverse scaled by 1/(nx*ny*nz).  Implemented
+ * as three fused axis passes (each gathers its pencils straight from the
+ * bricks, transforms them and scatters them back) instead of the reference's
+ * 19 array passes; the scratch buffer is not touched. */
+a2a_status a2a_dfft_forward(a2a_dfft* dfft, void** d_data);
+a2a_status a2a_dfft_inverse(a2a_dfft* dfft, void** d_data);
+a2a_status a2a_dfft_backward(a2a_dfft* dfft, void** d_data); /* alias of inverse */
+a2a_status a2a_dfft_forward_async(a2a_dfft* dfft, void** d_data, void* cuda_stream);
+a2a_status a2a_dfft_inverse_async(a2a_dfft* dfft, void** d_data, void* cuda_stream);
+
+/* One of the three fused passes of a transform, enqueued on `cuda_stream`
+ * (for profiling and for overlapping work between passes): pass 0 = Z,
+ * 1 = X, 2 = Y; forward then is passes 0,1,2 with inverse=0, and the inverse
+ * is passes 0,1,2 with inverse=1 (pass 2 applies the 1/(nx*ny*nz) scale).
+ * No reference counterpart: the reference's forward is not divisible. */
+a2a_status a2a_dfft_execute_pass_async(a2a_dfft* dfft, void** d_data, int pass, int inverse, void* cuda_stream);
+
+/* Number of kernel launches one forward (or inverse) enqueues. */
+a2a_status a2a_dfft_launches_per_transform(const a2a_dfft* dfft, int* out);
+
+a2a_status a2a_dfft_destroy(a2a_dfft* dfft);
+
+/* ---- misc --------------------------------------------------------------- */
+
+const char* a2a_status_string(a2a_status status);
+/* Detail of the last error raised on the calling thread ("" if none). */
+const char* a2a_last_error(void);
+int a2a_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* A2AFFT_B200_H */
