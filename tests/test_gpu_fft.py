@@ -47,8 +47,11 @@ def test_forward_inverse_vs_fp64_oracle(pkg, oracle, cuda, P, ng, prec):
     ei = oracle.rel_l2(inv, g)
     assert ef <= TOL[prec], f"forward rel L2 {ef:.3e}"
     assert ei <= TOL[prec], f"round trip rel L2 {ei:.3e}"
-    # the reference's own acceptance test, on the same data
-    assert np.allclose(np.fft.fftn(g.astype(np.complex128)), fwd, rtol=1e-5, atol=1e-8 * max(1.0, np.abs(ref).max()))
+    if prec == "c128":
+        # the reference's own acceptance test (stitch.py:89, numpy's default
+        # rtol/atol), which its FP64 build is held to
+        assert np.allclose(np.fft.fftn(g), fwd)
+        assert np.allclose(g, inv)
 
 
 @pytest.mark.parametrize("ng,P", [(256, 16), (512, 4), (1024, 4), (768, 4), (384, 4)])
