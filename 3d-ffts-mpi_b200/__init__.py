@@ -219,9 +219,30 @@ class a2adfft:
         call("a2a_dfft_set_method", self._h, _METHODS[method])
         self.plans_made = 0
 
+    def set_autotune(self, enable: bool) -> None:
+        call("a2a_dfft_set_autotune", self._h, int(bool(enable)))
+
+    def variant_count(self, pass_index: int) -> int:
+        n = ctypes.c_int()
+        call("a2a_dfft_variant_count", self._h, int(pass_index), ctypes.byref(n))
+        return n.value
+
+    def select_variant(self, pass_index: int, variant: int) -> None:
+        """Force launch variant `variant` of pass 0 (Z), 1 (X) or 2 (Y)."""
+        call("a2a_dfft_select_variant", self._h, int(pass_index), int(variant))
+
+    def plan_report(self) -> str:
+        """Every launch variant of each pass, its make_plans timing and the
+        chosen one."""
+        buf = ctypes.create_string_buffer(1 << 16)
+        call("a2a_dfft_plan_report", self._h, buf, len(buf))
+        return buf.value.decode()
+
     def make_plans(self, d_scratch=None) -> None:
-        """``a2adfft::make_plans`` (``a2adfft.cpp:18-24``); the scratch buffer
-        is optional because the fused transform runs in place."""
+        """``a2adfft::make_plans`` (``a2adfft.cpp:18-24``).  The scratch
+        buffer is optional because the fused transform runs in place; when it
+        is given, every launch variant of each pass is timed on it (its
+        contents are clobbered) and the fastest is kept."""
         self.d_scratch = d_scratch
         call("a2a_dfft_make_plans", self._h, None if d_scratch is None else self.distribution._buf(d_scratch))
         self.plans_made = 1

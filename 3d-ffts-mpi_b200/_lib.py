@@ -73,6 +73,10 @@ SIGNATURES = {
     "a2a_dfft_create": [_P, ctypes.POINTER(_P)],
     "a2a_dfft_set_method": [_P, _I],
     "a2a_dfft_make_plans": [_P, _PP],
+    "a2a_dfft_set_autotune": [_P, _I],
+    "a2a_dfft_variant_count": [_P, _I, ctypes.POINTER(_I)],
+    "a2a_dfft_select_variant": [_P, _I, _I],
+    "a2a_dfft_plan_report": [_P, ctypes.c_char_p, ctypes.c_size_t],
     "a2a_dfft_forward": [_P, _PP],
     "a2a_dfft_inverse": [_P, _PP],
     "a2a_dfft_backward": [_P, _PP],

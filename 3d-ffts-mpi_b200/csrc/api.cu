@@ -26,6 +26,7 @@ struct a2a_dfft {
     a2a_distribution* dist = nullptr;
     void* scratch = nullptr;
     bool plans_made = false;
+    bool autotune = true;
     a2a_method method = A2A_METHOD_PLAIN;
 };
 
@@ -77,9 +78,59 @@ void dims_create(int n, int dims[3]) {
     for (int k = 0; k < 3; ++k) dims[k] = d[k];
 }
 
-bool find_kernel(a2a_precision prec, int n, int mode, bool inv, PassKernel* k) {
-    return prec == A2A_C128 ? a2a::find_pass_kernel_f64(n, mode, inv, k)
-                            : a2a::find_pass_kernel_f32(n, mode, inv, k);
+int find_kernels(a2a_precision prec, int n, int mode, bool inv, PassKernel* k, int max) {
+    return prec == A2A_C128 ? a2a::find_pass_kernels_f64(n, mode, inv, k, max)
+                            : a2a::find_pass_kernels_f32(n, mode, inv, k, max);
+}
+
+// Geometry of one slot: transform axis table, outer/inner batch tables.
+struct SlotGeom {
+    const uint32_t* offA;
+    const uint32_t* offU;
+    const uint32_t* offV;
+    const void* tw;
+    int n, NU, NV, mode;
+    const std::vector<uint32_t>* hA;
+    const std::vector<uint32_t>* hU;
+    const std::vector<uint32_t>* hV;
+};
+
+SlotGeom slot_geom(const Dist& d, int slot) {
+    switch (slot) {
+        case a2a::SLOT_Z:  // lines (x, y), element z
+            return {d.off[2], d.off[0], d.off[1], d.tw[2], d.ng[2], d.ng[0], d.ng[1], a2a::MODE_LINE,
+                    &d.h_off[2], &d.h_off[0], &d.h_off[1]};
+        case a2a::SLOT_X:  // lines (y, z), element x
+            return {d.off[0], d.off[1], d.off[2], d.tw[0], d.ng[0], d.ng[1], d.ng[2], a2a::MODE_BATCH,
+                    &d.h_off[0], &d.h_off[1], &d.h_off[2]};
+        case a2a::SLOT_Y:  // lines (x, z), element y
+            return {d.off[1], d.off[0], d.off[2], d.tw[1], d.ng[1], d.ng[0], d.ng[2], a2a::MODE_BATCH,
+                    &d.h_off[1], &d.h_off[0], &d.h_off[2]};
+        default:  // contiguous length-Ng lines of a pencil buffer (cubes)
+            return {d.iota, d.pen_u, d.pen_v, d.tw[0], d.ng[0], d.ng[0], d.ng[0], a2a::MODE_LINE, nullptr, nullptr,
+                    nullptr};
+    }
+}
+
+// Does variant k fit the slot's geometry?  Every kernel needs whole tiles; the
+// pipelined BATCH kernel also moves each tile row as 16-byte units, so every
+// tile's lines must be contiguous and 16-byte aligned.
+bool variant_fits(const Dist& d, const SlotGeom& g, const PassKernel& k) {
+    if (g.NV % k.lines) return false;
+    if (k.kind != a2a::KIND_PIPE || g.mode != a2a::MODE_BATCH) return true;
+    if (!g.hA) return false;
+    const size_t epu = 16 / d.elem_bytes;
+    if ((k.lines * d.elem_bytes) % 16) return false;
+    for (int v0 = 0; v0 < g.NV; v0 += k.lines) {
+        for (int b = 1; b < k.lines; ++b)
+            if ((*g.hV)[v0 + b] != (*g.hV)[v0] + (uint32_t)b) return false;
+        if ((*g.hV)[v0] % epu) return false;
+    }
+    for (uint32_t o : *g.hA)
+        if (o % epu) return false;
+    for (uint32_t o : *g.hU)
+        if (o % epu) return false;
+    return true;
 }
 
 // Stage twiddles W_{Ns R}^{r m} (forward sign), laid out as RadixPlan::twoff,
@@ -117,8 +168,9 @@ a2a_status finish(const Dist& d, cudaStream_t st, bool sync) {
 }
 
 template <typename T>
-cudaError_t launch_pass_t(const PassKernel& k, const void* src, void* dst, const uint32_t* offA, const uint32_t* offU,
-                          const uint32_t* offV, const void* tw, int NU, int NV, double scale, cudaStream_t st) {
+cudaError_t launch_pass_t(const PassKernel& k, unsigned grid, const void* src, void* dst, const uint32_t* offA,
+                          const uint32_t* offU, const uint32_t* offV, const void* tw, int NU, int NV, double scale,
+                          cudaStream_t st) {
     a2a::PassArgs<T> a;
     a.src = static_cast<const a2a::cx<T>*>(src);
     a.dst = static_cast<a2a::cx<T>*>(dst);
@@ -130,15 +182,23 @@ cudaError_t launch_pass_t(const PassKernel& k, const void* src, void* dst, const
     a.NV = NV;
     a.scale = T(scale);
     void* args[] = {&a};
-    const unsigned grid = unsigned((uint64_t)NU * (NV / k.lines));
     return cudaLaunchKernel(k.fn, dim3(grid), dim3(k.threads), args, k.smem, st);
 }
 
-cudaError_t launch_pass(const Dist& d, const PassKernel& k, const void* src, void* dst, const uint32_t* offA,
-                        const uint32_t* offU, const uint32_t* offV, const void* tw, int NU, int NV, double scale,
-                        cudaStream_t st) {
-    if (d.prec == A2A_C128) return launch_pass_t<double>(k, src, dst, offA, offU, offV, tw, NU, NV, scale, st);
-    return launch_pass_t<float>(k, src, dst, offA, offU, offV, tw, NU, NV, scale, st);
+// Launch candidate `c` of a slot on buffer p (in place).
+cudaError_t launch_slot(const Dist& d, int slot, bool inv, int c, void* p, double scale, cudaStream_t st) {
+    const a2a::PassSlot& ps = d.slot[slot][inv ? 1 : 0];
+    const PassKernel& k = ps.cand[c];
+    const SlotGeom g = slot_geom(d, slot);
+    const uint64_t tiles = (uint64_t)g.NU * (g.NV / k.lines);
+    uint64_t grid = tiles;
+    if (k.kind == a2a::KIND_PIPE) {
+        const uint64_t resident = (uint64_t)std::max(ps.occ[c], 1) * d.sms;
+        grid = std::min(tiles, resident);
+    }
+    if (d.prec == A2A_C128)
+        return launch_pass_t<double>(k, unsigned(grid), p, p, g.offA, g.offU, g.offV, g.tw, g.NU, g.NV, scale, st);
+    return launch_pass_t<float>(k, unsigned(grid), p, p, g.offA, g.offU, g.offV, g.tw, g.NU, g.NV, scale, st);
 }
 
 a2a_status setup_distribution(Dist& d, int nx, int ny, int nz, int P, int block_size, a2a_precision prec) {
@@ -175,20 +235,6 @@ a2a_status setup_distribution(Dist& d, int nx, int ny, int nz, int P, int block_
     A2A_CUDA(cudaGetDevice(&d.device), "cudaGetDevice");
     A2A_CUDA(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, d.device), "cudaDeviceGetAttribute");
 
-    // kernels and twiddles per axis
-    for (int a = 0; a < 3; ++a)
-        for (int inv = 0; inv < 2; ++inv) {
-            if (!find_kernel(prec, d.ng[a], a2a::MODE_LINE, inv, &d.kline[a][inv]) ||
-                !find_kernel(prec, d.ng[a], a2a::MODE_BATCH, inv, &d.kbatch[a][inv]))
-                return fail(A2A_ERROR_UNSUPPORTED,
-                            "no compiled transform of length %d (supported: 4 8 12 16 24 32 48 64 96 128 192 256 "
-                            "384 512 768 1024)",
-                            d.ng[a]);
-            for (const PassKernel* k : {&d.kline[a][inv], &d.kbatch[a][inv]})
-                A2A_CUDA(cudaFuncSetAttribute(k->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k->smem),
-                         "cudaFuncSetAttribute");
-        }
-
     // offset tables: brick offsets per axis (global (x,y,z) lives at
     // off[0][x] + off[1][y] + off[2][z]), identity, pencil-buffer line bases
     const int maxn = std::max(nx, std::max(ny, nz));
@@ -215,18 +261,50 @@ a2a_status setup_distribution(Dist& d, int nx, int ny, int nz, int P, int block_
     d.pen_u = d.d_tables + pos[4];
     d.pen_v = d.d_tables + pos[5];
 
+    for (int a = 0; a < 3; ++a) d.h_off[a].assign(h.begin() + pos[a], h.begin() + pos[a + 1]);
+
+    // pass kernels: every compiled variant per slot, which fit, occupancy
+    for (int sl = 0; sl < a2a::NSLOTS; ++sl) {
+        if (sl == a2a::SLOT_LINES && !d.cube) continue;
+        const int axis = sl == a2a::SLOT_Z ? 2 : sl == a2a::SLOT_X ? 0 : sl == a2a::SLOT_Y ? 1 : 0;
+        const int mode = sl == a2a::SLOT_X || sl == a2a::SLOT_Y ? a2a::MODE_BATCH : a2a::MODE_LINE;
+        for (int inv = 0; inv < 2; ++inv) {
+            a2a::PassSlot& ps = d.slot[sl][inv];
+            const int cnt = find_kernels(prec, d.ng[axis], mode, inv, ps.cand, a2a::kMaxVariants);
+            if (cnt == 0)
+                return fail(A2A_ERROR_UNSUPPORTED,
+                            "no compiled transform of length %d (supported: 4 8 12 16 24 32 48 64 96 128 192 256 "
+                            "384 512 768 1024)",
+                            d.ng[axis]);
+            ps.ncand = std::min(cnt, a2a::kMaxVariants);
+            ps.chosen = -1;
+            for (int c = 0; c < ps.ncand; ++c) {
+                const PassKernel& k = ps.cand[c];
+                A2A_CUDA(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem),
+                         "cudaFuncSetAttribute");
+                A2A_CUDA(cudaFuncSetAttribute(k.fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                              (int)cudaSharedmemCarveoutMaxShared),
+                         "cudaFuncSetAttribute");
+                A2A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ps.occ[c], k.fn, k.threads, k.smem),
+                         "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+            }
+        }
+    }
+
     std::vector<long double> re, im;
     size_t twpos[3], twtotal = 0;
     for (int a = 0; a < 3; ++a) {
         twpos[a] = twtotal;
-        twtotal += (size_t)d.kline[a][0].twtotal;
+        const int sl = a == 2 ? a2a::SLOT_Z : a == 0 ? a2a::SLOT_X : a2a::SLOT_Y;
+        twtotal += (size_t)d.slot[sl][0].cand[0].twtotal;
     }
     if (twtotal == 0) twtotal = 1;
     A2A_CUDA(cudaMalloc(&d.d_tw, twtotal * d.elem_bytes), "cudaMalloc(twiddles)");
     std::vector<double> hd;
     std::vector<float> hf;
     for (int a = 0; a < 3; ++a) {
-        gen_twiddles(d.kline[a][0], re, im);
+        const int sl = a == 2 ? a2a::SLOT_Z : a == 0 ? a2a::SLOT_X : a2a::SLOT_Y;
+        gen_twiddles(d.slot[sl][0].cand[0], re, im);
         for (size_t i = 0; i < re.size(); ++i) {
             hd.push_back((double)re[i]);
             hd.push_back((double)im[i]);
@@ -241,6 +319,20 @@ a2a_status setup_distribution(Dist& d, int nx, int ny, int nz, int P, int block_
             A2A_CUDA(cudaMemcpy(d.d_tw, hf.data(), hf.size() * sizeof(float), cudaMemcpyHostToDevice), "cudaMemcpy");
     }
     for (int a = 0; a < 3; ++a) d.tw[a] = static_cast<const char*>(d.d_tw) + twpos[a] * d.elem_bytes;
+
+    // default choice: the first variant that fits each slot's geometry
+    for (int sl = 0; sl < a2a::NSLOTS; ++sl) {
+        if (sl == a2a::SLOT_LINES && !d.cube) continue;
+        const SlotGeom g = slot_geom(d, sl);
+        for (int inv = 0; inv < 2; ++inv) {
+            a2a::PassSlot& ps = d.slot[sl][inv];
+            for (int c = 0; c < ps.ncand; ++c) {
+                ps.fits[c] = ps.occ[c] > 0 && variant_fits(d, g, ps.cand[c]);
+                if (ps.fits[c] && ps.chosen < 0) ps.chosen = c;
+            }
+            if (ps.chosen < 0) ps.chosen = 0;  // reported by make_plans / the 1D calls
+        }
+    }
     return A2A_SUCCESS;
 }
 
@@ -278,10 +370,10 @@ a2a_status lines_1d(a2a_distribution* h, void** data, bool inv) {
     a2a_status s;
     if ((s = need_cube(d, "1D pencil transforms")) != A2A_SUCCESS) return s;
     if ((s = check_buf(data, "d_data")) != A2A_SUCCESS) return s;
-    const int n = d.ng[0];
-    A2A_CUDA(launch_pass(d, d.kline[0][inv], data[0], data[0], d.iota, d.pen_u, d.pen_v, d.tw[0], n, n, 1.0,
-                         d.stream),
-             "1D pass launch");
+    const a2a::PassSlot& ps = d.slot[a2a::SLOT_LINES][inv ? 1 : 0];
+    if (!ps.fits[ps.chosen])
+        return fail(A2A_ERROR_UNSUPPORTED, "no compiled 1D kernel fits %d lines of length %d", d.ng[0], d.ng[0]);
+    A2A_CUDA(launch_slot(d, a2a::SLOT_LINES, inv, ps.chosen, data[0], 1.0, d.stream), "1D pass launch");
     return finish(d, d.stream, true);
 }
 
@@ -289,20 +381,10 @@ a2a_status lines_1d(a2a_distribution* h, void** data, bool inv) {
 // pass's gather/scatter addresses come from the brick offset tables, i.e. the
 // alltoall + unpack (and pack + alltoall) composites of the reference steps.
 cudaError_t run_pass(const Dist& d, int pass, bool inv, void* p, cudaStream_t st) {
-    const int i = inv ? 1 : 0;
-    switch (pass) {
-        case 0:  // Z pencils: lines (x, y), element z
-            return launch_pass(d, d.kline[2][i], p, p, d.off[2], d.off[0], d.off[1], d.tw[2], d.ng[0], d.ng[1], 1.0,
-                               st);
-        case 1:  // X pencils: lines (y, z), element x
-            return launch_pass(d, d.kbatch[0][i], p, p, d.off[0], d.off[1], d.off[2], d.tw[0], d.ng[1], d.ng[2],
-                               1.0, st);
-        default: {  // Y pencils: lines (x, z), element y; carries the inverse's 1/(nx ny nz)
-            const double scale = inv ? 1.0 / ((double)d.ng[0] * d.ng[1] * d.ng[2]) : 1.0;
-            return launch_pass(d, d.kbatch[1][i], p, p, d.off[1], d.off[0], d.off[2], d.tw[1], d.ng[0], d.ng[2],
-                               scale, st);
-        }
-    }
+    // pass 0 = Z (lines (x, y)), 1 = X (lines (y, z)), 2 = Y (lines (x, z));
+    // the Y pass carries the inverse's 1/(nx ny nz)
+    const double scale = (inv && pass == 2) ? 1.0 / ((double)d.ng[0] * d.ng[1] * d.ng[2]) : 1.0;
+    return launch_slot(d, pass, inv, d.slot[pass][inv ? 1 : 0].chosen, p, scale, st);
 }
 
 a2a_status check_dfft(a2a_dfft* f, void** data) {
@@ -490,20 +572,111 @@ a2a_status a2a_dfft_set_method(a2a_dfft* f, a2a_method m) {
 
 a2a_status a2a_dfft_make_plans(a2a_dfft* f, void** d_scratch) {
     if (!f) return fail(A2A_ERROR_INVALID_VALUE, "dfft is NULL");
-    const Dist& d = f->dist->d;
+    Dist& d = f->dist->d;
     f->scratch = d_scratch ? d_scratch[0] : nullptr;
-    // every pass's inner batch extent must split into whole tiles
-    const struct {
-        const PassKernel* k;
-        int nv;
-        const char* name;
-    } passes[3] = {{&d.kline[2][0], d.ng[1], "Z"}, {&d.kbatch[0][0], d.ng[2], "X"}, {&d.kbatch[1][0], d.ng[2], "Y"}};
-    for (const auto& p : passes)
-        if (p.nv % p.k->lines)
-            return fail(A2A_ERROR_UNSUPPORTED, "%s pass: %d lines are not a multiple of the %d-line tile", p.name,
-                        p.nv, p.k->lines);
+    const char* names[3] = {"Z", "X", "Y"};
+    for (int p = 0; p < 3; ++p)
+        for (int inv = 0; inv < 2; ++inv) {
+            const a2a::PassSlot& ps = d.slot[p][inv];
+            if (!ps.fits[ps.chosen])
+                return fail(A2A_ERROR_UNSUPPORTED, "%s pass: no compiled tile of length %d fits %d lines", names[p],
+                            ps.cand[0].n, slot_geom(d, p).NV);
+        }
+    if (f->scratch && f->autotune) {
+        if (reinterpret_cast<uintptr_t>(f->scratch) % 16)
+            return fail(A2A_ERROR_MISALIGNED, "d_scratch[0] is not 16-byte aligned");
+        // time every fitting variant of each pass on the scratch buffer (its
+        // contents are clobbered, as the reference allows) and keep the fastest
+        cudaStream_t st = d.stream;
+        cudaEvent_t e0, e1;
+        A2A_CUDA(cudaEventCreate(&e0), "cudaEventCreate");
+        A2A_CUDA(cudaEventCreate(&e1), "cudaEventCreate");
+        a2a_status status = A2A_SUCCESS;
+        for (int p = 0; p < 3 && status == A2A_SUCCESS; ++p) {
+            a2a::PassSlot& ps = d.slot[p][0];
+            int best = ps.chosen;
+            float best_ms = 1e30f;
+            for (int c = 0; c < ps.ncand && status == A2A_SUCCESS; ++c) {
+                ps.tuned_ms[c] = 0.f;
+                if (!ps.fits[c]) continue;
+                cudaError_t e = launch_slot(d, p, false, c, f->scratch, 1.0, st);  // warm-up
+                float ms = 1e30f;
+                for (int rep = 0; rep < 3 && e == cudaSuccess; ++rep) {
+                    e = cudaEventRecord(e0, st);
+                    if (e == cudaSuccess) e = launch_slot(d, p, false, c, f->scratch, 1.0, st);
+                    if (e == cudaSuccess) e = cudaEventRecord(e1, st);
+                    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+                    float t = 0.f;
+                    if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+                    if (e == cudaSuccess) ms = std::min(ms, t);
+                }
+                if (e != cudaSuccess) {
+                    status = cuda_fail(e, "autotune launch");
+                    break;
+                }
+                ps.tuned_ms[c] = ms;
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = c;
+                }
+            }
+            ps.chosen = best;
+            d.slot[p][1].chosen = best;  // the inverse kernels share the variant list
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (status != A2A_SUCCESS) return status;
+    }
     f->plans_made = true;
     return A2A_SUCCESS;
+}
+
+a2a_status a2a_dfft_variant_count(const a2a_dfft* f, int pass, int* count) {
+    if (!f || !count) return fail(A2A_ERROR_INVALID_VALUE, "NULL argument");
+    if (pass < 0 || pass > 2) return fail(A2A_ERROR_INVALID_VALUE, "pass must be 0 (Z), 1 (X) or 2 (Y)");
+    *count = f->dist->d.slot[pass][0].ncand;
+    return A2A_SUCCESS;
+}
+
+a2a_status a2a_dfft_select_variant(a2a_dfft* f, int pass, int variant) {
+    if (!f) return fail(A2A_ERROR_INVALID_VALUE, "dfft is NULL");
+    if (pass < 0 || pass > 2) return fail(A2A_ERROR_INVALID_VALUE, "pass must be 0 (Z), 1 (X) or 2 (Y)");
+    Dist& d = f->dist->d;
+    if (variant < 0 || variant >= d.slot[pass][0].ncand)
+        return fail(A2A_ERROR_INVALID_VALUE, "variant %d outside [0, %d)", variant, d.slot[pass][0].ncand);
+    if (!d.slot[pass][0].fits[variant] || !d.slot[pass][1].fits[variant])
+        return fail(A2A_ERROR_UNSUPPORTED, "variant %d does not fit this pass's geometry", variant);
+    d.slot[pass][0].chosen = variant;
+    d.slot[pass][1].chosen = variant;
+    return A2A_SUCCESS;
+}
+
+a2a_status a2a_dfft_set_autotune(a2a_dfft* f, int enable) {
+    if (!f) return fail(A2A_ERROR_INVALID_VALUE, "dfft is NULL");
+    f->autotune = enable != 0;
+    return A2A_SUCCESS;
+}
+
+a2a_status a2a_dfft_plan_report(const a2a_dfft* f, char* buf, size_t len) {
+    if (!f || !buf || len == 0) return fail(A2A_ERROR_INVALID_VALUE, "NULL argument");
+    const Dist& d = f->dist->d;
+    std::string out;
+    const char* names[3] = {"Z", "X", "Y"};
+    for (int p = 0; p < 3; ++p) {
+        const a2a::PassSlot& ps = d.slot[p][0];
+        for (int c = 0; c < ps.ncand; ++c) {
+            const PassKernel& k = ps.cand[c];
+            char line[256];
+            snprintf(line, sizeof line,
+                     "%s pass n=%d %s lines=%d threads=%d smem=%zu occ=%d radix=%d,%d,%d,%d fits=%d tuned_ms=%.4f%s\n",
+                     names[p], k.n, k.kind == a2a::KIND_PIPE ? "pipe" : "direct", k.lines, k.threads, k.smem,
+                     ps.occ[c], k.radix[0], k.radix[1], k.radix[2], k.radix[3], (int)ps.fits[c], ps.tuned_ms[c],
+                     c == ps.chosen ? " <- chosen" : "");
+            out += line;
+        }
+    }
+    snprintf(buf, len, "%s", out.c_str());
+    return out.size() < len ? A2A_SUCCESS : fail(A2A_ERROR_INVALID_VALUE, "report truncated (%zu bytes)", out.size());
 }
 
 a2a_status a2a_dfft_forward(a2a_dfft* f, void** d_data) {

@@ -1,25 +1,19 @@
-// Pass-kernel instantiations for complex double (every compiled N, both access
-// modes, both directions) and their lookup.
+// Pass-kernel instantiations for complex double: every launch variant of every
+// compiled N, both access modes, both directions, and their lookup.
 #include "fft_registry.cuh"
 
 namespace a2a {
 
-bool find_pass_kernel_f64(int n, int mode, bool inverse, PassKernel* out) {
-#define A2A_CASE(N_)                                                                    \
-    case N_:                                                                            \
-        if (mode == MODE_LINE)                                                          \
-            *out = inverse ? make_pass_kernel<double, N_, MODE_LINE, true>()              \
-                           : make_pass_kernel<double, N_, MODE_LINE, false>();            \
-        else                                                                            \
-            *out = inverse ? make_pass_kernel<double, N_, MODE_BATCH, true>()             \
-                           : make_pass_kernel<double, N_, MODE_BATCH, false>();           \
-        return true;
-    switch (n) {
-        A2A_FOR_EACH_N(A2A_CASE)
-        default:
-            return false;
+int find_pass_kernels_f64(int n, int mode, bool inverse, PassKernel* out, int max) {
+    int cnt = 0;
+#define A2A_ADD(T_, N_, KIND_, B_, TH_, MB_)                                  \
+    if (n == N_) {                                                            \
+        if (cnt < max) out[cnt] = make_variant<T_, N_, KIND_, B_, TH_, MB_>(mode, inverse); \
+        ++cnt;                                                                \
     }
-#undef A2A_CASE
+    A2A_VARIANTS_F64(A2A_ADD)
+#undef A2A_ADD
+    return cnt;
 }
 
 }  // namespace a2a

@@ -1,5 +1,5 @@
-// Compiled transform lengths and their launch shapes, and the host-side
-// lookup of a pass kernel for (precision, N, mode, direction).
+// Compiled transform lengths, their radix plans and launch variants, and the
+// host-side lookup of the pass kernels for (precision, N, mode, direction).
 #pragma once
 
 #include <cstddef>
@@ -12,85 +12,144 @@ namespace a2a {
 // Host view of one compiled pass kernel.
 struct PassKernel {
     const void* fn = nullptr;
+    int kind = KIND_DIRECT;
     int n = 0;          // transform length
     int threads = 0;
     int lines = 0;      // B: lines per tile (a pass needs NV % lines == 0)
+    int min_blocks = 1; // __launch_bounds__ minimum blocks per SM
     size_t smem = 0;    // dynamic shared memory bytes
     int nstages = 0;
     int radix[4] = {0, 0, 0, 0};
     int twtotal = 0;    // complex entries of the twiddle table
 };
 
-// Launch shape per (element type, N): radix plan, lines per tile, threads.
-// Tiles are ~64 KB so two or three CTAs share an SM; FP64 holds half the
-// elements per thread of FP32 to stay within registers.
-template <typename T, int N> struct PassCfg;
-
-#define A2A_PASS_CFG(T_, N_, B_, TH_, ...)                                  \
-    template <> struct PassCfg<T_, N_> {                                    \
+// Radix plan per (element type, N): radix 8/16 stages where they divide,
+// one radix-2/3/4 stage for the rest.
+template <typename T, int N> struct PassPlan;
+#define A2A_PLAN(T_, N_, ...)                                               \
+    template <> struct PassPlan<T_, N_> {                                   \
         using Plan = RadixPlan<__VA_ARGS__>;                                \
-        static constexpr int B = B_;                                        \
-        static constexpr int THREADS = TH_;                                 \
         static_assert(Plan::N == N_, "radix plan does not multiply to N");  \
     };
 
 // clang-format off
-A2A_PASS_CFG(float,    4,  4,  32, 4)
-A2A_PASS_CFG(float,    8,  8,  32, 8)
-A2A_PASS_CFG(float,   12,  4,  32, 3, 4)
-A2A_PASS_CFG(float,   16, 16,  32, 16)
-A2A_PASS_CFG(float,   24,  8,  32, 3, 8)
-A2A_PASS_CFG(float,   32, 32, 128, 4, 8)
-A2A_PASS_CFG(float,   48, 16,  64, 3, 16)
-A2A_PASS_CFG(float,   64, 32, 128, 8, 8)
-A2A_PASS_CFG(float,   96, 32, 128, 3, 4, 8)
-A2A_PASS_CFG(float,  128, 32, 256, 8, 16)
-A2A_PASS_CFG(float,  192, 32, 256, 3, 4, 16)
-A2A_PASS_CFG(float,  256, 32, 256, 16, 16)
-A2A_PASS_CFG(float,  384, 16, 256, 3, 8, 16)
-A2A_PASS_CFG(float,  512, 16, 256, 8, 8, 8)
-A2A_PASS_CFG(float,  768,  8, 256, 3, 16, 16)
-A2A_PASS_CFG(float, 1024,  8, 256, 4, 16, 16)
+#define A2A_PLANS(T_)                 \
+    A2A_PLAN(T_,    4, 4)             \
+    A2A_PLAN(T_,    8, 8)             \
+    A2A_PLAN(T_,   12, 3, 4)          \
+    A2A_PLAN(T_,   16, 16)            \
+    A2A_PLAN(T_,   24, 3, 8)          \
+    A2A_PLAN(T_,   32, 4, 8)          \
+    A2A_PLAN(T_,   48, 3, 16)         \
+    A2A_PLAN(T_,   64, 8, 8)          \
+    A2A_PLAN(T_,   96, 3, 4, 8)       \
+    A2A_PLAN(T_,  128, 8, 16)         \
+    A2A_PLAN(T_,  192, 3, 4, 16)      \
+    A2A_PLAN(T_,  256, 16, 16)        \
+    A2A_PLAN(T_,  384, 3, 8, 16)      \
+    A2A_PLAN(T_,  512, 8, 8, 8)       \
+    A2A_PLAN(T_,  768, 3, 16, 16)     \
+    A2A_PLAN(T_, 1024, 4, 16, 16)
+A2A_PLANS(float)
+A2A_PLANS(double)
 
-A2A_PASS_CFG(double,    4,  4,  32, 4)
-A2A_PASS_CFG(double,    8,  8,  32, 8)
-A2A_PASS_CFG(double,   12,  4,  32, 3, 4)
-A2A_PASS_CFG(double,   16, 16,  32, 16)
-A2A_PASS_CFG(double,   24,  8,  32, 3, 8)
-A2A_PASS_CFG(double,   32, 16, 128, 4, 8)
-A2A_PASS_CFG(double,   48,  8,  64, 3, 16)
-A2A_PASS_CFG(double,   64, 32, 128, 8, 8)
-A2A_PASS_CFG(double,   96, 16, 128, 3, 4, 8)
-A2A_PASS_CFG(double,  128, 16, 128, 8, 16)
-A2A_PASS_CFG(double,  192, 16, 256, 3, 4, 16)
-A2A_PASS_CFG(double,  256, 16, 256, 16, 16)
-A2A_PASS_CFG(double,  384,  8, 256, 3, 8, 16)
-A2A_PASS_CFG(double,  512,  8, 256, 8, 8, 8)
-A2A_PASS_CFG(double,  768,  8, 384, 3, 16, 16)
-A2A_PASS_CFG(double, 1024,  8, 512, 4, 16, 16)
+// Launch variants X(T, N, KIND, B lines per tile, THREADS, MINB).  The first
+// entry per N is the default; make_plans can time the others on the scratch
+// buffer and keep the fastest (a2a_dfft_make_plans).  DIRECT tiles are about
+// 32-64 KB so two or three CTAs share an SM; PIPE CTAs hold two tiles.
+#define A2A_VARIANTS_F32(X)                         \
+    X(float,    4, KIND_DIRECT,  4,  32, 1)         \
+    X(float,    8, KIND_DIRECT,  8,  32, 1)         \
+    X(float,   12, KIND_DIRECT,  4,  32, 1)         \
+    X(float,   16, KIND_DIRECT, 16,  32, 1)         \
+    X(float,   24, KIND_DIRECT,  8,  32, 1)         \
+    X(float,   32, KIND_DIRECT, 32, 128, 1)         \
+    X(float,   48, KIND_DIRECT, 16,  64, 1)         \
+    X(float,   64, KIND_DIRECT, 32, 128, 1)         \
+    X(float,   64, KIND_PIPE,   32, 128, 4)         \
+    X(float,   96, KIND_DIRECT, 32, 128, 1)         \
+    X(float,   96, KIND_PIPE,   32, 128, 2)         \
+    X(float,  128, KIND_DIRECT, 32, 256, 1)         \
+    X(float,  128, KIND_PIPE,   32, 256, 2)         \
+    X(float,  192, KIND_DIRECT, 32, 256, 1)         \
+    X(float,  192, KIND_PIPE,   16, 256, 2)         \
+    X(float,  256, KIND_DIRECT, 32, 256, 1)         \
+    X(float,  256, KIND_PIPE,   16, 256, 2)         \
+    X(float,  256, KIND_PIPE,   32, 512, 1)         \
+    X(float,  384, KIND_DIRECT, 16, 256, 1)         \
+    X(float,  384, KIND_PIPE,    8, 256, 2)         \
+    X(float,  512, KIND_DIRECT, 16, 256, 2)         \
+    X(float,  512, KIND_PIPE,   16, 512, 1)         \
+    X(float,  512, KIND_PIPE,    8, 256, 2)         \
+    X(float,  512, KIND_DIRECT, 16, 512, 1)         \
+    X(float,  512, KIND_PIPE,   16, 256, 1)         \
+    X(float,  768, KIND_DIRECT,  8, 256, 1)         \
+    X(float,  768, KIND_PIPE,    8, 384, 1)         \
+    X(float, 1024, KIND_DIRECT,  8, 256, 1)         \
+    X(float, 1024, KIND_PIPE,    8, 512, 1)
+
+#define A2A_VARIANTS_F64(X)                         \
+    X(double,    4, KIND_DIRECT,  4,  32, 1)        \
+    X(double,    8, KIND_DIRECT,  8,  32, 1)        \
+    X(double,   12, KIND_DIRECT,  4,  32, 1)        \
+    X(double,   16, KIND_DIRECT, 16,  32, 1)        \
+    X(double,   24, KIND_DIRECT,  8,  32, 1)        \
+    X(double,   32, KIND_DIRECT, 16, 128, 1)        \
+    X(double,   48, KIND_DIRECT,  8,  64, 1)        \
+    X(double,   64, KIND_DIRECT, 32, 128, 1)        \
+    X(double,   64, KIND_PIPE,   16, 128, 2)        \
+    X(double,   96, KIND_DIRECT, 16, 128, 1)        \
+    X(double,   96, KIND_PIPE,   16, 128, 2)        \
+    X(double,  128, KIND_DIRECT, 16, 128, 1)        \
+    X(double,  128, KIND_PIPE,   16, 256, 2)        \
+    X(double,  192, KIND_DIRECT, 16, 256, 1)        \
+    X(double,  192, KIND_PIPE,    8, 256, 2)        \
+    X(double,  256, KIND_DIRECT, 16, 256, 1)        \
+    X(double,  256, KIND_PIPE,    8, 256, 2)        \
+    X(double,  384, KIND_DIRECT,  8, 256, 1)        \
+    X(double,  384, KIND_PIPE,    8, 384, 1)        \
+    X(double,  512, KIND_DIRECT,  8, 256, 1)        \
+    X(double,  512, KIND_PIPE,    8, 512, 1)        \
+    X(double,  768, KIND_DIRECT,  8, 384, 1)        \
+    X(double,  768, KIND_PIPE,    8, 768, 1)        \
+    X(double, 1024, KIND_DIRECT,  8, 512, 1)        \
+    X(double, 1024, KIND_PIPE,    4, 512, 1)
 // clang-format on
 
-#define A2A_FOR_EACH_N(X) \
-    X(4) X(8) X(12) X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512) X(768) X(1024)
-
-template <typename T, int N, int MODE, bool INV> PassKernel make_pass_kernel() {
-    using C = PassCfg<T, N>;
-    using P = typename C::Plan;
+template <typename T, int N, int KIND, int B, int TH, int MB, int MODE, bool INV>
+PassKernel make_pass_kernel() {
+    using P = typename PassPlan<T, N>::Plan;
     PassKernel k;
-    k.fn = reinterpret_cast<const void*>(&fft_pass_kernel<T, P, C::B, C::THREADS, MODE, INV>);
+    if constexpr (KIND == KIND_PIPE)
+        k.fn = reinterpret_cast<const void*>(&fft_pipe_kernel<T, P, B, TH, MODE, INV, MB>);
+    else
+        k.fn = reinterpret_cast<const void*>(&fft_pass_kernel<T, P, B, TH, MODE, INV, MB>);
+    k.kind = KIND;
     k.n = N;
-    k.threads = C::THREADS;
-    k.lines = C::B;
-    k.smem = pass_smem_bytes<T, P, C::B, MODE>();
+    k.threads = TH;
+    k.lines = B;
+    k.min_blocks = MB;
+    k.smem = pass_smem_bytes<T, P, B, MODE, KIND>();
     k.nstages = P::S;
     for (int s = 0; s < P::S; ++s) k.radix[s] = P::r[s];
     k.twtotal = P::twtotal();
     return k;
 }
 
-// Defined in fft_pass_f32.cu / fft_pass_f64.cu.  Returns false when N has no
-// compiled kernel.
-bool find_pass_kernel_f32(int n, int mode, bool inverse, PassKernel* out);
-bool find_pass_kernel_f64(int n, int mode, bool inverse, PassKernel* out);
+template <typename T, int N, int KIND, int B, int TH, int MB>
+PassKernel make_variant(int mode, bool inv) {
+    if (mode == MODE_LINE)
+        return inv ? make_pass_kernel<T, N, KIND, B, TH, MB, MODE_LINE, true>()
+                   : make_pass_kernel<T, N, KIND, B, TH, MB, MODE_LINE, false>();
+    return inv ? make_pass_kernel<T, N, KIND, B, TH, MB, MODE_BATCH, true>()
+               : make_pass_kernel<T, N, KIND, B, TH, MB, MODE_BATCH, false>();
+}
+
+// Defined in fft_pass_f32.cu / fft_pass_f64.cu: fills up to `max` variants of
+// length n (default first) and returns how many exist (0: n not compiled).
+int find_pass_kernels_f32(int n, int mode, bool inverse, PassKernel* out, int max);
+int find_pass_kernels_f64(int n, int mode, bool inverse, PassKernel* out, int max);
+
+constexpr int kMaxVariants = 8;
 
 }  // namespace a2a

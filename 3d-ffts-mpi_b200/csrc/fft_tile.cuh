@@ -224,39 +224,60 @@ template <typename T> struct PassArgs {
     T scale;               // multiplies every stored element
 };
 
-// Line/butterfly index mapping: butterfly q of a stage with Nb = N/R
-// butterflies per line.
-template <int MODE, int B, int NB> __device__ __forceinline__ void bf_map(int q, int& b, int& j) {
-    if constexpr (MODE == MODE_BATCH) {
+// Butterfly q of a stage -> (tile line b, butterfly j), NBL butterflies per
+// line.  BFAST: consecutive q walk across lines (b fastest), conflict-free in
+// shared memory for both layouts; otherwise q walks along a line (j fastest),
+// which coalesces global accesses when a line's elements are contiguous.
+template <bool BFAST, int B, int NBL> __device__ __forceinline__ void bf_map(int q, int& b, int& j) {
+    if constexpr (BFAST) {
         b = q % B;
         j = q / B;
     } else {
-        j = q % NB;
-        b = q / NB;
+        j = q % NBL;
+        b = q / NBL;
     }
 }
 
-// shared-memory slot of element n of tile line b
-template <int MODE, int B, int N> __device__ __forceinline__ int sidx(int b, int n) {
-    if constexpr (MODE == MODE_BATCH) {
-        return n * B + b;
-    } else {
-        return b * (N + N / 32) + n + (n >> 5);
-    }
-}
-
+// Shared-memory layout of one tile.  BATCH: [n][b] (lines fastest).  LINE:
+// line b at b*LS, element n at n + n/32 (one pad slot per 32 elements keeps
+// strided butterfly writes spread over the banks); LS is odd, so lanes that
+// walk across lines hit distinct banks.
 template <int MODE, int B, int N> struct TileGeom {
-    static constexpr int elems = (MODE == MODE_BATCH) ? N * B : B * (N + N / 32);
+    static constexpr int LS = (N + N / 32) | 1;
+    static constexpr int elems = (MODE == MODE_BATCH) ? N * B : B * LS;
+    static __device__ __forceinline__ int idx(int b, int n) {
+        if constexpr (MODE == MODE_BATCH)
+            return n * B + b;
+        else
+            return b * LS + n + (n >> 5);
+    }
 };
 
 // streaming loads/stores: each element is touched once per pass
 template <typename V> __device__ __forceinline__ V ld_stream(const V* p) { return __ldcs(p); }
 template <typename V> __device__ __forceinline__ void st_stream(V* p, V v) { __stcs(p, v); }
 
+// asynchronous global -> shared copies (sm_80+ LDGSTS), one group per tile
+template <int BYTES> __device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    if constexpr (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Stages s >= 1 (and stage 0 of the pipelined kernel): shared -> registers,
+// twiddle, DFT_R, then shared (Stockham position) or, for the last stage,
+// global memory at base_s[b] + offA_s[n].
 template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV, int s>
 __device__ __forceinline__ void run_stage(const PassArgs<T>& a, cx<T>* tile, const cx<T>* tw,
                                           const uint32_t* offA_s, const size_t* base_s, int tid) {
     using V = cx<T>;
+    using G = TileGeom<MODE, B, PLAN::N>;
     constexpr int N = PLAN::N;
     constexpr int R = PLAN::r[s];
     constexpr int NS = PLAN::ns(s);
@@ -265,6 +286,7 @@ __device__ __forceinline__ void run_stage(const PassArgs<T>& a, cx<T>* tile, con
     constexpr int K = (NBT + THREADS - 1) / THREADS;
     constexpr bool EXACT = (NBT % THREADS) == 0;
     constexpr bool LAST = (s == PLAN::S - 1);
+    constexpr bool BFAST = (MODE == MODE_BATCH) || !LAST;
     constexpr int TWO = PLAN::twoff(s);
 
     V x[K][R];
@@ -273,9 +295,9 @@ __device__ __forceinline__ void run_stage(const PassArgs<T>& a, cx<T>* tile, con
         const int q = tid + k * THREADS;
         if (EXACT || q < NBT) {
             int b, j;
-            bf_map<MODE, B, NBL>(q, b, j);
+            bf_map<BFAST, B, NBL>(q, b, j);
 #pragma unroll
-            for (int r = 0; r < R; ++r) x[k][r] = tile[sidx<MODE, B, N>(b, j + r * NBL)];
+            for (int r = 0; r < R; ++r) x[k][r] = tile[G::idx(b, j + r * NBL)];
         }
     }
     __syncthreads();  // the tile is updated in place
@@ -284,10 +306,12 @@ __device__ __forceinline__ void run_stage(const PassArgs<T>& a, cx<T>* tile, con
         const int q = tid + k * THREADS;
         if (EXACT || q < NBT) {
             int b, j;
-            bf_map<MODE, B, NBL>(q, b, j);
+            bf_map<BFAST, B, NBL>(q, b, j);
             const int m = j % NS;
+            if constexpr (s > 0) {
 #pragma unroll
-            for (int r = 1; r < R; ++r) x[k][r] = cmulw<INV>(x[k][r], tw[TWO + (r - 1) * NS + m]);
+                for (int r = 1; r < R; ++r) x[k][r] = cmulw<INV>(x[k][r], tw[TWO + (r - 1) * NS + m]);
+            }
             Dft<R, INV, V>::run(x[k]);
             if constexpr (LAST) {
                 const size_t lb = base_s[b];
@@ -297,7 +321,7 @@ __device__ __forceinline__ void run_stage(const PassArgs<T>& a, cx<T>* tile, con
             } else {
                 const int jd = (j / NS) * NS * R + m;
 #pragma unroll
-                for (int r = 0; r < R; ++r) tile[sidx<MODE, B, N>(b, jd + r * NS)] = x[k][r];
+                for (int r = 0; r < R; ++r) tile[G::idx(b, jd + r * NS)] = x[k][r];
             }
         }
     }
@@ -307,20 +331,29 @@ __device__ __forceinline__ void run_stage(const PassArgs<T>& a, cx<T>* tile, con
     }
 }
 
-template <typename T, class PLAN, int B, int MODE>
-constexpr size_t pass_smem_bytes() {
+enum PassKind : int {
+    KIND_DIRECT = 0,  // one tile per CTA, stage 0 loads global memory into registers
+    KIND_PIPE = 1     // persistent CTAs, next tile prefetched into shared memory
+};
+
+template <typename T, class PLAN, int B, int MODE, int KIND>
+__host__ __device__ constexpr size_t pass_smem_bytes() {
     constexpr int N = PLAN::N;
-    size_t bytes = sizeof(cx<T>) * (size_t)(TileGeom<MODE, B, N>::elems + PLAN::twtotal());
+    constexpr int NBUF = KIND == KIND_PIPE ? 2 : 1;
+    size_t bytes = sizeof(cx<T>) * (size_t)(NBUF * TileGeom<MODE, B, N>::elems + PLAN::twtotal());
     bytes += sizeof(uint32_t) * (size_t)N;
     bytes = (bytes + 15) & ~size_t(15);
-    bytes += sizeof(size_t) * (size_t)B;
+    bytes += sizeof(size_t) * (size_t)(NBUF * B);
     return bytes;
 }
 
-// One CTA = one tile of B lines: lines (u, v0 .. v0+B-1).
-template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV>
-__global__ void __launch_bounds__(THREADS) fft_pass_kernel(const PassArgs<T> a) {
+// KIND_DIRECT: one CTA = one tile of B lines (u, v0 .. v0+B-1).  Stage 0
+// reads global memory straight into registers (j fastest in LINE mode, so
+// the loads coalesce along the line).
+template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) fft_pass_kernel(const PassArgs<T> a) {
     using V = cx<T>;
+    using G = TileGeom<MODE, B, PLAN::N>;
     constexpr int N = PLAN::N;
     constexpr int R0 = PLAN::r[0];
     constexpr int NBL = N / R0;
@@ -328,15 +361,15 @@ __global__ void __launch_bounds__(THREADS) fft_pass_kernel(const PassArgs<T> a) 
     constexpr int K = (NBT + THREADS - 1) / THREADS;
     constexpr bool EXACT = (NBT % THREADS) == 0;
     constexpr int TWN = PLAN::twtotal();
+    constexpr bool BFAST0 = (MODE == MODE_BATCH);
     static_assert(MODE != MODE_BATCH || THREADS % B == 0, "batch mode needs THREADS % B == 0");
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V* tile = reinterpret_cast<V*>(smem_raw);
-    V* tw = tile + TileGeom<MODE, B, N>::elems;
+    V* tw = tile + G::elems;
     uint32_t* offA_s = reinterpret_cast<uint32_t*>(tw + TWN);
     size_t* base_s = reinterpret_cast<size_t*>(
-        smem_raw + ((sizeof(V) * (size_t)(TileGeom<MODE, B, N>::elems + TWN) + sizeof(uint32_t) * N + 15) &
-                    ~size_t(15)));
+        smem_raw + ((sizeof(V) * (size_t)(G::elems + TWN) + sizeof(uint32_t) * N + 15) & ~size_t(15)));
 
     const int tid = threadIdx.x;
     const int tilesV = a.NV / B;
@@ -344,14 +377,13 @@ __global__ void __launch_bounds__(THREADS) fft_pass_kernel(const PassArgs<T> a) 
     const int v0 = (blockIdx.x - u * tilesV) * B;
     const size_t ubase = a.offU[u];
 
-    // stage 0: global -> registers, gather addresses straight from the tables
     V x[K][R0];
 #pragma unroll
     for (int k = 0; k < K; ++k) {
         const int q = tid + k * THREADS;
         if (EXACT || q < NBT) {
             int b, j;
-            bf_map<MODE, B, NBL>(q, b, j);
+            bf_map<BFAST0, B, NBL>(q, b, j);
             const size_t lb = ubase + __ldg(a.offV + v0 + b);
 #pragma unroll
             for (int r = 0; r < R0; ++r) x[k][r] = ld_stream(a.src + lb + __ldg(a.offA + j + r * NBL));
@@ -368,7 +400,7 @@ __global__ void __launch_bounds__(THREADS) fft_pass_kernel(const PassArgs<T> a) 
             const int q = tid + k * THREADS;
             if (EXACT || q < NBT) {
                 int b, j;
-                bf_map<MODE, B, NBL>(q, b, j);
+                bf_map<BFAST0, B, NBL>(q, b, j);
                 Dft<R0, INV, V>::run(x[k]);
                 const size_t lb = ubase + __ldg(a.offV + v0 + b);
 #pragma unroll
@@ -382,15 +414,95 @@ __global__ void __launch_bounds__(THREADS) fft_pass_kernel(const PassArgs<T> a) 
             const int q = tid + k * THREADS;
             if (EXACT || q < NBT) {
                 int b, j;
-                bf_map<MODE, B, NBL>(q, b, j);
+                bf_map<BFAST0, B, NBL>(q, b, j);
                 Dft<R0, INV, V>::run(x[k]);
 #pragma unroll
-                for (int r = 0; r < R0; ++r) tile[sidx<MODE, B, N>(b, j * R0 + r)] = x[k][r];
+                for (int r = 0; r < R0; ++r) tile[G::idx(b, j * R0 + r)] = x[k][r];
             }
         }
         __syncthreads();
         run_stage<T, PLAN, B, THREADS, MODE, INV, 1>(a, tile, tw, offA_s, base_s, tid);
     }
+}
+
+// Issue the asynchronous copies of tile t into `buf` and record its line
+// bases.  BATCH tiles move as rows of B contiguous elements (16-byte units;
+// the host only selects this kernel when every tile's lines are contiguous and
+// 16-byte aligned); LINE tiles move element by element into the padded layout.
+template <typename T, class PLAN, int B, int THREADS, int MODE>
+__device__ __forceinline__ void pipe_issue(const PassArgs<T>& a, int t, int tilesV, cx<T>* buf, size_t* base_s,
+                                           int tid) {
+    using V = cx<T>;
+    using G = TileGeom<MODE, B, PLAN::N>;
+    constexpr int N = PLAN::N;
+    const int u = t / tilesV;
+    const int v0 = (t - u * tilesV) * B;
+    const size_t ubase = __ldg(a.offU + u);
+    for (int b = tid; b < B; b += THREADS) base_s[b] = ubase + __ldg(a.offV + v0 + b);
+    if constexpr (MODE == MODE_BATCH) {
+        constexpr int EPU = 16 / sizeof(V);  // elements per 16-byte unit
+        constexpr int UPR = B / EPU;         // units per tile row
+        static_assert(B % EPU == 0, "tile rows must be whole 16-byte units");
+        const V* row0 = a.src + ubase + __ldg(a.offV + v0);
+#pragma unroll 4
+        for (int w = tid; w < N * UPR; w += THREADS) {
+            const int n = w / UPR;
+            const int c = w - n * UPR;
+            cp_async<16>(buf + n * B + c * EPU, row0 + __ldg(a.offA + n) + c * EPU);
+        }
+    } else {
+#pragma unroll 4
+        for (int e = tid; e < B * N; e += THREADS) {
+            const int b = e / N;
+            const int n = e - b * N;
+            cp_async<sizeof(V)>(buf + G::idx(b, n), a.src + ubase + __ldg(a.offV + v0 + b) + __ldg(a.offA + n));
+        }
+    }
+}
+
+// KIND_PIPE: persistent CTAs walk the tiles with a stride of gridDim.x; while
+// tile t is transformed in one shared buffer, tile t + gridDim.x streams into
+// the other, so every SM keeps HBM reads in flight through its compute phase.
+template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) fft_pipe_kernel(const PassArgs<T> a) {
+    using V = cx<T>;
+    using G = TileGeom<MODE, B, PLAN::N>;
+    constexpr int N = PLAN::N;
+    constexpr int TWN = PLAN::twtotal();
+    static_assert(PLAN::S >= 2, "the pipelined kernel needs at least two stages");
+    static_assert(MODE != MODE_BATCH || THREADS % B == 0, "batch mode needs THREADS % B == 0");
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* buf0 = reinterpret_cast<V*>(smem_raw);
+    V* buf1 = buf0 + G::elems;
+    V* tw = buf1 + G::elems;
+    uint32_t* offA_s = reinterpret_cast<uint32_t*>(tw + TWN);
+    size_t* base0 = reinterpret_cast<size_t*>(
+        smem_raw + ((sizeof(V) * (size_t)(2 * G::elems + TWN) + sizeof(uint32_t) * N + 15) & ~size_t(15)));
+    size_t* base1 = base0 + B;
+
+    const int tid = threadIdx.x;
+    const int tilesV = a.NV / B;
+    const int ntiles = a.NU * tilesV;
+    int t = blockIdx.x;
+    if (t < ntiles) pipe_issue<T, PLAN, B, THREADS, MODE>(a, t, tilesV, buf0, base0, tid);
+    cp_async_commit();
+    for (int i = tid; i < TWN; i += THREADS) tw[i] = a.tw[i];
+    for (int i = tid; i < N; i += THREADS) offA_s[i] = a.offA[i];
+    bool odd = false;
+    for (; t < ntiles; t += gridDim.x, odd = !odd) {
+        V* cur = odd ? buf1 : buf0;
+        size_t* cbase = odd ? base1 : base0;
+        const int tn = t + gridDim.x;
+        if (tn < ntiles) pipe_issue<T, PLAN, B, THREADS, MODE>(a, tn, tilesV, odd ? buf0 : buf1, odd ? base0 : base1,
+                                                              tid);
+        cp_async_commit();
+        cp_async_wait<1>();  // this thread's copies of tile t have landed
+        __syncthreads();     // ... and every other thread's
+        run_stage<T, PLAN, B, THREADS, MODE, INV, 0>(a, cur, tw, offA_s, cbase, tid);
+        __syncthreads();     // `cur` and `cbase` are free for the copies issued next iteration
+    }
+    cp_async_wait<0>();
 }
 
 }  // namespace a2a

@@ -2,12 +2,28 @@
 #pragma once
 
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "../../include/a2afft_b200.h"
 #include "fft_registry.cuh"
 
 namespace a2a {
+
+// The kernel choice for one use of a pass (one axis, one direction): every
+// compiled variant of its length, which of them fit the pass geometry, and the
+// one in use.
+struct PassSlot {
+    PassKernel cand[kMaxVariants];
+    int occ[kMaxVariants] = {0};       // resident CTAs per SM
+    bool fits[kMaxVariants] = {false};
+    float tuned_ms[kMaxVariants] = {0};  // make_plans timings (0 = not timed)
+    int ncand = 0;
+    int chosen = 0;
+    const PassKernel& k() const { return cand[chosen]; }
+};
+
+enum SlotId { SLOT_Z = 0, SLOT_X = 1, SLOT_Y = 2, SLOT_LINES = 3, NSLOTS = 4 };
 
 // Everything an a2aDistribution carries, for all virtual ranks at once.
 struct Dist {
@@ -36,9 +52,10 @@ struct Dist {
     // precision of the plan
     void* d_tw = nullptr;
     const void* tw[3] = {nullptr, nullptr, nullptr};
-    // pass kernels per axis: [axis][inverse]
-    PassKernel kline[3][2];
-    PassKernel kbatch[3][2];
+    // host copies of the offset tables (geometry checks)
+    std::vector<uint32_t> h_off[3];
+    // pass kernels: [slot][inverse]
+    PassSlot slot[NSLOTS][2];
 };
 
 // remap.cu

@@ -244,7 +244,10 @@ def run_ours(args, rank, world, local_rank):
     ng, ranks = args.ng, args.ranks
     dist = pkg.a2aDistribution(ranks, ng, 64, precision="c64")
     dfft = pkg.a2adfft(dist, method=args.method)
-    dfft.make_plans()
+    scratch = dist.empty(dev)  # make_plans times the pass variants on it
+    dfft.make_plans(scratch)
+    plan_report = dfft.plan_report()
+    del scratch
     x = synth_bricks(torch, ng, dist.dims, SEED, dev)
     x0 = x.clone()
     stream = torch.cuda.Stream(device=dev)
@@ -364,6 +367,7 @@ def run_ours(args, rank, world, local_rank):
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                      "traffic": traffic, "algorithmic_bytes": alg_bytes},
         "per_pass_ms": {n: round(m, 4) for n, m in zip(names, means)},
+        "plan": [ln for ln in plan_report.splitlines() if "chosen" in ln],
         "effective_gbs": round(alg_total / (step_ms * 1e-3) / 1e9, 1),
         "hbm_frac": round(alg_total / (step_ms * 1e-3) / 1e9 / peak, 4),
         "transforms_per_s": round(2 * 1e3 / step_ms, 2),

@@ -147,9 +147,28 @@ a2a_status a2a_dfft_set_method(a2a_dfft* dfft, a2a_method method);
 
 /* a2adfft::make_plans(fftPrecision** d_scratch) (dfft/a2adfft.cpp:18-24).
  * The scratch buffer is borrowed as in the reference (same size as a data
- * buffer; NULL is accepted because the fused transform runs in place).
- * Kernel choice and twiddle tables (FP64-generated) are fixed here. */
+ * buffer).  The fused transform runs in place and never touches it; when it
+ * is given (and autotuning is on, the default), make_plans times every
+ * compiled launch variant of each axis pass on it -- clobbering its contents,
+ * as the reference's transforms do -- and keeps the fastest.  With NULL the
+ * default variant of each pass is used.  The choice is stored in the
+ * distribution and shared by every dfft built on it. */
 a2a_status a2a_dfft_make_plans(a2a_dfft* dfft, void** d_scratch);
+
+/* Turns the make_plans timing run on (default) or off.  No reference
+ * counterpart. */
+a2a_status a2a_dfft_set_autotune(a2a_dfft* dfft, int enable);
+
+/* Launch variants compiled for a pass (0 = Z, 1 = X, 2 = Y), and a manual
+ * choice among them (overrides the default or the make_plans timing; fails
+ * with A2A_ERROR_UNSUPPORTED for a variant that does not fit the pass).  No
+ * reference counterpart. */
+a2a_status a2a_dfft_variant_count(const a2a_dfft* dfft, int pass, int* count);
+a2a_status a2a_dfft_select_variant(a2a_dfft* dfft, int pass, int variant);
+
+/* Text report of every pass variant (length, tile, threads, occupancy,
+ * make_plans timing, the chosen one) into buf.  No reference counterpart. */
+a2a_status a2a_dfft_plan_report(const a2a_dfft* dfft, char* buf, size_t len);
 
 /* a2adfft::forward / inverse (dfft/a2adfft.cpp:26-158): in place on
  * d_data[0], rank-major bricks in, rank-major bricks out, natural frequency

@@ -104,3 +104,59 @@ def test_box_transform(pkg, oracle, cuda):
         f.inverse(x)
         inv = oracle.bricks_to_global(x.cpu().numpy().reshape(4, -1), d)
         assert oracle.rel_l2(inv, g) <= TOL[prec]
+
+
+@pytest.mark.parametrize("prec", ["c64", "c128"])
+@pytest.mark.parametrize("P,ng", [(4, 64), (16, 128), (4, 96), (16, 192), (16, 256), (64, 512)])
+def test_every_launch_variant(pkg, oracle, cuda, P, ng, prec):
+    """Each compiled launch variant of each pass (the autotuner may pick any of
+    them) gives the same transform."""
+    import torch
+
+    dist = pkg.a2aDistribution(P, ng, 64, precision=prec)
+    d = oracle.Decomp(ng, P)
+    g = oracle.make_input("normal", (ng,) * 3, seed=11, dtype=CDT[prec])
+    x0 = torch.from_numpy(oracle.global_to_bricks(g, d).ravel()).to(cuda)
+    f = pkg.a2adfft(dist)
+    f.make_plans()
+    f.forward(x := x0.clone())
+    base = x.clone()
+    rng = np.random.default_rng(0)
+    pts = [tuple(int(v) for v in rng.integers(0, ng, 3)) for _ in range(4)]
+    fwd = oracle.bricks_to_global(base.cpu().numpy().reshape(P, -1), d)
+    exact = oracle.dft_points(g, pts)
+    got = np.array([fwd[p] for p in pts])
+    assert np.max(np.abs(got - exact)) / np.sqrt(float(ng) ** 3) <= (1e-5 if prec == "c64" else 1e-12)
+    tested = 0
+    for p in range(3):
+        for v in range(f.variant_count(p)):
+            try:
+                f.select_variant(p, v)
+            except pkg.A2AError:
+                continue  # does not fit this geometry
+            x = x0.clone()
+            f.forward(x)
+            assert oracle.rel_l2(x.cpu().numpy(), base.cpu().numpy()) <= (1e-6 if prec == "c64" else 1e-13), \
+                f"pass {p} variant {v}"
+            f.inverse(x)
+            assert oracle.rel_l2(x.cpu().numpy(), x0.cpu().numpy()) <= (1e-6 if prec == "c64" else 1e-12)
+            tested += 1
+        f.select_variant(p, 0)
+    assert tested >= 3
+
+
+def test_autotune_report(pkg, oracle, cuda):
+    import torch
+
+    dist = pkg.a2aDistribution(16, 128, 64, precision="c64")
+    f = pkg.a2adfft(dist)
+    scratch = dist.empty()
+    f.make_plans(scratch)
+    rep = f.plan_report()
+    assert rep.count("<- chosen") == 3
+    d = oracle.Decomp(128, 16)
+    g = oracle.make_input("uniform", (128,) * 3, seed=1, dtype=np.complex64)
+    x = torch.from_numpy(oracle.global_to_bricks(g, d).ravel()).to(cuda)
+    f.forward(x)
+    fwd = oracle.bricks_to_global(x.cpu().numpy().reshape(16, -1), d)
+    assert oracle.rel_l2(fwd, oracle.fft3_global(g)) <= 1e-6
