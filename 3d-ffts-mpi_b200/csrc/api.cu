@@ -112,17 +112,22 @@ SlotGeom slot_geom(const Dist& d, int slot) {
     }
 }
 
-// Does variant k fit the slot's geometry?  Every kernel needs whole tiles; the
-// pipelined BATCH kernel also moves each tile row as 16-byte units, so every
-// tile's lines must be contiguous and 16-byte aligned.
+// Does variant k fit the slot's geometry?  Every kernel needs whole tiles.
+// Kernels that move several lines per 16-byte access (the pipelined BATCH
+// kernel: whole tile rows; LPT = 2: line pairs) need those lines contiguous
+// and 16-byte aligned in every tile.
 bool variant_fits(const Dist& d, const SlotGeom& g, const PassKernel& k) {
     if (g.NV % k.lines) return false;
-    if (k.kind != a2a::KIND_PIPE || g.mode != a2a::MODE_BATCH) return true;
+    int vec = 1;  // lines per 16-byte access
+    if (k.kind == a2a::KIND_PIPE && g.mode == a2a::MODE_BATCH) vec = k.lines;
+    if (k.lpt > 1) vec = k.lpt;
+    if (k.lpt > 1 && g.mode != a2a::MODE_BATCH) return false;
+    if (vec == 1) return true;
     if (!g.hA) return false;
     const size_t epu = 16 / d.elem_bytes;
-    if ((k.lines * d.elem_bytes) % 16) return false;
-    for (int v0 = 0; v0 < g.NV; v0 += k.lines) {
-        for (int b = 1; b < k.lines; ++b)
+    if ((vec * d.elem_bytes) % 16) return false;
+    for (int v0 = 0; v0 < g.NV; v0 += vec) {
+        for (int b = 1; b < vec; ++b)
             if ((*g.hV)[v0 + b] != (*g.hV)[v0] + (uint32_t)b) return false;
         if ((*g.hV)[v0] % epu) return false;
     }
@@ -131,6 +136,17 @@ bool variant_fits(const Dist& d, const SlotGeom& g, const PassKernel& k) {
     for (uint32_t o : *g.hU)
         if (o % epu) return false;
     return true;
+}
+
+// Whether offA[j + r N/R] == offA[j] + offA[r N/R] holds for the first and
+// last stage of kernel k on a slot whose axis has brick extent l: true when
+// l and N/R divide one another (no carry from the in-brick position into the
+// rank part of the offset).
+int split_ok(int l, const PassKernel& k) {
+    const int nb0 = k.n / k.radix[0];
+    const int nbl = k.n / k.radix[k.nstages - 1];
+    auto ok = [l](int nb) { return (l % nb == 0) || (nb % l == 0); };
+    return ok(nb0) && ok(nbl) ? 1 : 0;
 }
 
 // Stage twiddles W_{Ns R}^{r m} (forward sign), laid out as RadixPlan::twoff,
@@ -170,7 +186,7 @@ a2a_status finish(const Dist& d, cudaStream_t st, bool sync) {
 template <typename T>
 cudaError_t launch_pass_t(const PassKernel& k, unsigned grid, const void* src, void* dst, const uint32_t* offA,
                           const uint32_t* offU, const uint32_t* offV, const void* tw, int NU, int NV, double scale,
-                          cudaStream_t st) {
+                          int split, cudaStream_t st) {
     a2a::PassArgs<T> a;
     a.src = static_cast<const a2a::cx<T>*>(src);
     a.dst = static_cast<a2a::cx<T>*>(dst);
@@ -181,6 +197,7 @@ cudaError_t launch_pass_t(const PassKernel& k, unsigned grid, const void* src, v
     a.NU = NU;
     a.NV = NV;
     a.scale = T(scale);
+    a.split = split;
     void* args[] = {&a};
     return cudaLaunchKernel(k.fn, dim3(grid), dim3(k.threads), args, k.smem, st);
 }
@@ -196,9 +213,13 @@ cudaError_t launch_slot(const Dist& d, int slot, bool inv, int c, void* p, doubl
         const uint64_t resident = (uint64_t)std::max(ps.occ[c], 1) * d.sms;
         grid = std::min(tiles, resident);
     }
+    const int l = slot == a2a::SLOT_Z ? d.local[2] : slot == a2a::SLOT_X ? d.local[0]
+                : slot == a2a::SLOT_Y ? d.local[1] : d.ng[0];
+    const int split = split_ok(l, k);
     if (d.prec == A2A_C128)
-        return launch_pass_t<double>(k, unsigned(grid), p, p, g.offA, g.offU, g.offV, g.tw, g.NU, g.NV, scale, st);
-    return launch_pass_t<float>(k, unsigned(grid), p, p, g.offA, g.offU, g.offV, g.tw, g.NU, g.NV, scale, st);
+        return launch_pass_t<double>(k, unsigned(grid), p, p, g.offA, g.offU, g.offV, g.tw, g.NU, g.NV, scale, split,
+                                     st);
+    return launch_pass_t<float>(k, unsigned(grid), p, p, g.offA, g.offU, g.offV, g.tw, g.NU, g.NV, scale, split, st);
 }
 
 a2a_status setup_distribution(Dist& d, int nx, int ny, int nz, int P, int block_size, a2a_precision prec) {
@@ -281,9 +302,6 @@ a2a_status setup_distribution(Dist& d, int nx, int ny, int nz, int P, int block_
             for (int c = 0; c < ps.ncand; ++c) {
                 const PassKernel& k = ps.cand[c];
                 A2A_CUDA(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem),
-                         "cudaFuncSetAttribute");
-                A2A_CUDA(cudaFuncSetAttribute(k.fn, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                              (int)cudaSharedmemCarveoutMaxShared),
                          "cudaFuncSetAttribute");
                 A2A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ps.occ[c], k.fn, k.threads, k.smem),
                          "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
@@ -668,8 +686,9 @@ a2a_status a2a_dfft_plan_report(const a2a_dfft* f, char* buf, size_t len) {
             const PassKernel& k = ps.cand[c];
             char line[256];
             snprintf(line, sizeof line,
-                     "%s pass n=%d %s lines=%d threads=%d smem=%zu occ=%d radix=%d,%d,%d,%d fits=%d tuned_ms=%.4f%s\n",
-                     names[p], k.n, k.kind == a2a::KIND_PIPE ? "pipe" : "direct", k.lines, k.threads, k.smem,
+                     "%s pass n=%d %s lines=%d lpt=%d threads=%d smem=%zu occ=%d radix=%d,%d,%d,%d fits=%d "
+                     "tuned_ms=%.4f%s\n",
+                     names[p], k.n, k.kind == a2a::KIND_PIPE ? "pipe" : "direct", k.lines, k.lpt, k.threads, k.smem,
                      ps.occ[c], k.radix[0], k.radix[1], k.radix[2], k.radix[3], (int)ps.fits[c], ps.tuned_ms[c],
                      c == ps.chosen ? " <- chosen" : "");
             out += line;

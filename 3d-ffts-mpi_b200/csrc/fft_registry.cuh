@@ -17,6 +17,7 @@ struct PassKernel {
     int threads = 0;
     int lines = 0;      // B: lines per tile (a pass needs NV % lines == 0)
     int min_blocks = 1; // __launch_bounds__ minimum blocks per SM
+    int lpt = 1;        // lines a thread moves per access (2: 16-byte line pairs)
     size_t smem = 0;    // dynamic shared memory bytes
     int nstages = 0;
     int radix[4] = {0, 0, 0, 0};
@@ -53,96 +54,121 @@ template <typename T, int N> struct PassPlan;
 A2A_PLANS(float)
 A2A_PLANS(double)
 
-// Launch variants X(T, N, KIND, B lines per tile, THREADS, MINB).  The first
+// Launch variants X(T, N, KIND, B lines per tile, THREADS, MINB, LPT).  The first
 // entry per N is the default; make_plans can time the others on the scratch
 // buffer and keep the fastest (a2a_dfft_make_plans).  DIRECT tiles are about
 // 32-64 KB so two or three CTAs share an SM; PIPE CTAs hold two tiles.
-#define A2A_VARIANTS_F32(X)                         \
-    X(float,    4, KIND_DIRECT,  4,  32, 1)         \
-    X(float,    8, KIND_DIRECT,  8,  32, 1)         \
-    X(float,   12, KIND_DIRECT,  4,  32, 1)         \
-    X(float,   16, KIND_DIRECT, 16,  32, 1)         \
-    X(float,   24, KIND_DIRECT,  8,  32, 1)         \
-    X(float,   32, KIND_DIRECT, 32, 128, 1)         \
-    X(float,   48, KIND_DIRECT, 16,  64, 1)         \
-    X(float,   64, KIND_DIRECT, 32, 128, 1)         \
-    X(float,   64, KIND_PIPE,   32, 128, 4)         \
-    X(float,   96, KIND_DIRECT, 32, 128, 1)         \
-    X(float,   96, KIND_PIPE,   32, 128, 2)         \
-    X(float,  128, KIND_DIRECT, 32, 256, 1)         \
-    X(float,  128, KIND_PIPE,   32, 256, 2)         \
-    X(float,  192, KIND_DIRECT, 32, 256, 1)         \
-    X(float,  192, KIND_PIPE,   16, 256, 2)         \
-    X(float,  256, KIND_DIRECT, 32, 256, 1)         \
-    X(float,  256, KIND_PIPE,   16, 256, 2)         \
-    X(float,  256, KIND_PIPE,   32, 512, 1)         \
-    X(float,  384, KIND_DIRECT, 16, 256, 1)         \
-    X(float,  384, KIND_PIPE,    8, 256, 2)         \
-    X(float,  512, KIND_DIRECT, 16, 256, 2)         \
-    X(float,  512, KIND_PIPE,   16, 512, 1)         \
-    X(float,  512, KIND_PIPE,    8, 256, 2)         \
-    X(float,  512, KIND_DIRECT, 16, 512, 1)         \
-    X(float,  512, KIND_PIPE,   16, 256, 1)         \
-    X(float,  768, KIND_DIRECT,  8, 256, 1)         \
-    X(float,  768, KIND_PIPE,    8, 384, 1)         \
-    X(float, 1024, KIND_DIRECT,  8, 256, 1)         \
-    X(float, 1024, KIND_PIPE,    8, 512, 1)
+#define A2A_VARIANTS_F32(X)                            \
+    X(float,    4, KIND_DIRECT,  4,  32, 1, 1)         \
+    X(float,    8, KIND_DIRECT,  8,  32, 1, 1)         \
+    X(float,   12, KIND_DIRECT,  4,  32, 1, 1)         \
+    X(float,   16, KIND_DIRECT, 16,  32, 1, 1)         \
+    X(float,   24, KIND_DIRECT,  8,  32, 1, 1)         \
+    X(float,   32, KIND_DIRECT, 32, 128, 1, 1)         \
+    X(float,   32, KIND_DIRECT, 32,  64, 1, 2)         \
+    X(float,   48, KIND_DIRECT, 16,  64, 1, 1)         \
+    X(float,   48, KIND_DIRECT, 16,  32, 1, 2)         \
+    X(float,   64, KIND_DIRECT, 32, 128, 1, 1)         \
+    X(float,   64, KIND_DIRECT, 32, 128, 1, 2)         \
+    X(float,   64, KIND_PIPE,   32, 128, 4, 1)         \
+    X(float,   96, KIND_DIRECT, 32, 128, 1, 1)         \
+    X(float,   96, KIND_DIRECT, 32, 128, 1, 2)         \
+    X(float,   96, KIND_PIPE,   32, 128, 2, 1)         \
+    X(float,  128, KIND_DIRECT, 32, 256, 1, 1)         \
+    X(float,  128, KIND_DIRECT, 32, 128, 1, 2)         \
+    X(float,  128, KIND_DIRECT, 16, 128, 4, 1)         \
+    X(float,  128, KIND_PIPE,   32, 256, 2, 1)         \
+    X(float,  192, KIND_DIRECT, 32, 256, 1, 1)         \
+    X(float,  192, KIND_DIRECT, 32, 256, 1, 2)         \
+    X(float,  192, KIND_PIPE,   16, 256, 2, 1)         \
+    X(float,  256, KIND_DIRECT, 32, 256, 1, 1)         \
+    X(float,  256, KIND_DIRECT, 32, 256, 1, 2)         \
+    X(float,  256, KIND_DIRECT, 16, 256, 2, 1)         \
+    X(float,  256, KIND_DIRECT, 16, 128, 4, 2)         \
+    X(float,  256, KIND_PIPE,   16, 256, 2, 1)         \
+    X(float,  384, KIND_DIRECT, 16, 256, 1, 1)         \
+    X(float,  384, KIND_DIRECT, 16, 256, 1, 2)         \
+    X(float,  384, KIND_PIPE,    8, 256, 2, 1)         \
+    X(float,  512, KIND_DIRECT, 16, 512, 1, 1)         \
+    X(float,  512, KIND_DIRECT, 16, 256, 2, 2)         \
+    X(float,  512, KIND_DIRECT, 16, 512, 1, 2)         \
+    X(float,  512, KIND_DIRECT,  8, 128, 4, 1)         \
+    X(float,  512, KIND_DIRECT,  8, 128, 4, 2)         \
+    X(float,  512, KIND_DIRECT, 16, 256, 2, 1)         \
+    X(float,  512, KIND_PIPE,    8, 256, 2, 1)         \
+    X(float,  768, KIND_DIRECT,  8, 256, 1, 1)         \
+    X(float,  768, KIND_DIRECT,  8, 256, 1, 2)         \
+    X(float,  768, KIND_DIRECT, 16, 384, 1, 2)         \
+    X(float,  768, KIND_PIPE,    8, 384, 1, 1)         \
+    X(float, 1024, KIND_DIRECT,  8, 256, 1, 1)         \
+    X(float, 1024, KIND_DIRECT,  8, 256, 1, 2)         \
+    X(float, 1024, KIND_DIRECT, 16, 512, 1, 2)         \
+    X(float, 1024, KIND_DIRECT,  8, 512, 1, 1)         \
+    X(float, 1024, KIND_PIPE,    8, 512, 1, 1)
 
 #define A2A_VARIANTS_F64(X)                         \
-    X(double,    4, KIND_DIRECT,  4,  32, 1)        \
-    X(double,    8, KIND_DIRECT,  8,  32, 1)        \
-    X(double,   12, KIND_DIRECT,  4,  32, 1)        \
-    X(double,   16, KIND_DIRECT, 16,  32, 1)        \
-    X(double,   24, KIND_DIRECT,  8,  32, 1)        \
-    X(double,   32, KIND_DIRECT, 16, 128, 1)        \
-    X(double,   48, KIND_DIRECT,  8,  64, 1)        \
-    X(double,   64, KIND_DIRECT, 32, 128, 1)        \
-    X(double,   64, KIND_PIPE,   16, 128, 2)        \
-    X(double,   96, KIND_DIRECT, 16, 128, 1)        \
-    X(double,   96, KIND_PIPE,   16, 128, 2)        \
-    X(double,  128, KIND_DIRECT, 16, 128, 1)        \
-    X(double,  128, KIND_PIPE,   16, 256, 2)        \
-    X(double,  192, KIND_DIRECT, 16, 256, 1)        \
-    X(double,  192, KIND_PIPE,    8, 256, 2)        \
-    X(double,  256, KIND_DIRECT, 16, 256, 1)        \
-    X(double,  256, KIND_PIPE,    8, 256, 2)        \
-    X(double,  384, KIND_DIRECT,  8, 256, 1)        \
-    X(double,  384, KIND_PIPE,    8, 384, 1)        \
-    X(double,  512, KIND_DIRECT,  8, 256, 1)        \
-    X(double,  512, KIND_PIPE,    8, 512, 1)        \
-    X(double,  768, KIND_DIRECT,  8, 384, 1)        \
-    X(double,  768, KIND_PIPE,    8, 768, 1)        \
-    X(double, 1024, KIND_DIRECT,  8, 512, 1)        \
-    X(double, 1024, KIND_PIPE,    4, 512, 1)
+    X(double,    4, KIND_DIRECT,  4,  32, 1, 1)        \
+    X(double,    8, KIND_DIRECT,  8,  32, 1, 1)        \
+    X(double,   12, KIND_DIRECT,  4,  32, 1, 1)        \
+    X(double,   16, KIND_DIRECT, 16,  32, 1, 1)        \
+    X(double,   24, KIND_DIRECT,  8,  32, 1, 1)        \
+    X(double,   32, KIND_DIRECT, 16, 128, 1, 1)        \
+    X(double,   48, KIND_DIRECT,  8,  64, 1, 1)        \
+    X(double,   64, KIND_DIRECT, 32, 128, 1, 1)        \
+    X(double,   64, KIND_PIPE,   16, 128, 2, 1)        \
+    X(double,   96, KIND_DIRECT, 16, 128, 1, 1)        \
+    X(double,   96, KIND_PIPE,   16, 128, 2, 1)        \
+    X(double,  128, KIND_DIRECT, 16, 128, 1, 1)        \
+    X(double,  128, KIND_PIPE,   16, 256, 2, 1)        \
+    X(double,  192, KIND_DIRECT, 16, 256, 1, 1)        \
+    X(double,  192, KIND_PIPE,    8, 256, 1, 1)        \
+    X(double,  256, KIND_DIRECT, 16, 256, 1, 1)        \
+    X(double,  256, KIND_PIPE,    8, 256, 1, 1)        \
+    X(double,  384, KIND_DIRECT,  8, 256, 1, 1)        \
+    X(double,  384, KIND_PIPE,    8, 384, 1, 1)        \
+    X(double,  512, KIND_DIRECT,  8, 256, 1, 1)        \
+    X(double,  512, KIND_PIPE,    8, 512, 1, 1)        \
+    X(double,  768, KIND_DIRECT,  8, 384, 1, 1)        \
+    X(double, 1024, KIND_DIRECT,  8, 512, 1, 1)
 // clang-format on
 
-template <typename T, int N, int KIND, int B, int TH, int MB, int MODE, bool INV>
+template <typename T, int N, int KIND, int B, int TH, int MB, int LPT, int MODE, bool INV>
 PassKernel make_pass_kernel() {
     using P = typename PassPlan<T, N>::Plan;
     PassKernel k;
     if constexpr (KIND == KIND_PIPE)
-        k.fn = reinterpret_cast<const void*>(&fft_pipe_kernel<T, P, B, TH, MODE, INV, MB>);
+        k.fn = reinterpret_cast<const void*>(&fft_pipe_kernel<T, P, B, TH, MODE, INV, MB, LPT>);
     else
-        k.fn = reinterpret_cast<const void*>(&fft_pass_kernel<T, P, B, TH, MODE, INV, MB>);
+        k.fn = reinterpret_cast<const void*>(&fft_pass_kernel<T, P, B, TH, MODE, INV, MB, LPT>);
     k.kind = KIND;
     k.n = N;
     k.threads = TH;
     k.lines = B;
     k.min_blocks = MB;
-    k.smem = pass_smem_bytes<T, P, B, MODE, KIND>();
+    k.lpt = LPT;
+    k.smem = pass_smem_bytes<T, P, B, MODE, KIND, LPT>();
     k.nstages = P::S;
     for (int s = 0; s < P::S; ++s) k.radix[s] = P::r[s];
     k.twtotal = P::twtotal();
     return k;
 }
 
-template <typename T, int N, int KIND, int B, int TH, int MB>
-PassKernel make_variant(int mode, bool inv) {
-    if (mode == MODE_LINE)
-        return inv ? make_pass_kernel<T, N, KIND, B, TH, MB, MODE_LINE, true>()
-                   : make_pass_kernel<T, N, KIND, B, TH, MB, MODE_LINE, false>();
-    return inv ? make_pass_kernel<T, N, KIND, B, TH, MB, MODE_BATCH, true>()
-               : make_pass_kernel<T, N, KIND, B, TH, MB, MODE_BATCH, false>();
+// A variant with LPT = 2 exists only for the batch mode (line pairs); in line
+// mode the lookup skips it.
+template <typename T, int N, int KIND, int B, int TH, int MB, int LPT>
+bool make_variant(int mode, bool inv, PassKernel* out) {
+    if (mode == MODE_LINE) {
+        if constexpr (LPT != 1) {
+            return false;
+        } else {
+            *out = inv ? make_pass_kernel<T, N, KIND, B, TH, MB, 1, MODE_LINE, true>()
+                       : make_pass_kernel<T, N, KIND, B, TH, MB, 1, MODE_LINE, false>();
+            return true;
+        }
+    }
+    *out = inv ? make_pass_kernel<T, N, KIND, B, TH, MB, LPT, MODE_BATCH, true>()
+               : make_pass_kernel<T, N, KIND, B, TH, MB, LPT, MODE_BATCH, false>();
+    return true;
 }
 
 // Defined in fft_pass_f32.cu / fft_pass_f64.cu: fills up to `max` variants of

@@ -36,6 +36,9 @@ template <typename T> using cx = typename CxOf<T>::type;
 template <typename V> struct RealOf;
 template <> struct RealOf<float2> { using type = float; };
 template <> struct RealOf<double2> { using type = double; };
+// float4 = the same element of two adjacent lines (complex float each); the
+// batch passes move line pairs with 16-byte accesses
+template <> struct RealOf<float4> { using type = float; };
 
 template <typename V>
 __host__ __device__ __forceinline__ V mk(typename RealOf<V>::type re, typename RealOf<V>::type im) {
@@ -59,9 +62,25 @@ __device__ __forceinline__ V cmul(V a, typename RealOf<V>::type c, typename Real
     return mk<V>(a.x * c - a.y * s, a.x * s + a.y * c);
 }
 // a * w, or a * conj(w)
-template <bool CONJ, typename V> __device__ __forceinline__ V cmulw(V a, V w) {
+template <bool CONJ, typename V, typename W> __device__ __forceinline__ V cmulw(V a, W w) {
     return CONJ ? cmul(a, w.x, -w.y) : cmul(a, w.x, w.y);
 }
+
+// line-pair (float4) versions of the complex operations
+__device__ __forceinline__ float4 add(float4 a, float4 b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
+__device__ __forceinline__ float4 sub(float4 a, float4 b) { return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w); }
+__device__ __forceinline__ float4 neg(float4 a) { return make_float4(-a.x, -a.y, -a.z, -a.w); }
+__device__ __forceinline__ float4 mul_pi(float4 a) { return make_float4(-a.y, a.x, -a.w, a.z); }
+__device__ __forceinline__ float4 mul_mi(float4 a) { return make_float4(a.y, -a.x, a.w, -a.z); }
+__device__ __forceinline__ float4 scl(float4 a, float s) { return make_float4(a.x * s, a.y * s, a.z * s, a.w * s); }
+__device__ __forceinline__ float4 cmul(float4 a, float c, float s) {
+    return make_float4(a.x * c - a.y * s, a.x * s + a.y * c, a.z * c - a.w * s, a.z * s + a.w * c);
+}
+
+// element a thread moves per (tile line, n): one complex, or for LPT = 2 the
+// same index of two adjacent lines
+template <typename T, int LPT> struct ElemOf { using type = cx<T>; };
+template <> struct ElemOf<float, 2> { using type = float4; };
 
 // cos(2 pi m / 16) and sin(2 pi m / 16), m = 0..15: the sixteenth roots of
 // unity, to 21 significant digits.
@@ -222,6 +241,10 @@ template <typename T> struct PassArgs {
     int NU;
     int NV;                // multiple of B
     T scale;               // multiplies every stored element
+    // offA[j + r N/R] == offA[j] + offA[r N/R] for the first and last stage
+    // (the brick extent along the axis and N/R divide one another): addresses
+    // are then one table value per butterfly plus CTA-uniform deltas
+    int split;
 };
 
 // Butterfly q of a stage -> (tile line b, butterfly j), NBL butterflies per
@@ -238,16 +261,16 @@ template <bool BFAST, int B, int NBL> __device__ __forceinline__ void bf_map(int
     }
 }
 
-// Shared-memory layout of one tile.  BATCH: [n][b] (lines fastest).  LINE:
-// line b at b*LS, element n at n + n/32 (one pad slot per 32 elements keeps
-// strided butterfly writes spread over the banks); LS is odd, so lanes that
-// walk across lines hit distinct banks.
-template <int MODE, int B, int N> struct TileGeom {
+// Shared-memory layout of one tile of BV vector lines.  BATCH: [n][bv]
+// (lines fastest).  LINE: line b at b*LS, element n at n + n/32 (one pad
+// slot per 32 elements keeps strided butterfly writes spread over the banks);
+// LS is odd, so lanes that walk across lines hit distinct banks.
+template <int MODE, int BV, int N> struct TileGeom {
     static constexpr int LS = (N + N / 32) | 1;
-    static constexpr int elems = (MODE == MODE_BATCH) ? N * B : B * LS;
+    static constexpr int elems = (MODE == MODE_BATCH) ? N * BV : BV * LS;
     static __device__ __forceinline__ int idx(int b, int n) {
         if constexpr (MODE == MODE_BATCH)
-            return n * B + b;
+            return n * BV + b;
         else
             return b * LS + n + (n >> 5);
     }
@@ -272,52 +295,65 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
 
 // Stages s >= 1 (and stage 0 of the pipelined kernel): shared -> registers,
 // twiddle, DFT_R, then shared (Stockham position) or, for the last stage,
-// global memory at base_s[b] + offA_s[n].
-template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV, int s>
-__device__ __forceinline__ void run_stage(const PassArgs<T>& a, cx<T>* tile, const cx<T>* tw,
-                                          const uint32_t* offA_s, const size_t* base_s, int tid) {
-    using V = cx<T>;
-    using G = TileGeom<MODE, B, PLAN::N>;
+// global memory at base_s[b] + offA_s[n].  A thread moves LPT lines at once.
+template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV, int LPT, int s>
+__device__ __forceinline__ void run_stage(const PassArgs<T>& a, typename ElemOf<T, LPT>::type* tile,
+                                          const cx<T>* tw, const uint32_t* offA_s, const size_t* base_s, int tid) {
+    using E = typename ElemOf<T, LPT>::type;
+    constexpr int BV = B / LPT;
+    using G = TileGeom<MODE, BV, PLAN::N>;
     constexpr int N = PLAN::N;
     constexpr int R = PLAN::r[s];
     constexpr int NS = PLAN::ns(s);
     constexpr int NBL = N / R;             // butterflies per line
-    constexpr int NBT = B * NBL;           // butterflies per tile
+    constexpr int NBT = BV * NBL;          // butterflies per tile
     constexpr int K = (NBT + THREADS - 1) / THREADS;
     constexpr bool EXACT = (NBT % THREADS) == 0;
     constexpr bool LAST = (s == PLAN::S - 1);
     constexpr bool BFAST = (MODE == MODE_BATCH) || !LAST;
     constexpr int TWO = PLAN::twoff(s);
 
-    V x[K][R];
+    E x[K][R];
 #pragma unroll
     for (int k = 0; k < K; ++k) {
         const int q = tid + k * THREADS;
         if (EXACT || q < NBT) {
             int b, j;
-            bf_map<BFAST, B, NBL>(q, b, j);
+            bf_map<BFAST, BV, NBL>(q, b, j);
 #pragma unroll
             for (int r = 0; r < R; ++r) x[k][r] = tile[G::idx(b, j + r * NBL)];
         }
     }
     __syncthreads();  // the tile is updated in place
+    uint32_t dl[R];
+    if constexpr (LAST) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) dl[r] = offA_s[r * NBL];
+    }
 #pragma unroll
     for (int k = 0; k < K; ++k) {
         const int q = tid + k * THREADS;
         if (EXACT || q < NBT) {
             int b, j;
-            bf_map<BFAST, B, NBL>(q, b, j);
+            bf_map<BFAST, BV, NBL>(q, b, j);
             const int m = j % NS;
             if constexpr (s > 0) {
 #pragma unroll
                 for (int r = 1; r < R; ++r) x[k][r] = cmulw<INV>(x[k][r], tw[TWO + (r - 1) * NS + m]);
             }
-            Dft<R, INV, V>::run(x[k]);
+            Dft<R, INV, E>::run(x[k]);
             if constexpr (LAST) {
-                const size_t lb = base_s[b];
+                cx<T>* line = a.dst + base_s[b];
+                if (a.split) {
+                    cx<T>* p = line + offA_s[j];
 #pragma unroll
-                for (int r = 0; r < R; ++r)
-                    st_stream(a.dst + lb + offA_s[j + r * NBL], scl(x[k][r], a.scale));
+                    for (int r = 0; r < R; ++r)
+                        st_stream(reinterpret_cast<E*>(p + dl[r]), scl(x[k][r], a.scale));
+                } else {
+#pragma unroll
+                    for (int r = 0; r < R; ++r)
+                        st_stream(reinterpret_cast<E*>(line + offA_s[j + r * NBL]), scl(x[k][r], a.scale));
+                }
             } else {
                 const int jd = (j / NS) * NS * R + m;
 #pragma unroll
@@ -327,7 +363,7 @@ __device__ __forceinline__ void run_stage(const PassArgs<T>& a, cx<T>* tile, con
     }
     if constexpr (!LAST) {
         __syncthreads();
-        run_stage<T, PLAN, B, THREADS, MODE, INV, s + 1>(a, tile, tw, offA_s, base_s, tid);
+        run_stage<T, PLAN, B, THREADS, MODE, INV, LPT, s + 1>(a, tile, tw, offA_s, base_s, tid);
     }
 }
 
@@ -336,40 +372,46 @@ enum PassKind : int {
     KIND_PIPE = 1     // persistent CTAs, next tile prefetched into shared memory
 };
 
-template <typename T, class PLAN, int B, int MODE, int KIND>
+template <typename T, class PLAN, int B, int MODE, int KIND, int LPT>
 __host__ __device__ constexpr size_t pass_smem_bytes() {
+    using E = typename ElemOf<T, LPT>::type;
     constexpr int N = PLAN::N;
+    constexpr int BV = B / LPT;
     constexpr int NBUF = KIND == KIND_PIPE ? 2 : 1;
-    size_t bytes = sizeof(cx<T>) * (size_t)(NBUF * TileGeom<MODE, B, N>::elems + PLAN::twtotal());
+    size_t bytes = sizeof(E) * (size_t)(NBUF * TileGeom<MODE, BV, N>::elems);
+    bytes += sizeof(cx<T>) * (size_t)PLAN::twtotal();
     bytes += sizeof(uint32_t) * (size_t)N;
     bytes = (bytes + 15) & ~size_t(15);
-    bytes += sizeof(size_t) * (size_t)(NBUF * B);
+    bytes += sizeof(size_t) * (size_t)(NBUF * BV);
     return bytes;
 }
 
 // KIND_DIRECT: one CTA = one tile of B lines (u, v0 .. v0+B-1).  Stage 0
 // reads global memory straight into registers (j fastest in LINE mode, so
-// the loads coalesce along the line).
-template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV, int MINB>
+// the loads coalesce along the line).  With LPT = 2 (BATCH, complex float) a
+// thread moves the same element of two adjacent lines as one 16-byte access.
+template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV, int MINB, int LPT>
 __global__ void __launch_bounds__(THREADS, MINB) fft_pass_kernel(const PassArgs<T> a) {
-    using V = cx<T>;
-    using G = TileGeom<MODE, B, PLAN::N>;
+    using E = typename ElemOf<T, LPT>::type;
+    constexpr int BV = B / LPT;
+    using G = TileGeom<MODE, BV, PLAN::N>;
     constexpr int N = PLAN::N;
     constexpr int R0 = PLAN::r[0];
     constexpr int NBL = N / R0;
-    constexpr int NBT = B * NBL;
+    constexpr int NBT = BV * NBL;
     constexpr int K = (NBT + THREADS - 1) / THREADS;
     constexpr bool EXACT = (NBT % THREADS) == 0;
     constexpr int TWN = PLAN::twtotal();
     constexpr bool BFAST0 = (MODE == MODE_BATCH);
-    static_assert(MODE != MODE_BATCH || THREADS % B == 0, "batch mode needs THREADS % B == 0");
+    static_assert(MODE != MODE_BATCH || THREADS % BV == 0, "batch mode needs THREADS % (B/LPT) == 0");
+    static_assert(LPT == 1 || MODE == MODE_BATCH, "line pairs only in batch mode");
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    V* tile = reinterpret_cast<V*>(smem_raw);
-    V* tw = tile + G::elems;
+    E* tile = reinterpret_cast<E*>(smem_raw);
+    cx<T>* tw = reinterpret_cast<cx<T>*>(tile + G::elems);
     uint32_t* offA_s = reinterpret_cast<uint32_t*>(tw + TWN);
     size_t* base_s = reinterpret_cast<size_t*>(
-        smem_raw + ((sizeof(V) * (size_t)(G::elems + TWN) + sizeof(uint32_t) * N + 15) & ~size_t(15)));
+        smem_raw + ((sizeof(E) * (size_t)G::elems + sizeof(cx<T>) * TWN + sizeof(uint32_t) * N + 15) & ~size_t(15)));
 
     const int tid = threadIdx.x;
     const int tilesV = a.NV / B;
@@ -377,22 +419,34 @@ __global__ void __launch_bounds__(THREADS, MINB) fft_pass_kernel(const PassArgs<
     const int v0 = (blockIdx.x - u * tilesV) * B;
     const size_t ubase = a.offU[u];
 
-    V x[K][R0];
+    uint32_t d0[R0];
+    if (a.split) {
+#pragma unroll
+        for (int r = 0; r < R0; ++r) d0[r] = __ldg(a.offA + r * NBL);
+    }
+    E x[K][R0];
 #pragma unroll
     for (int k = 0; k < K; ++k) {
         const int q = tid + k * THREADS;
         if (EXACT || q < NBT) {
             int b, j;
-            bf_map<BFAST0, B, NBL>(q, b, j);
-            const size_t lb = ubase + __ldg(a.offV + v0 + b);
+            bf_map<BFAST0, BV, NBL>(q, b, j);
+            const cx<T>* line = a.src + ubase + __ldg(a.offV + v0 + b * LPT);
+            if (a.split) {
+                const cx<T>* p = line + __ldg(a.offA + j);
 #pragma unroll
-            for (int r = 0; r < R0; ++r) x[k][r] = ld_stream(a.src + lb + __ldg(a.offA + j + r * NBL));
+                for (int r = 0; r < R0; ++r) x[k][r] = ld_stream(reinterpret_cast<const E*>(p + d0[r]));
+            } else {
+#pragma unroll
+                for (int r = 0; r < R0; ++r)
+                    x[k][r] = ld_stream(reinterpret_cast<const E*>(line + __ldg(a.offA + j + r * NBL)));
+            }
         }
     }
     // tables for the later stages (overlaps the loads in flight)
     for (int i = tid; i < TWN; i += THREADS) tw[i] = a.tw[i];
     for (int i = tid; i < N; i += THREADS) offA_s[i] = a.offA[i];
-    for (int i = tid; i < B; i += THREADS) base_s[i] = ubase + a.offV[v0 + i];
+    for (int i = tid; i < BV; i += THREADS) base_s[i] = ubase + a.offV[v0 + i * LPT];
 
     if constexpr (PLAN::S == 1) {
 #pragma unroll
@@ -400,12 +454,12 @@ __global__ void __launch_bounds__(THREADS, MINB) fft_pass_kernel(const PassArgs<
             const int q = tid + k * THREADS;
             if (EXACT || q < NBT) {
                 int b, j;
-                bf_map<BFAST0, B, NBL>(q, b, j);
-                Dft<R0, INV, V>::run(x[k]);
-                const size_t lb = ubase + __ldg(a.offV + v0 + b);
+                bf_map<BFAST0, BV, NBL>(q, b, j);
+                Dft<R0, INV, E>::run(x[k]);
+                cx<T>* line = a.dst + ubase + __ldg(a.offV + v0 + b * LPT);
 #pragma unroll
                 for (int r = 0; r < R0; ++r)
-                    st_stream(a.dst + lb + __ldg(a.offA + j + r * NBL), scl(x[k][r], a.scale));
+                    st_stream(reinterpret_cast<E*>(line + __ldg(a.offA + j + r * NBL)), scl(x[k][r], a.scale));
             }
         }
     } else {
@@ -414,14 +468,14 @@ __global__ void __launch_bounds__(THREADS, MINB) fft_pass_kernel(const PassArgs<
             const int q = tid + k * THREADS;
             if (EXACT || q < NBT) {
                 int b, j;
-                bf_map<BFAST0, B, NBL>(q, b, j);
-                Dft<R0, INV, V>::run(x[k]);
+                bf_map<BFAST0, BV, NBL>(q, b, j);
+                Dft<R0, INV, E>::run(x[k]);
 #pragma unroll
                 for (int r = 0; r < R0; ++r) tile[G::idx(b, j * R0 + r)] = x[k][r];
             }
         }
         __syncthreads();
-        run_stage<T, PLAN, B, THREADS, MODE, INV, 1>(a, tile, tw, offA_s, base_s, tid);
+        run_stage<T, PLAN, B, THREADS, MODE, INV, LPT, 1>(a, tile, tw, offA_s, base_s, tid);
     }
 }
 
@@ -463,7 +517,7 @@ __device__ __forceinline__ void pipe_issue(const PassArgs<T>& a, int t, int tile
 // KIND_PIPE: persistent CTAs walk the tiles with a stride of gridDim.x; while
 // tile t is transformed in one shared buffer, tile t + gridDim.x streams into
 // the other, so every SM keeps HBM reads in flight through its compute phase.
-template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV, int MINB>
+template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV, int MINB, int LPT>
 __global__ void __launch_bounds__(THREADS, MINB) fft_pipe_kernel(const PassArgs<T> a) {
     using V = cx<T>;
     using G = TileGeom<MODE, B, PLAN::N>;
@@ -471,6 +525,7 @@ __global__ void __launch_bounds__(THREADS, MINB) fft_pipe_kernel(const PassArgs<
     constexpr int TWN = PLAN::twtotal();
     static_assert(PLAN::S >= 2, "the pipelined kernel needs at least two stages");
     static_assert(MODE != MODE_BATCH || THREADS % B == 0, "batch mode needs THREADS % B == 0");
+    static_assert(LPT == 1, "the pipelined kernel moves one line per thread");
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V* buf0 = reinterpret_cast<V*>(smem_raw);
@@ -499,7 +554,7 @@ __global__ void __launch_bounds__(THREADS, MINB) fft_pipe_kernel(const PassArgs<
         cp_async_commit();
         cp_async_wait<1>();  // this thread's copies of tile t have landed
         __syncthreads();     // ... and every other thread's
-        run_stage<T, PLAN, B, THREADS, MODE, INV, 0>(a, cur, tw, offA_s, cbase, tid);
+        run_stage<T, PLAN, B, THREADS, MODE, INV, 1, 0>(a, cur, tw, offA_s, cbase, tid);
         __syncthreads();     // `cur` and `cbase` are free for the copies issued next iteration
     }
     cp_async_wait<0>();
