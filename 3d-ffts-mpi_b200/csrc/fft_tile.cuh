@@ -42,6 +42,7 @@ template <> struct RealOf<float4> { using type = float; };
 
 template <typename V>
 __host__ __device__ __forceinline__ V mk(typename RealOf<V>::type re, typename RealOf<V>::type im) {
+    static_assert(sizeof(V) == 2 * sizeof(typename RealOf<V>::type), "mk builds one complex value");
     V v;
     v.x = re;
     v.y = im;
@@ -61,11 +62,6 @@ template <typename V>
 __device__ __forceinline__ V cmul(V a, typename RealOf<V>::type c, typename RealOf<V>::type s) {
     return mk<V>(a.x * c - a.y * s, a.x * s + a.y * c);
 }
-// a * w, or a * conj(w)
-template <bool CONJ, typename V, typename W> __device__ __forceinline__ V cmulw(V a, W w) {
-    return CONJ ? cmul(a, w.x, -w.y) : cmul(a, w.x, w.y);
-}
-
 // line-pair (float4) versions of the complex operations
 __device__ __forceinline__ float4 add(float4 a, float4 b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
 __device__ __forceinline__ float4 sub(float4 a, float4 b) { return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w); }
@@ -75,6 +71,11 @@ __device__ __forceinline__ float4 mul_mi(float4 a) { return make_float4(a.y, -a.
 __device__ __forceinline__ float4 scl(float4 a, float s) { return make_float4(a.x * s, a.y * s, a.z * s, a.w * s); }
 __device__ __forceinline__ float4 cmul(float4 a, float c, float s) {
     return make_float4(a.x * c - a.y * s, a.x * s + a.y * c, a.z * c - a.w * s, a.z * s + a.w * c);
+}
+
+// a * w, or a * conj(w)
+template <bool CONJ, typename V, typename W> __device__ __forceinline__ V cmulw(V a, W w) {
+    return CONJ ? cmul(a, w.x, -w.y) : cmul(a, w.x, w.y);
 }
 
 // element a thread moves per (tile line, n): one complex, or for LPT = 2 the
