@@ -152,7 +152,6 @@ def test_every_launch_variant(pkg, oracle, cuda, P, shape, prec):
             f.inverse(x)
             assert oracle.rel_l2(x.cpu().numpy(), x0.cpu().numpy()) <= tol, f"pass {p} variant {v} round trip"
             tested += 1
-        f.select_variant(p, 0)
     assert tested >= 3
 
 
