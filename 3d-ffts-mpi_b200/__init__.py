@@ -222,6 +222,12 @@ class a2adfft:
     def set_autotune(self, enable: bool) -> None:
         call("a2a_dfft_set_autotune", self._h, int(bool(enable)))
 
+    def check_device(self) -> None:
+        """Raise A2AError(A2A_ERROR_TIMEOUT) if a pass kernel gave up a
+        bounded wait since the last check (after async calls: synchronise
+        first)."""
+        call("a2a_dfft_check_device", self._h)
+
     def variant_count(self, pass_index: int) -> int:
         n = ctypes.c_int()
         call("a2a_dfft_variant_count", self._h, int(pass_index), ctypes.byref(n))

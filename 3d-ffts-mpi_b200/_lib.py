@@ -75,6 +75,7 @@ SIGNATURES = {
     "a2a_dfft_make_plans": [_P, _PP],
     "a2a_dfft_set_autotune": [_P, _I],
     "a2a_dfft_variant_count": [_P, _I, ctypes.POINTER(_I)],
+    "a2a_dfft_check_device": [_P],
     "a2a_dfft_select_variant": [_P, _I, _I],
     "a2a_dfft_plan_report": [_P, ctypes.c_char_p, ctypes.c_size_t],
     "a2a_dfft_forward": [_P, _PP],

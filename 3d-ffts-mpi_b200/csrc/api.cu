@@ -119,7 +119,8 @@ SlotGeom slot_geom(const Dist& d, int slot) {
 bool variant_fits(const Dist& d, const SlotGeom& g, const PassKernel& k) {
     if (g.NV % k.lines) return false;
     int vec = 1;  // lines per 16-byte access
-    if (k.kind == a2a::KIND_PIPE && g.mode == a2a::MODE_BATCH) vec = k.lines;
+    if ((k.kind == a2a::KIND_PIPE || k.kind == a2a::KIND_TMA) && g.mode == a2a::MODE_BATCH) vec = k.lines;
+    if (k.kind == a2a::KIND_TMA && g.mode != a2a::MODE_BATCH) return false;
     if (k.lpt > 1) vec = k.lpt;
     if (k.lpt > 1 && g.mode != a2a::MODE_BATCH) return false;
     if (vec == 1) return true;
@@ -186,7 +187,7 @@ a2a_status finish(const Dist& d, cudaStream_t st, bool sync) {
 template <typename T>
 cudaError_t launch_pass_t(const PassKernel& k, unsigned grid, const void* src, void* dst, const uint32_t* offA,
                           const uint32_t* offU, const uint32_t* offV, const void* tw, int NU, int NV, double scale,
-                          int split, cudaStream_t st) {
+                          int split, int* err, cudaStream_t st) {
     a2a::PassArgs<T> a;
     a.src = static_cast<const a2a::cx<T>*>(src);
     a.dst = static_cast<a2a::cx<T>*>(dst);
@@ -198,6 +199,7 @@ cudaError_t launch_pass_t(const PassKernel& k, unsigned grid, const void* src, v
     a.NV = NV;
     a.scale = T(scale);
     a.split = split;
+    a.err = err;
     void* args[] = {&a};
     return cudaLaunchKernel(k.fn, dim3(grid), dim3(k.threads), args, k.smem, st);
 }
@@ -209,7 +211,7 @@ cudaError_t launch_slot(const Dist& d, int slot, bool inv, int c, void* p, doubl
     const SlotGeom g = slot_geom(d, slot);
     const uint64_t tiles = (uint64_t)g.NU * (g.NV / k.lines);
     uint64_t grid = tiles;
-    if (k.kind == a2a::KIND_PIPE) {
+    if (k.kind == a2a::KIND_PIPE || k.kind == a2a::KIND_TMA) {
         const uint64_t resident = (uint64_t)std::max(ps.occ[c], 1) * d.sms;
         grid = std::min(tiles, resident);
     }
@@ -218,8 +220,9 @@ cudaError_t launch_slot(const Dist& d, int slot, bool inv, int c, void* p, doubl
     const int split = split_ok(l, k);
     if (d.prec == A2A_C128)
         return launch_pass_t<double>(k, unsigned(grid), p, p, g.offA, g.offU, g.offV, g.tw, g.NU, g.NV, scale, split,
-                                     st);
-    return launch_pass_t<float>(k, unsigned(grid), p, p, g.offA, g.offU, g.offV, g.tw, g.NU, g.NV, scale, split, st);
+                                     d.d_err, st);
+    return launch_pass_t<float>(k, unsigned(grid), p, p, g.offA, g.offU, g.offV, g.tw, g.NU, g.NV, scale, split,
+                                d.d_err, st);
 }
 
 a2a_status setup_distribution(Dist& d, int nx, int ny, int nz, int P, int block_size, a2a_precision prec) {
@@ -275,12 +278,15 @@ a2a_status setup_distribution(Dist& d, int nx, int ny, int nz, int P, int block_
     for (int u = 0; u < nx; ++u) h.push_back(uint32_t((uint64_t)u * nx * nx));
     pos[5] = h.size();
     for (int v = 0; v < nx; ++v) h.push_back(uint32_t((uint64_t)v * nx));
+    const size_t err_pos = h.size();
+    h.push_back(0u);  // device error flag (bounded waits that gave up)
     A2A_CUDA(cudaMalloc(&d.d_tables, h.size() * sizeof(uint32_t)), "cudaMalloc(tables)");
     A2A_CUDA(cudaMemcpy(d.d_tables, h.data(), h.size() * sizeof(uint32_t), cudaMemcpyHostToDevice), "cudaMemcpy");
     for (int a = 0; a < 3; ++a) d.off[a] = d.d_tables + pos[a];
     d.iota = d.d_tables + pos[3];
     d.pen_u = d.d_tables + pos[4];
     d.pen_v = d.d_tables + pos[5];
+    d.d_err = reinterpret_cast<int*>(d.d_tables + err_pos);
 
     for (int a = 0; a < 3; ++a) d.h_off[a].assign(h.begin() + pos[a], h.begin() + pos[a + 1]);
 
@@ -411,13 +417,25 @@ a2a_status check_dfft(a2a_dfft* f, void** data) {
     return check_buf(data, "d_data");
 }
 
+// Reads and clears the device error flag (a bounded wait in a kernel gave up).
+a2a_status check_device_flag(const Dist& d) {
+    int flag = 0;
+    A2A_CUDA(cudaMemcpy(&flag, d.d_err, sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy(error flag)");
+    if (flag) {
+        A2A_CUDA(cudaMemset(d.d_err, 0, sizeof(int)), "cudaMemset(error flag)");
+        return fail(A2A_ERROR_TIMEOUT, "a pass kernel's bounded wait for its tile copies gave up");
+    }
+    return A2A_SUCCESS;
+}
+
 // The fused transform: Z, X then Y pass.
 a2a_status fused(a2a_dfft* f, void** data, bool inv, cudaStream_t st, bool sync) {
     a2a_status s;
     if ((s = check_dfft(f, data)) != A2A_SUCCESS) return s;
     const Dist& d = f->dist->d;
     for (int pass = 0; pass < 3; ++pass) A2A_CUDA(run_pass(d, pass, inv, data[0], st), "axis pass launch");
-    return finish(d, st, sync);
+    if ((s = finish(d, st, sync)) != A2A_SUCCESS) return s;
+    return sync ? check_device_flag(d) : A2A_SUCCESS;
 }
 
 template <typename F> a2a_status step(a2a_distribution* h, void** b1, void** b2, F&& body) {
@@ -649,6 +667,11 @@ a2a_status a2a_dfft_make_plans(a2a_dfft* f, void** d_scratch) {
     return A2A_SUCCESS;
 }
 
+a2a_status a2a_dfft_check_device(const a2a_dfft* f) {
+    if (!f) return fail(A2A_ERROR_INVALID_VALUE, "dfft is NULL");
+    return check_device_flag(f->dist->d);
+}
+
 a2a_status a2a_dfft_variant_count(const a2a_dfft* f, int pass, int* count) {
     if (!f || !count) return fail(A2A_ERROR_INVALID_VALUE, "NULL argument");
     if (pass < 0 || pass > 2) return fail(A2A_ERROR_INVALID_VALUE, "pass must be 0 (Z), 1 (X) or 2 (Y)");
@@ -688,7 +711,7 @@ a2a_status a2a_dfft_plan_report(const a2a_dfft* f, char* buf, size_t len) {
             snprintf(line, sizeof line,
                      "%s pass n=%d %s lines=%d lpt=%d threads=%d smem=%zu occ=%d radix=%d,%d,%d,%d fits=%d "
                      "tuned_ms=%.4f%s\n",
-                     names[p], k.n, k.kind == a2a::KIND_PIPE ? "pipe" : "direct", k.lines, k.lpt, k.threads, k.smem,
+                     names[p], k.n, k.kind == a2a::KIND_PIPE ? "pipe" : k.kind == a2a::KIND_TMA ? "tma" : "direct", k.lines, k.lpt, k.threads, k.smem,
                      ps.occ[c], k.radix[0], k.radix[1], k.radix[2], k.radix[3], (int)ps.fits[c], ps.tuned_ms[c],
                      c == ps.chosen ? " <- chosen" : "");
             out += line;

@@ -92,6 +92,8 @@ A2A_PLANS(double)
     X(float,  192, KIND_DIRECT,  4,  64, 1, 1)         \
     X(float,  256, KIND_DIRECT, 16, 256, 2, 1)         \
     X(float,  256, KIND_DIRECT, 32, 256, 1, 2)         \
+    X(float,  256, KIND_TMA,    16, 256, 2, 1)         \
+    X(float,  256, KIND_TMA,    32, 512, 1, 1)         \
     X(float,  256, KIND_DIRECT, 16, 128, 4, 2)         \
     X(float,  256, KIND_DIRECT, 32, 256, 1, 1)         \
     X(float,  256, KIND_PIPE,   16, 256, 2, 1)         \
@@ -102,6 +104,9 @@ A2A_PLANS(double)
     X(float,  384, KIND_DIRECT,  4,  64, 1, 1)         \
     X(float,  512, KIND_DIRECT, 16, 512, 1, 2)         \
     X(float,  512, KIND_DIRECT,  8, 128, 4, 1)         \
+    X(float,  512, KIND_TMA,    16, 512, 1, 2)         \
+    X(float,  512, KIND_TMA,    16, 256, 1, 2)         \
+    X(float,  512, KIND_TMA,     8, 256, 2, 2)         \
     X(float,  512, KIND_DIRECT, 16, 256, 2, 2)         \
     X(float,  512, KIND_DIRECT, 16, 256, 2, 1)         \
     X(float,  512, KIND_DIRECT,  8, 128, 4, 2)         \
@@ -113,6 +118,7 @@ A2A_PLANS(double)
     X(float,  768, KIND_PIPE,    8, 384, 1, 1)         \
     X(float,  768, KIND_DIRECT,  4, 128, 1, 1)         \
     X(float, 1024, KIND_DIRECT, 16, 512, 1, 2)         \
+    X(float, 1024, KIND_TMA,     8, 512, 1, 1)         \
     X(float, 1024, KIND_DIRECT,  8, 256, 1, 1)         \
     X(float, 1024, KIND_DIRECT,  8, 256, 1, 2)         \
     X(float, 1024, KIND_DIRECT,  8, 512, 1, 1)         \
@@ -153,6 +159,7 @@ A2A_PLANS(double)
     X(double,  384, KIND_PIPE,    8, 384, 1, 1)        \
     X(double,  384, KIND_DIRECT,  4, 128, 1, 1)        \
     X(double,  512, KIND_DIRECT,  8, 256, 1, 1)        \
+    X(double,  512, KIND_TMA,     8, 256, 1, 1)        \
     X(double,  512, KIND_DIRECT,  8, 512, 1, 1)        \
     X(double,  512, KIND_PIPE,    8, 512, 1, 1)        \
     X(double,  512, KIND_DIRECT,  4, 128, 1, 1)        \
@@ -168,6 +175,8 @@ PassKernel make_pass_kernel() {
     PassKernel k;
     if constexpr (KIND == KIND_PIPE)
         k.fn = reinterpret_cast<const void*>(&fft_pipe_kernel<T, P, B, TH, MODE, INV, MB, LPT>);
+    else if constexpr (KIND == KIND_TMA)
+        k.fn = reinterpret_cast<const void*>(&fft_tma_kernel<T, P, B, TH, MODE, INV, MB, LPT>);
     else
         k.fn = reinterpret_cast<const void*>(&fft_pass_kernel<T, P, B, TH, MODE, INV, MB, LPT>);
     k.kind = KIND;
@@ -183,12 +192,12 @@ PassKernel make_pass_kernel() {
     return k;
 }
 
-// A variant with LPT = 2 exists only for the batch mode (line pairs); in line
-// mode the lookup skips it.
+// Line pairs (LPT = 2) and TMA row copies exist only for the batch mode; in
+// line mode the lookup skips those variants.
 template <typename T, int N, int KIND, int B, int TH, int MB, int LPT>
 bool make_variant(int mode, bool inv, PassKernel* out) {
     if (mode == MODE_LINE) {
-        if constexpr (LPT != 1) {
+        if constexpr (LPT != 1 || KIND == KIND_TMA) {
             return false;
         } else {
             *out = inv ? make_pass_kernel<T, N, KIND, B, TH, MB, 1, MODE_LINE, true>()
@@ -206,6 +215,6 @@ bool make_variant(int mode, bool inv, PassKernel* out) {
 int find_pass_kernels_f32(int n, int mode, bool inverse, PassKernel* out, int max);
 int find_pass_kernels_f64(int n, int mode, bool inverse, PassKernel* out, int max);
 
-constexpr int kMaxVariants = 8;
+constexpr int kMaxVariants = 12;
 
 }  // namespace a2a

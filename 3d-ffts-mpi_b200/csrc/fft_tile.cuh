@@ -246,6 +246,7 @@ template <typename T> struct PassArgs {
     // (the brick extent along the axis and N/R divide one another): addresses
     // are then one table value per butterfly plus CTA-uniform deltas
     int split;
+    int* err;              // set to 1 by a kernel whose bounded wait gave up
 };
 
 // Butterfly q of a stage -> (tile line b, butterfly j), NBL butterflies per
@@ -262,12 +263,17 @@ template <bool BFAST, int B, int NBL> __device__ __forceinline__ void bf_map(int
     }
 }
 
-// Shared-memory layout of one tile of BV vector lines.  BATCH: [n][bv]
-// (lines fastest).  LINE: line b at b*LS, element n at n + n/32 (one pad
-// slot per 32 elements keeps strided butterfly writes spread over the banks);
-// LS is odd, so lanes that walk across lines hit distinct banks.
-template <int MODE, int BV, int N> struct TileGeom {
-    static constexpr int LS = (N + N / 32) | 1;
+// Shared-memory layout of one tile of BV vector lines of ESZ-byte elements.
+// BATCH: [n][bv] (lines fastest).  LINE: line b at b*LS, element n at
+// n + n/32 (one pad slot per 32 elements spreads strided butterfly writes over
+// the banks).  LS is chosen so that a warp walking across lines -- BV lines
+// times 32/BV consecutive elements -- covers every bank evenly:
+// LS == 32/BV modulo the number of elements per 128-byte bank row.
+template <int MODE, int BV, int N, int ESZ> struct TileGeom {
+    static constexpr int SLOTS = 128 / ESZ;
+    static constexpr int LS0 = N + N / 32;
+    static constexpr int WANT = (32 / BV) % SLOTS;
+    static constexpr int LS = LS0 + ((WANT - LS0 % SLOTS) % SLOTS + SLOTS) % SLOTS;
     static constexpr int elems = (MODE == MODE_BATCH) ? N * BV : BV * LS;
     static __device__ __forceinline__ int idx(int b, int n) {
         if constexpr (MODE == MODE_BATCH)
@@ -302,7 +308,7 @@ __device__ __forceinline__ void run_stage(const PassArgs<T>& a, typename ElemOf<
                                           const cx<T>* tw, const uint32_t* offA_s, const size_t* base_s, int tid) {
     using E = typename ElemOf<T, LPT>::type;
     constexpr int BV = B / LPT;
-    using G = TileGeom<MODE, BV, PLAN::N>;
+    using G = TileGeom<MODE, BV, PLAN::N, sizeof(E)>;
     constexpr int N = PLAN::N;
     constexpr int R = PLAN::r[s];
     constexpr int NS = PLAN::ns(s);
@@ -370,20 +376,24 @@ __device__ __forceinline__ void run_stage(const PassArgs<T>& a, typename ElemOf<
 
 enum PassKind : int {
     KIND_DIRECT = 0,  // one tile per CTA, stage 0 loads global memory into registers
-    KIND_PIPE = 1     // persistent CTAs, next tile prefetched into shared memory
+    KIND_PIPE = 1,    // persistent CTAs, next tile prefetched into shared memory (LDGSTS)
+    KIND_TMA = 2      // persistent CTAs, tile rows fetched by TMA bulk copies, mbarrier completion
 };
+
+constexpr int kTmaBuffers = 2;
 
 template <typename T, class PLAN, int B, int MODE, int KIND, int LPT>
 __host__ __device__ constexpr size_t pass_smem_bytes() {
     using E = typename ElemOf<T, LPT>::type;
     constexpr int N = PLAN::N;
     constexpr int BV = B / LPT;
-    constexpr int NBUF = KIND == KIND_PIPE ? 2 : 1;
-    size_t bytes = sizeof(E) * (size_t)(NBUF * TileGeom<MODE, BV, N>::elems);
+    constexpr int NBUF = KIND == KIND_PIPE ? 2 : KIND == KIND_TMA ? kTmaBuffers : 1;
+    size_t bytes = sizeof(E) * (size_t)(NBUF * TileGeom<MODE, BV, N, sizeof(E)>::elems);
     bytes += sizeof(cx<T>) * (size_t)PLAN::twtotal();
     bytes += sizeof(uint32_t) * (size_t)N;
     bytes = (bytes + 15) & ~size_t(15);
     bytes += sizeof(size_t) * (size_t)(NBUF * BV);
+    if (KIND == KIND_TMA) bytes += sizeof(unsigned long long) * NBUF;  // mbarriers
     return bytes;
 }
 
@@ -395,7 +405,7 @@ template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV, int MI
 __global__ void __launch_bounds__(THREADS, MINB) fft_pass_kernel(const PassArgs<T> a) {
     using E = typename ElemOf<T, LPT>::type;
     constexpr int BV = B / LPT;
-    using G = TileGeom<MODE, BV, PLAN::N>;
+    using G = TileGeom<MODE, BV, PLAN::N, sizeof(E)>;
     constexpr int N = PLAN::N;
     constexpr int R0 = PLAN::r[0];
     constexpr int NBL = N / R0;
@@ -488,7 +498,7 @@ template <typename T, class PLAN, int B, int THREADS, int MODE>
 __device__ __forceinline__ void pipe_issue(const PassArgs<T>& a, int t, int tilesV, cx<T>* buf, size_t* base_s,
                                            int tid) {
     using V = cx<T>;
-    using G = TileGeom<MODE, B, PLAN::N>;
+    using G = TileGeom<MODE, B, PLAN::N, sizeof(V)>;
     constexpr int N = PLAN::N;
     const int u = t / tilesV;
     const int v0 = (t - u * tilesV) * B;
@@ -521,7 +531,7 @@ __device__ __forceinline__ void pipe_issue(const PassArgs<T>& a, int t, int tile
 template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV, int MINB, int LPT>
 __global__ void __launch_bounds__(THREADS, MINB) fft_pipe_kernel(const PassArgs<T> a) {
     using V = cx<T>;
-    using G = TileGeom<MODE, B, PLAN::N>;
+    using G = TileGeom<MODE, B, PLAN::N, sizeof(V)>;
     constexpr int N = PLAN::N;
     constexpr int TWN = PLAN::twtotal();
     static_assert(PLAN::S >= 2, "the pipelined kernel needs at least two stages");
@@ -559,6 +569,140 @@ __global__ void __launch_bounds__(THREADS, MINB) fft_pipe_kernel(const PassArgs<
         __syncthreads();     // `cur` and `cbase` are free for the copies issued next iteration
     }
     cp_async_wait<0>();
+}
+
+// ---------------------------------------------------------------------------
+// TMA bulk-copy pipeline (BATCH mode).  Every tile row -- B contiguous lines
+// at one index n, B * sizeof(complex) bytes -- is one cp.async.bulk from
+// global into shared memory, completing on the tile buffer's mbarrier; one
+// warp issues all of a tile's rows.  Persistent CTAs keep kTmaBuffers tiles in
+// flight, so the fetch of later tiles overlaps the butterflies of the current
+// one without occupying L1 miss slots or the load/store queue.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, uint32_t bytes) {
+    asm volatile(
+        "{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}\n" ::"r"(smem_u32(bar)),
+        "r"(bytes)
+        : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+    return t;
+}
+// Wait for the given phase parity of an mbarrier, giving up after about half
+// a second (or 2^22 polls): returns false then.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, uint32_t parity) {
+    const uint64_t t0 = global_ns();
+    for (int i = 0; i < (1 << 22); ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(smem_u32(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if ((i & 1023) == 1023 && global_ns() - t0 > 500000000ull) return false;
+    }
+    return false;
+}
+
+template <typename T, class PLAN, int B, int THREADS, int LPT>
+__device__ __forceinline__ void tma_issue(const PassArgs<T>& a, int t, int tilesV, typename ElemOf<T, LPT>::type* buf,
+                                          size_t* base_s, unsigned long long* bar, int tid) {
+    using E = typename ElemOf<T, LPT>::type;
+    constexpr int BV = B / LPT;
+    constexpr int N = PLAN::N;
+    constexpr uint32_t ROW = B * sizeof(cx<T>);
+    const int u = t / tilesV;
+    const int v0 = (t - u * tilesV) * B;
+    const size_t ubase = __ldg(a.offU + u);
+    for (int b = tid; b < BV; b += THREADS) base_s[b] = ubase + __ldg(a.offV + v0 + b * LPT);
+    if (tid < 32) {
+        if (tid == 0) {
+            fence_proxy_async_smem();  // earlier generic reads of buf are ordered before the async writes
+            mbar_arrive_expect_tx(bar, ROW * N);
+        }
+        __syncwarp();
+        const cx<T>* row0 = a.src + ubase + __ldg(a.offV + v0);
+        for (int n = tid; n < N; n += 32) bulk_g2s(buf + n * BV, row0 + __ldg(a.offA + n), ROW, bar);
+    }
+}
+
+template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV, int MINB, int LPT>
+__global__ void __launch_bounds__(THREADS, MINB) fft_tma_kernel(const PassArgs<T> a) {
+    using E = typename ElemOf<T, LPT>::type;
+    constexpr int BV = B / LPT;
+    using G = TileGeom<MODE_BATCH, BV, PLAN::N, sizeof(E)>;
+    constexpr int N = PLAN::N;
+    constexpr int TWN = PLAN::twtotal();
+    constexpr int NBUF = kTmaBuffers;
+    static_assert(MODE == MODE_BATCH, "TMA tiles move whole rows of contiguous lines");
+    static_assert(PLAN::S >= 2, "the pipelined kernel needs at least two stages");
+    static_assert(THREADS % BV == 0, "batch mode needs THREADS % (B/LPT) == 0");
+    static_assert((B * sizeof(cx<T>)) % 16 == 0, "bulk copies move multiples of 16 bytes");
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    E* buf = reinterpret_cast<E*>(smem_raw);
+    cx<T>* tw = reinterpret_cast<cx<T>*>(buf + NBUF * G::elems);
+    uint32_t* offA_s = reinterpret_cast<uint32_t*>(tw + TWN);
+    size_t* base_s = reinterpret_cast<size_t*>(
+        smem_raw +
+        ((sizeof(E) * (size_t)(NBUF * G::elems) + sizeof(cx<T>) * TWN + sizeof(uint32_t) * N + 15) & ~size_t(15)));
+    unsigned long long* bar = reinterpret_cast<unsigned long long*>(base_s + NBUF * BV);
+
+    const int tid = threadIdx.x;
+    const int tilesV = a.NV / B;
+    const int ntiles = a.NU * tilesV;
+    if (tid == 0) {
+        for (int i = 0; i < NBUF; ++i) mbar_init(bar + i, 1);
+        fence_mbar_init();
+    }
+    for (int i = tid; i < TWN; i += THREADS) tw[i] = a.tw[i];
+    for (int i = tid; i < N; i += THREADS) offA_s[i] = a.offA[i];
+    __syncthreads();
+    for (int i = 0; i < NBUF; ++i) {
+        const int ti = blockIdx.x + i * gridDim.x;
+        if (ti < ntiles)
+            tma_issue<T, PLAN, B, THREADS, LPT>(a, ti, tilesV, buf + i * G::elems, base_s + i * BV, bar + i, tid);
+    }
+    __syncthreads();  // line bases visible to every thread
+    int it = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
+        const int slot = it % NBUF;
+        const bool ok = mbar_wait_bounded(bar + slot, (uint32_t)((it / NBUF) & 1));
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) atomicExch(a.err, 1);
+            return;
+        }
+        run_stage<T, PLAN, B, THREADS, MODE_BATCH, INV, LPT, 0>(a, buf + slot * G::elems, tw, offA_s,
+                                                               base_s + slot * BV, tid);
+        __syncthreads();  // buffer `slot` and its line bases are free again
+        const int tn = t + NBUF * gridDim.x;
+        if (tn < ntiles)
+            tma_issue<T, PLAN, B, THREADS, LPT>(a, tn, tilesV, buf + slot * G::elems, base_s + slot * BV, bar + slot,
+                                                tid);
+        __syncthreads();  // the new line bases are visible before they are read
+    }
 }
 
 }  // namespace a2a

@@ -48,6 +48,7 @@ struct Dist {
     const uint32_t* iota = nullptr;
     const uint32_t* pen_u = nullptr;
     const uint32_t* pen_v = nullptr;
+    int* d_err = nullptr;  // set by a kernel whose bounded wait gave up
     // FP64-generated stage twiddles per axis (forward sign), in the
     // precision of the plan
     void* d_tw = nullptr;

@@ -159,6 +159,12 @@ a2a_status a2a_dfft_make_plans(a2a_dfft* dfft, void** d_scratch);
  * counterpart. */
 a2a_status a2a_dfft_set_autotune(a2a_dfft* dfft, int enable);
 
+/* Reads and clears the distribution's device error flag: A2A_ERROR_TIMEOUT
+ * when a pass kernel gave up a bounded wait for its tile copies since the
+ * last check (the synchronous transforms check it themselves; after
+ * _async calls, synchronise the stream first).  No reference counterpart. */
+a2a_status a2a_dfft_check_device(const a2a_dfft* dfft);
+
 /* Launch variants compiled for a pass (0 = Z, 1 = X, 2 = Y), and a manual
  * choice among them (overrides the default or the make_plans timing; fails
  * with A2A_ERROR_UNSUPPORTED for a variant that does not fit the pass).  No
