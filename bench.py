@@ -59,6 +59,8 @@ def parse_args():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg")
     ap.add_argument("--no-check", action="store_true", help="skip the accuracy check (profiling runs)")
+    ap.add_argument("--variants", default=None,
+                    help="Z,X,Y launch-variant indices instead of timing them all in make_plans (profiling runs)")
     return ap.parse_args()
 
 
@@ -244,10 +246,15 @@ def run_ours(args, rank, world, local_rank):
     ng, ranks = args.ng, args.ranks
     dist = pkg.a2aDistribution(ranks, ng, 64, precision="c64")
     dfft = pkg.a2adfft(dist, method=args.method)
-    scratch = dist.empty(dev)  # make_plans times the pass variants on it
-    dfft.make_plans(scratch)
+    if args.variants:
+        dfft.make_plans()
+        for p, v in enumerate(int(t) for t in args.variants.split(",")):
+            dfft.select_variant(p, v)
+    else:
+        scratch = dist.empty(dev)  # make_plans times the pass variants on it
+        dfft.make_plans(scratch)
+        del scratch
     plan_report = dfft.plan_report()
-    del scratch
     x = synth_bricks(torch, ng, dist.dims, SEED, dev)
     x0 = x.clone()
     stream = torch.cuda.Stream(device=dev)
