@@ -13,6 +13,10 @@
 #include <string>
 #include <vector>
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "fft_tc.cuh"
 #include "internal.h"
 
 using a2a::Dist;
@@ -28,6 +32,12 @@ struct a2a_dfft {
     bool plans_made = false;
     bool autotune = true;
     a2a_method method = A2A_METHOD_PLAIN;
+    // split tensor-core method: kernels per pass [Z, X, Y][inverse], twiddles
+    // of their radix plans per axis, split radix-16 operands per direction
+    PassKernel tc[3][2];
+    void* d_tc = nullptr;
+    const void* tc_tw[3] = {nullptr, nullptr, nullptr};
+    const void* tc_b[2] = {nullptr, nullptr};
 };
 
 namespace {
@@ -411,6 +421,31 @@ cudaError_t run_pass(const Dist& d, int pass, bool inv, void* p, cudaStream_t st
     return launch_slot(d, pass, inv, d.slot[pass][inv ? 1 : 0].chosen, p, scale, st);
 }
 
+// One pass of the split tensor-core method.
+cudaError_t run_tc_pass(const a2a_dfft* f, int pass, bool inv, void* p, cudaStream_t st) {
+    const Dist& d = f->dist->d;
+    const SlotGeom g = slot_geom(d, pass);
+    const int axis = pass == 0 ? 2 : pass == 1 ? 0 : 1;
+    const PassKernel& k = f->tc[pass][inv ? 1 : 0];
+    const double scale = (inv && pass == 2) ? 1.0 / ((double)d.ng[0] * d.ng[1] * d.ng[2]) : 1.0;
+    a2a::PassArgs<float> a;
+    a.src = static_cast<const float2*>(p);
+    a.dst = static_cast<float2*>(p);
+    a.offA = g.offA;
+    a.offU = g.offU;
+    a.offV = g.offV;
+    a.tw = static_cast<const float2*>(f->tc_tw[axis]);
+    a.NU = g.NU;
+    a.NV = g.NV;
+    a.scale = float(scale);
+    a.split = 0;
+    a.err = d.d_err;
+    a.tcb = f->tc_b[inv ? 1 : 0];
+    void* args[] = {&a};
+    const unsigned grid = unsigned((uint64_t)g.NU * (g.NV / k.lines));
+    return cudaLaunchKernel(k.fn, dim3(grid), dim3(k.threads), args, k.smem, st);
+}
+
 a2a_status check_dfft(a2a_dfft* f, void** data) {
     if (!f) return fail(A2A_ERROR_INVALID_VALUE, "dfft is NULL");
     if (!f->plans_made) return fail(A2A_ERROR_NO_PLANS, "make_plans has not been called");
@@ -433,7 +468,12 @@ a2a_status fused(a2a_dfft* f, void** data, bool inv, cudaStream_t st, bool sync)
     a2a_status s;
     if ((s = check_dfft(f, data)) != A2A_SUCCESS) return s;
     const Dist& d = f->dist->d;
-    for (int pass = 0; pass < 3; ++pass) A2A_CUDA(run_pass(d, pass, inv, data[0], st), "axis pass launch");
+    for (int pass = 0; pass < 3; ++pass) {
+        if (f->method == A2A_METHOD_PLAIN)
+            A2A_CUDA(run_pass(d, pass, inv, data[0], st), "axis pass launch");
+        else
+            A2A_CUDA(run_tc_pass(f, pass, inv, data[0], st), "tensor-core pass launch");
+    }
     if ((s = finish(d, st, sync)) != A2A_SUCCESS) return s;
     return sync ? check_device_flag(d) : A2A_SUCCESS;
 }
@@ -449,6 +489,95 @@ template <typename F> a2a_status step(a2a_distribution* h, void** b1, void** b2,
     cudaError_t e = body(d, b1[0], b2[0]);
     if (e != cudaSuccess) return cuda_fail(e, "pencil step launch");
     return finish(d, d.stream, true);
+}
+
+}  // namespace
+
+namespace {
+
+// Byte image of the split radix-16 operand for one direction: the real
+// 32 x 32 DFT matrix R (K x N: rows 0-15 take x_re, 16-31 x_im; columns 0-15
+// give y_re, 16-31 y_im), split as R = Rh + Rl in fp16 or bf16, stored as the
+// K-major N x K operand of the UMMA canonical no-swizzle layout: element
+// (n, k) at (k/8)*512 + (n/8)*128 + (n%8)*16 + (k%8)*2; Rh then Rl.
+void tc_operand_image(bool inverse, int fmt, std::vector<uint16_t>& img) {
+    const long double pi = acosl(-1.0L);
+    img.assign(a2a::kTcBBytes / 2, 0);
+    for (int k = 0; k < 32; ++k)
+        for (int n = 0; n < 32; ++n) {
+            const int r = k % 16, c = n % 16;
+            const long double ang = 2.0L * pi * (long double)((r * c) % 16) / 16.0L;
+            const double C = (double)cosl(ang);
+            const double S = (inverse ? 1.0 : -1.0) * (double)sinl(ang);
+            double v;
+            if (k < 16) v = n < 16 ? C : S;
+            else v = n < 16 ? -S : C;
+            uint16_t hi, lo;
+            if (fmt == a2a::TC_FP16) {
+                const __half h = __float2half_rn((float)v);
+                hi = __half_as_ushort(h);
+                lo = __half_as_ushort(__float2half_rn((float)(v - (double)__half2float(h))));
+            } else {
+                const __nv_bfloat16 h = __float2bfloat16_rn((float)v);
+                hi = __bfloat16_as_ushort(h);
+                lo = __bfloat16_as_ushort(__float2bfloat16_rn((float)(v - (double)__bfloat162float(h))));
+            }
+            const size_t off = (size_t)(k / 8) * a2a::kTcChunkB + (n / 8) * 128 + (n % 8) * 16 + (k % 8) * 2;
+            img[off / 2] = hi;
+            img[(a2a::kTcMatB + off) / 2] = lo;
+        }
+}
+
+a2a_status setup_tc(a2a_dfft* f, a2a_method m) {
+    const Dist& d = f->dist->d;
+    if (d.prec != A2A_C64) return fail(A2A_ERROR_NOT_IMPLEMENTED, "the split tensor-core methods take A2A_C64 data");
+    const int fmt = m == A2A_METHOD_SPLIT_FP16 ? a2a::TC_FP16 : a2a::TC_BF16;
+    const char* names[3] = {"Z", "X", "Y"};
+    for (int p = 0; p < 3; ++p) {
+        const SlotGeom g = slot_geom(d, p);
+        for (int inv = 0; inv < 2; ++inv)
+            if (!a2a::find_tc_kernel(g.n, g.mode, inv, fmt, &f->tc[p][inv]))
+                return fail(A2A_ERROR_NOT_IMPLEMENTED,
+                            "%s pass: no tensor-core kernel of length %d (available: 64 128 256 512 1024)", names[p],
+                            g.n);
+        if (g.NV % f->tc[p][0].lines)
+            return fail(A2A_ERROR_UNSUPPORTED, "%s pass: %d lines are not a multiple of the %d-line tile", names[p],
+                        g.NV, f->tc[p][0].lines);
+        for (int inv = 0; inv < 2; ++inv)
+            A2A_CUDA(cudaFuncSetAttribute(f->tc[p][inv].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)f->tc[p][inv].smem),
+                     "cudaFuncSetAttribute");
+    }
+    // twiddles of the tensor-core radix plans (per axis) and the operands
+    std::vector<float> tw;
+    size_t twpos[3];
+    std::vector<long double> re, im;
+    for (int axis = 0; axis < 3; ++axis) {
+        const int p = axis == 2 ? 0 : axis == 0 ? 1 : 2;
+        twpos[axis] = tw.size() / 2;
+        gen_twiddles(f->tc[p][0], re, im);
+        for (size_t i = 0; i < re.size(); ++i) {
+            tw.push_back((float)re[i]);
+            tw.push_back((float)im[i]);
+        }
+    }
+    const size_t tw_bytes = ((tw.size() * sizeof(float)) + 255) & ~size_t(255);
+    std::vector<uint16_t> b0, b1;
+    tc_operand_image(false, fmt, b0);
+    tc_operand_image(true, fmt, b1);
+    if (f->d_tc) cudaFree(f->d_tc);
+    f->d_tc = nullptr;
+    A2A_CUDA(cudaMalloc(&f->d_tc, tw_bytes + 2 * a2a::kTcBBytes), "cudaMalloc(tensor-core tables)");
+    char* base = static_cast<char*>(f->d_tc);
+    if (!tw.empty())
+        A2A_CUDA(cudaMemcpy(base, tw.data(), tw.size() * sizeof(float), cudaMemcpyHostToDevice), "cudaMemcpy");
+    A2A_CUDA(cudaMemcpy(base + tw_bytes, b0.data(), a2a::kTcBBytes, cudaMemcpyHostToDevice), "cudaMemcpy");
+    A2A_CUDA(cudaMemcpy(base + tw_bytes + a2a::kTcBBytes, b1.data(), a2a::kTcBBytes, cudaMemcpyHostToDevice),
+             "cudaMemcpy");
+    for (int axis = 0; axis < 3; ++axis) f->tc_tw[axis] = base + twpos[axis] * sizeof(float2);
+    f->tc_b[0] = base + tw_bytes;
+    f->tc_b[1] = base + tw_bytes + a2a::kTcBBytes;
+    return A2A_SUCCESS;
 }
 
 }  // namespace
@@ -600,7 +729,10 @@ a2a_status a2a_dfft_set_method(a2a_dfft* f, a2a_method m) {
     if (!f) return fail(A2A_ERROR_INVALID_VALUE, "dfft is NULL");
     if (m != A2A_METHOD_PLAIN && m != A2A_METHOD_SPLIT_BF16 && m != A2A_METHOD_SPLIT_FP16)
         return fail(A2A_ERROR_INVALID_VALUE, "unknown method %d", (int)m);
-    if (m != A2A_METHOD_PLAIN) return fail(A2A_ERROR_NOT_IMPLEMENTED, "split tensor-core methods are not built yet");
+    if (m != A2A_METHOD_PLAIN) {
+        const a2a_status s = setup_tc(f, m);
+        if (s != A2A_SUCCESS) return s;
+    }
     f->method = m;
     f->plans_made = false;
     return A2A_SUCCESS;
@@ -618,7 +750,7 @@ a2a_status a2a_dfft_make_plans(a2a_dfft* f, void** d_scratch) {
                 return fail(A2A_ERROR_UNSUPPORTED, "%s pass: no compiled tile of length %d fits %d lines", names[p],
                             ps.cand[0].n, slot_geom(d, p).NV);
         }
-    if (f->scratch && f->autotune) {
+    if (f->scratch && f->autotune && f->method == A2A_METHOD_PLAIN) {
         if (reinterpret_cast<uintptr_t>(f->scratch) % 16)
             return fail(A2A_ERROR_MISALIGNED, "d_scratch[0] is not 16-byte aligned");
         // time every fitting variant of each pass on the scratch buffer (its
@@ -717,6 +849,15 @@ a2a_status a2a_dfft_plan_report(const a2a_dfft* f, char* buf, size_t len) {
             out += line;
         }
     }
+    if (f->method != A2A_METHOD_PLAIN)
+        for (int p = 0; p < 3; ++p) {
+            const PassKernel& k = f->tc[p][0];
+            char line[256];
+            snprintf(line, sizeof line, "%s pass n=%d tensor-core %s lines=%d threads=%d smem=%zu radix=%d,%d,%d <- in use\n",
+                     names[p], k.n, f->method == A2A_METHOD_SPLIT_FP16 ? "split-fp16" : "split-bf16", k.lines, k.threads,
+                     k.smem, k.radix[0], k.radix[1], k.radix[2]);
+            out += line;
+        }
     snprintf(buf, len, "%s", out.c_str());
     return out.size() < len ? A2A_SUCCESS : fail(A2A_ERROR_INVALID_VALUE, "report truncated (%zu bytes)", out.size());
 }
@@ -739,8 +880,12 @@ a2a_status a2a_dfft_execute_pass_async(a2a_dfft* f, void** d_data, int pass, int
     a2a_status s;
     if ((s = check_dfft(f, d_data)) != A2A_SUCCESS) return s;
     if (pass < 0 || pass > 2) return fail(A2A_ERROR_INVALID_VALUE, "pass must be 0 (Z), 1 (X) or 2 (Y)");
-    A2A_CUDA(run_pass(f->dist->d, pass, inverse != 0, d_data[0], static_cast<cudaStream_t>(stream)),
-             "axis pass launch");
+    if (f->method == A2A_METHOD_PLAIN)
+        A2A_CUDA(run_pass(f->dist->d, pass, inverse != 0, d_data[0], static_cast<cudaStream_t>(stream)),
+                 "axis pass launch");
+    else
+        A2A_CUDA(run_tc_pass(f, pass, inverse != 0, d_data[0], static_cast<cudaStream_t>(stream)),
+                 "tensor-core pass launch");
     return A2A_SUCCESS;
 }
 
@@ -751,6 +896,7 @@ a2a_status a2a_dfft_launches_per_transform(const a2a_dfft* f, int* out) {
 }
 
 a2a_status a2a_dfft_destroy(a2a_dfft* f) {
+    if (f && f->d_tc) cudaFree(f->d_tc);
     delete f;
     return A2A_SUCCESS;
 }

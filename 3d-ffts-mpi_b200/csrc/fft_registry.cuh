@@ -217,4 +217,8 @@ int find_pass_kernels_f64(int n, int mode, bool inverse, PassKernel* out, int ma
 
 constexpr int kMaxVariants = 12;
 
+// fft_tc.cu: the split-precision tensor-core kernel of length n (fmt 0 =
+// fp16, 1 = bf16); false when n has none.
+bool find_tc_kernel(int n, int mode, bool inverse, int fmt, PassKernel* out);
+
 }  // namespace a2a

@@ -1,0 +1,54 @@
+// Instantiations of the split-precision tensor-core pass kernels and their
+// lookup.  Lengths whose plan ends in radix-16 stages: every stage after the
+// first is a tensor-core GEMM.
+#include "fft_tc.cuh"
+#include "internal.h"
+
+namespace a2a {
+
+template <int N> struct TcPlan;
+template <> struct TcPlan<64> { using Plan = RadixPlan<4, 16>; static constexpr int B = 32; };
+template <> struct TcPlan<128> { using Plan = RadixPlan<8, 16>; static constexpr int B = 16; };
+template <> struct TcPlan<256> { using Plan = RadixPlan<16, 16>; static constexpr int B = 16; };
+template <> struct TcPlan<512> { using Plan = RadixPlan<2, 16, 16>; static constexpr int B = 8; };
+template <> struct TcPlan<1024> { using Plan = RadixPlan<4, 16, 16>; static constexpr int B = 4; };
+
+template <int N, int MODE, bool INV, int FMT> PassKernel make_tc_kernel() {
+    using P = typename TcPlan<N>::Plan;
+    constexpr int B = TcPlan<N>::B;
+    PassKernel k;
+    k.fn = reinterpret_cast<const void*>(&fft_tc_kernel<P, B, MODE, INV, FMT>);
+    k.kind = KIND_TC;
+    k.n = N;
+    k.threads = B * N / 16;
+    k.lines = B;
+    k.min_blocks = 1;
+    k.lpt = 1;
+    k.smem = tc_smem_bytes<P, B, MODE>();
+    k.nstages = P::S;
+    for (int s = 0; s < P::S; ++s) k.radix[s] = P::r[s];
+    k.twtotal = P::twtotal();
+    return k;
+}
+
+template <int N> PassKernel tc_pick(int mode, bool inv, int fmt) {
+    if (mode == MODE_LINE) {
+        if (fmt == TC_FP16) return inv ? make_tc_kernel<N, MODE_LINE, true, TC_FP16>() : make_tc_kernel<N, MODE_LINE, false, TC_FP16>();
+        return inv ? make_tc_kernel<N, MODE_LINE, true, TC_BF16>() : make_tc_kernel<N, MODE_LINE, false, TC_BF16>();
+    }
+    if (fmt == TC_FP16) return inv ? make_tc_kernel<N, MODE_BATCH, true, TC_FP16>() : make_tc_kernel<N, MODE_BATCH, false, TC_FP16>();
+    return inv ? make_tc_kernel<N, MODE_BATCH, true, TC_BF16>() : make_tc_kernel<N, MODE_BATCH, false, TC_BF16>();
+}
+
+bool find_tc_kernel(int n, int mode, bool inverse, int fmt, PassKernel* out) {
+    switch (n) {
+        case 64: *out = tc_pick<64>(mode, inverse, fmt); return true;
+        case 128: *out = tc_pick<128>(mode, inverse, fmt); return true;
+        case 256: *out = tc_pick<256>(mode, inverse, fmt); return true;
+        case 512: *out = tc_pick<512>(mode, inverse, fmt); return true;
+        case 1024: *out = tc_pick<1024>(mode, inverse, fmt); return true;
+        default: return false;
+    }
+}
+
+}  // namespace a2a

@@ -1,0 +1,339 @@
+// Split-precision tensor-core form of the axis pass: every radix-16 stage is
+// a dense GEMM on the 5th-generation tensor cores (tcgen05.mma, kind::f16,
+// FP32 accumulators in tensor memory), the other stage (radix 2/4/8) and the
+// twiddles stay on the CUDA cores in FP32.
+//
+// One radix-16 butterfly is y = F16 x with F16 the 16-point DFT matrix.  As a
+// real GEMM row: [y_re | y_im] = [x_re | x_im] R with the 32 x 32 matrix
+//   R = [[C, S], [-S, C]],  C = cos(2 pi r k / 16),  S = -+ sin(2 pi r k / 16).
+// Operands are split into a high and a low 16-bit part (fp16 or bf16):
+// x = xh + xl after scaling each row by a power of two into [-1, 1),
+// R = Rh + Rl (generated in FP64 on the host), and the product keeps the
+// three significant terms  xh Rh + xh Rl + xl Rh  (xl Rl is below FP32
+// rounding).  The A operand of a 128-row block is [xh | xl] (K = 64, K-major,
+// no swizzle); six K = 16 MMAs (xh with Rh and Rl, xl with Rh) accumulate into
+// 32 FP32 columns of tensor memory, which each warp reads back for its 32
+// rows with tcgen05.ld.  A row is one butterfly: the thread that built row m
+// reads row m back, undoes its scale and stores the 16 outputs.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "fft_tile.cuh"
+
+namespace a2a {
+
+enum TcFormat : int { TC_FP16 = 0, TC_BF16 = 1 };
+
+// Shared-memory operand layout (UMMA canonical K-major, SWIZZLE_NONE): an
+// 8-row x 16-byte core matrix is 128 contiguous bytes; core matrices step by
+// SBO = 128 bytes along M (or N) and by LBO bytes along K.
+constexpr int kTcRows = 128;                     // M of one MMA block
+constexpr int kTcChunkA = kTcRows / 8 * 128;     // bytes of one 8-wide K chunk of A (2048)
+constexpr int kTcBlockA = 8 * kTcChunkA;         // bytes of one A block: K = 64 halves (16 KB)
+constexpr int kTcChunkB = 32 / 8 * 128;          // bytes of one K chunk of B (N = 32): 512
+constexpr int kTcMatB = 4 * kTcChunkB;           // one 32 x 32 matrix: 2 KB
+constexpr int kTcBBytes = 2 * kTcMatB;           // Rh and Rl
+
+__host__ __device__ constexpr uint64_t umma_smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | ((uint64_t)1 << 46);  // version 1, no swizzle
+}
+// kind::f16 instruction descriptor: FP32 accumulator, A/B format, both
+// K-major, N = 32, M = 128.
+__host__ __device__ constexpr uint32_t umma_idesc_f16(int fmt) {
+    return (1u << 4) | ((uint32_t)fmt << 7) | ((uint32_t)fmt << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+}
+
+template <int FMT> __device__ __forceinline__ void split16(float v, uint16_t& hi, uint16_t& lo) {
+    if constexpr (FMT == TC_FP16) {
+        const __half h = __float2half_rn(v);
+        hi = __half_as_ushort(h);
+        lo = __half_as_ushort(__float2half_rn(v - __half2float(h)));
+    } else {
+        const __nv_bfloat16 h = __float2bfloat16_rn(v);
+        hi = __bfloat16_as_ushort(h);
+        lo = __bfloat16_as_ushort(__float2bfloat16_rn(v - __bfloat162float(h)));
+    }
+}
+
+struct TcCtx {
+    unsigned char* abuf;       // A blocks (kTcBlockA bytes each)
+    uint32_t a_addr, b_addr;   // shared addresses of A and of [Rh | Rl]
+    uint32_t tmem;             // accumulator base (lane 0, column 0)
+    unsigned long long* bar;   // MMA completion
+    uint32_t phase;
+};
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)
+        : "memory");
+}
+__device__ __forceinline__ void tc_commit(unsigned long long* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, float* v) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// One radix-16 stage on the tensor cores.  THREADS == butterflies per stage;
+// thread q owns butterfly q, i.e. A row q % 128 of block q / 128.
+template <class PLAN, int B, int THREADS, int MODE, bool INV, int FMT, int s, bool SRC_GLOBAL>
+__device__ __forceinline__ void tc_stage(const PassArgs<float>& a, float2* tile, const float2* tw,
+                                         const uint32_t* offA_s, const size_t* base_s, TcCtx& ctx, int tid,
+                                         size_t ubase, int v0) {
+    using G = TileGeom<MODE, B, PLAN::N, sizeof(float2)>;
+    constexpr int N = PLAN::N;
+    constexpr int R = PLAN::r[s];
+    static_assert(R == 16, "tensor-core stages are radix 16");
+    constexpr int NS = PLAN::ns(s);
+    constexpr int NBL = N / R;
+    static_assert(B * NBL == THREADS, "one butterfly per thread in a tensor-core stage");
+    constexpr int NBLK = THREADS / kTcRows;
+    static_assert(THREADS % kTcRows == 0, "whole 128-row MMA blocks");
+    constexpr bool LAST = (s == PLAN::S - 1);
+    constexpr bool BFAST = (MODE == MODE_BATCH) || !(LAST || SRC_GLOBAL);
+    constexpr int TWO = PLAN::twoff(s);
+
+    int b, j;
+    bf_map<BFAST, B, NBL>(tid, b, j);
+    float2 x[16];
+    if constexpr (SRC_GLOBAL) {
+        const float2* line = a.src + ubase + __ldg(a.offV + v0 + b);
+#pragma unroll
+        for (int r = 0; r < 16; ++r) x[r] = ld_stream(line + __ldg(a.offA + j + r * NBL));
+    } else {
+#pragma unroll
+        for (int r = 0; r < 16; ++r) x[r] = tile[G::idx(b, j + r * NBL)];
+    }
+    const int m = j % NS;
+    if constexpr (s > 0) {
+#pragma unroll
+        for (int r = 1; r < 16; ++r) x[r] = cmulw<INV>(x[r], tw[TWO + (r - 1) * NS + m]);
+    }
+    // scale the row into [-1, 1) by a power of two
+    float mx = 0.f;
+#pragma unroll
+    for (int r = 0; r < 16; ++r) mx = fmaxf(mx, fmaxf(fabsf(x[r].x), fabsf(x[r].y)));
+    int e = 0;
+    if (mx > 0.f) frexpf(mx, &e);
+    // A row: chunks 0,1 = hi re; 2,3 = hi im; 4,5 = lo re; 6,7 = lo im
+    {
+        const int row = tid % kTcRows;
+        unsigned char* rowp = ctx.abuf + (tid / kTcRows) * kTcBlockA + (row / 8) * 128 + (row % 8) * 16;
+#pragma unroll
+        for (int part = 0; part < 4; ++part) {  // re 0..7, re 8..15, im 0..7, im 8..15
+            uint16_t h[8], l[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const int r = (part & 1) * 8 + i;
+                const float v = ldexpf((part < 2) ? x[r].x : x[r].y, -e);
+                split16<FMT>(v, h[i], l[i]);
+            }
+            uint4 hv, lv;
+            hv.x = h[0] | (uint32_t(h[1]) << 16);
+            hv.y = h[2] | (uint32_t(h[3]) << 16);
+            hv.z = h[4] | (uint32_t(h[5]) << 16);
+            hv.w = h[6] | (uint32_t(h[7]) << 16);
+            lv.x = l[0] | (uint32_t(l[1]) << 16);
+            lv.y = l[2] | (uint32_t(l[3]) << 16);
+            lv.z = l[4] | (uint32_t(l[5]) << 16);
+            lv.w = l[6] | (uint32_t(l[7]) << 16);
+            *reinterpret_cast<uint4*>(rowp + part * kTcChunkA) = hv;
+            *reinterpret_cast<uint4*>(rowp + (4 + part) * kTcChunkA) = lv;
+        }
+    }
+    fence_proxy_async_smem();  // the tensor cores read A through the async proxy
+    __syncthreads();           // all A rows written; all tile reads of this stage done
+    if (tid == 0) {
+        tc_fence_after();
+        const uint32_t idesc = umma_idesc_f16(FMT);
+#pragma unroll
+        for (int blk = 0; blk < NBLK; ++blk) {
+            const uint32_t d = ctx.tmem + blk * 32;
+            const uint32_t ab = ctx.a_addr + blk * kTcBlockA;
+            // (A K-step, B matrix, B K-step): xh Rh, xh Rl, xl Rh
+            tc_mma(d, umma_smem_desc(ab + 0 * kTcChunkA, kTcChunkA, 128),
+                   umma_smem_desc(ctx.b_addr + 0 * kTcChunkB, kTcChunkB, 128), idesc, 0);
+            tc_mma(d, umma_smem_desc(ab + 2 * kTcChunkA, kTcChunkA, 128),
+                   umma_smem_desc(ctx.b_addr + 2 * kTcChunkB, kTcChunkB, 128), idesc, 1);
+            tc_mma(d, umma_smem_desc(ab + 0 * kTcChunkA, kTcChunkA, 128),
+                   umma_smem_desc(ctx.b_addr + kTcMatB + 0 * kTcChunkB, kTcChunkB, 128), idesc, 1);
+            tc_mma(d, umma_smem_desc(ab + 2 * kTcChunkA, kTcChunkA, 128),
+                   umma_smem_desc(ctx.b_addr + kTcMatB + 2 * kTcChunkB, kTcChunkB, 128), idesc, 1);
+            tc_mma(d, umma_smem_desc(ab + 4 * kTcChunkA, kTcChunkA, 128),
+                   umma_smem_desc(ctx.b_addr + 0 * kTcChunkB, kTcChunkB, 128), idesc, 1);
+            tc_mma(d, umma_smem_desc(ab + 6 * kTcChunkA, kTcChunkA, 128),
+                   umma_smem_desc(ctx.b_addr + 2 * kTcChunkB, kTcChunkB, 128), idesc, 1);
+        }
+        tc_commit(ctx.bar);
+    }
+    const bool ok = mbar_wait_bounded(ctx.bar, ctx.phase);
+    ctx.phase ^= 1u;
+    tc_fence_after();
+    float y[32];
+    {
+        const int warp = tid / 32;
+        const uint32_t taddr = ctx.tmem + ((uint32_t)((warp % 4) * 32) << 16) + (warp / 4) * 32;
+        tc_ld32(taddr, y);
+    }
+    if (!ok && (tid % 32) == 0) atomicExch(a.err, 1);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) x[k] = make_float2(ldexpf(y[k], e), ldexpf(y[16 + k], e));
+    if constexpr (LAST) {
+        float2* line = a.dst + base_s[b];
+#pragma unroll
+        for (int r = 0; r < 16; ++r) st_stream(line + offA_s[j + r * NBL], scl(x[r], a.scale));
+    } else {
+        const int jd = (j / NS) * NS * R + m;
+#pragma unroll
+        for (int r = 0; r < 16; ++r) tile[G::idx(b, jd + r * NS)] = x[r];
+    }
+    tc_fence_before();
+    __syncthreads();  // tile written; accumulators read before the next stage's MMAs
+    if constexpr (!LAST)
+        tc_stage<PLAN, B, THREADS, MODE, INV, FMT, s + 1, false>(a, tile, tw, offA_s, base_s, ctx, tid, ubase, v0);
+}
+
+template <class PLAN, int B, int MODE>
+__host__ __device__ constexpr size_t tc_smem_bytes() {
+    constexpr int N = PLAN::N;
+    constexpr int THREADS = B * N / 16;
+    size_t bytes = sizeof(float2) * (size_t)TileGeom<MODE, B, N, sizeof(float2)>::elems;
+    bytes = (bytes + 127) & ~size_t(127);
+    bytes += (size_t)(THREADS / kTcRows) * kTcBlockA + kTcBBytes;
+    bytes += sizeof(float2) * (size_t)PLAN::twtotal();
+    bytes += sizeof(uint32_t) * (size_t)N;
+    bytes = (bytes + 15) & ~size_t(15);
+    bytes += sizeof(size_t) * (size_t)B + 16;  // line bases, mbarrier, tensor-memory address
+    return bytes;
+}
+
+// One CTA = one tile of B lines, THREADS = B N / 16.  Tensor memory:
+// 32 columns per 128-row block, allocated and freed by warp 0.
+template <class PLAN, int B, int MODE, bool INV, int FMT>
+__global__ void __launch_bounds__(B * PLAN::N / 16, 1) fft_tc_kernel(const PassArgs<float> a) {
+    constexpr int N = PLAN::N;
+    constexpr int THREADS = B * N / 16;
+    constexpr int NBLK = THREADS / kTcRows;
+    constexpr uint32_t TCOLS = NBLK <= 1 ? 32 : NBLK <= 2 ? 64 : NBLK <= 4 ? 128 : 256;
+    using G = TileGeom<MODE, B, N, sizeof(float2)>;
+    constexpr int TWN = PLAN::twtotal();
+    constexpr int R0 = PLAN::r[0];
+
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    float2* tile = reinterpret_cast<float2*>(smem_raw);
+    size_t off = (sizeof(float2) * (size_t)G::elems + 127) & ~size_t(127);
+    unsigned char* abuf = smem_raw + off;
+    off += (size_t)NBLK * kTcBlockA;
+    unsigned char* bmat = smem_raw + off;
+    off += kTcBBytes;
+    float2* tw = reinterpret_cast<float2*>(smem_raw + off);
+    off += sizeof(float2) * (size_t)TWN;
+    uint32_t* offA_s = reinterpret_cast<uint32_t*>(smem_raw + off);
+    off = (off + sizeof(uint32_t) * N + 15) & ~size_t(15);
+    size_t* base_s = reinterpret_cast<size_t*>(smem_raw + off);
+    off += sizeof(size_t) * B;
+    unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem_raw + off);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem_raw + off + 8);
+
+    const int tid = threadIdx.x;
+    const int tilesV = a.NV / B;
+    const int u = blockIdx.x / tilesV;
+    const int v0 = (blockIdx.x - u * tilesV) * B;
+    const size_t ubase = a.offU[u];
+
+    if (tid < 32) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TCOLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        fence_mbar_init();
+    }
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(a.tcb);
+        uint4* dst = reinterpret_cast<uint4*>(bmat);
+        for (int i = tid; i < kTcBBytes / 16; i += THREADS) dst[i] = src[i];
+    }
+    for (int i = tid; i < TWN; i += THREADS) tw[i] = a.tw[i];
+    for (int i = tid; i < N; i += THREADS) offA_s[i] = a.offA[i];
+    for (int i = tid; i < B; i += THREADS) base_s[i] = ubase + a.offV[v0 + i];
+    fence_proxy_async_smem();  // B operand visible to the tensor cores
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+
+    TcCtx ctx;
+    ctx.abuf = abuf;
+    ctx.a_addr = smem_u32(abuf);
+    ctx.b_addr = smem_u32(bmat);
+    ctx.tmem = *tmem_slot;
+    ctx.bar = bar;
+    ctx.phase = 0;
+
+    if constexpr (R0 == 16) {
+        tc_stage<PLAN, B, THREADS, MODE, INV, FMT, 0, true>(a, tile, tw, offA_s, base_s, ctx, tid, ubase, v0);
+    } else {
+        // stage 0 on the CUDA cores: global -> registers -> shared
+        constexpr int NBL = N / R0;
+        constexpr int NBT = B * NBL;
+        constexpr int K = (NBT + THREADS - 1) / THREADS;
+        constexpr bool EXACT = (NBT % THREADS) == 0;
+        constexpr bool BFAST0 = (MODE == MODE_BATCH);
+        float2 x[K][R0];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int q = tid + k * THREADS;
+            if (EXACT || q < NBT) {
+                int b, j;
+                bf_map<BFAST0, B, NBL>(q, b, j);
+                const float2* line = a.src + ubase + __ldg(a.offV + v0 + b);
+#pragma unroll
+                for (int r = 0; r < R0; ++r) x[k][r] = ld_stream(line + __ldg(a.offA + j + r * NBL));
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int q = tid + k * THREADS;
+            if (EXACT || q < NBT) {
+                int b, j;
+                bf_map<BFAST0, B, NBL>(q, b, j);
+                Dft<R0, INV, float2>::run(x[k]);
+#pragma unroll
+                for (int r = 0; r < R0; ++r) tile[G::idx(b, j * R0 + r)] = x[k][r];
+            }
+        }
+        __syncthreads();
+        tc_stage<PLAN, B, THREADS, MODE, INV, FMT, 1, false>(a, tile, tw, offA_s, base_s, ctx, tid, ubase, v0);
+    }
+    // every stage ends with tcgen05.wait::ld and a block barrier
+    tc_fence_after();
+    if (tid < 32)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(ctx.tmem), "r"(TCOLS)
+                     : "memory");
+}
+
+}  // namespace a2a

@@ -247,6 +247,7 @@ template <typename T> struct PassArgs {
     // are then one table value per butterfly plus CTA-uniform deltas
     int split;
     int* err;              // set to 1 by a kernel whose bounded wait gave up
+    const void* tcb;       // tensor-core kernels: the split radix-16 operand [Rh | Rl]
 };
 
 // Butterfly q of a stage -> (tile line b, butterfly j), NBL butterflies per
@@ -377,7 +378,8 @@ __device__ __forceinline__ void run_stage(const PassArgs<T>& a, typename ElemOf<
 enum PassKind : int {
     KIND_DIRECT = 0,  // one tile per CTA, stage 0 loads global memory into registers
     KIND_PIPE = 1,    // persistent CTAs, next tile prefetched into shared memory (LDGSTS)
-    KIND_TMA = 2      // persistent CTAs, tile rows fetched by TMA bulk copies, mbarrier completion
+    KIND_TMA = 2,     // persistent CTAs, tile rows fetched by TMA bulk copies, mbarrier completion
+    KIND_TC = 3       // radix-16 stages as split-precision tcgen05 GEMMs
 };
 
 constexpr int kTmaBuffers = 2;
