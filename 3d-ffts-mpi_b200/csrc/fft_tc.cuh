@@ -11,10 +11,11 @@
 // R = Rh + Rl (generated in FP64 on the host), and the product keeps the
 // three significant terms  xh Rh + xh Rl + xl Rh  (xl Rl is below FP32
 // rounding).  The A operand of a 128-row block is [xh | xl] (K = 64, K-major,
-// no swizzle); six K = 16 MMAs (xh with Rh and Rl, xl with Rh) accumulate into
-// 32 FP32 columns of tensor memory, which each warp reads back for its 32
-// rows with tcgen05.ld.  A row is one butterfly: the thread that built row m
-// reads row m back, undoes its scale and stores the 16 outputs.
+// no swizzle); six K = 16 MMAs accumulate xh Rh into 32 FP32 columns of
+// tensor memory and the corrections xh Rl + xl Rh into 32 more, which each
+// warp reads back for its 32 rows with tcgen05.ld and adds in FP32.  A row is
+// one butterfly: the thread that built row m reads row m back, undoes its
+// scale and stores the 16 outputs.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -170,36 +171,43 @@ __device__ __forceinline__ void tc_stage(const PassArgs<float>& a, float2* tile,
         const uint32_t idesc = umma_idesc_f16(FMT);
 #pragma unroll
         for (int blk = 0; blk < NBLK; ++blk) {
-            const uint32_t d = ctx.tmem + blk * 32;
+            // two accumulators per block: the main term xh Rh, and the
+            // corrections xh Rl + xl Rh (2^-11 smaller), added in FP32 after
+            // the read-back so the corrections do not share the main term's
+            // accumulator rounding
+            const uint32_t dmain = ctx.tmem + blk * 64;
+            const uint32_t dcorr = dmain + 32;
             const uint32_t ab = ctx.a_addr + blk * kTcBlockA;
-            // (A K-step, B matrix, B K-step): xh Rh, xh Rl, xl Rh
-            tc_mma(d, umma_smem_desc(ab + 0 * kTcChunkA, kTcChunkA, 128),
-                   umma_smem_desc(ctx.b_addr + 0 * kTcChunkB, kTcChunkB, 128), idesc, 0);
-            tc_mma(d, umma_smem_desc(ab + 2 * kTcChunkA, kTcChunkA, 128),
-                   umma_smem_desc(ctx.b_addr + 2 * kTcChunkB, kTcChunkB, 128), idesc, 1);
-            tc_mma(d, umma_smem_desc(ab + 0 * kTcChunkA, kTcChunkA, 128),
-                   umma_smem_desc(ctx.b_addr + kTcMatB + 0 * kTcChunkB, kTcChunkB, 128), idesc, 1);
-            tc_mma(d, umma_smem_desc(ab + 2 * kTcChunkA, kTcChunkA, 128),
-                   umma_smem_desc(ctx.b_addr + kTcMatB + 2 * kTcChunkB, kTcChunkB, 128), idesc, 1);
-            tc_mma(d, umma_smem_desc(ab + 4 * kTcChunkA, kTcChunkA, 128),
-                   umma_smem_desc(ctx.b_addr + 0 * kTcChunkB, kTcChunkB, 128), idesc, 1);
-            tc_mma(d, umma_smem_desc(ab + 6 * kTcChunkA, kTcChunkA, 128),
-                   umma_smem_desc(ctx.b_addr + 2 * kTcChunkB, kTcChunkB, 128), idesc, 1);
+            const uint64_t ah_re = umma_smem_desc(ab + 0 * kTcChunkA, kTcChunkA, 128);
+            const uint64_t ah_im = umma_smem_desc(ab + 2 * kTcChunkA, kTcChunkA, 128);
+            const uint64_t al_re = umma_smem_desc(ab + 4 * kTcChunkA, kTcChunkA, 128);
+            const uint64_t al_im = umma_smem_desc(ab + 6 * kTcChunkA, kTcChunkA, 128);
+            const uint64_t rh_re = umma_smem_desc(ctx.b_addr + 0 * kTcChunkB, kTcChunkB, 128);
+            const uint64_t rh_im = umma_smem_desc(ctx.b_addr + 2 * kTcChunkB, kTcChunkB, 128);
+            const uint64_t rl_re = umma_smem_desc(ctx.b_addr + kTcMatB + 0 * kTcChunkB, kTcChunkB, 128);
+            const uint64_t rl_im = umma_smem_desc(ctx.b_addr + kTcMatB + 2 * kTcChunkB, kTcChunkB, 128);
+            tc_mma(dmain, ah_re, rh_re, idesc, 0);
+            tc_mma(dmain, ah_im, rh_im, idesc, 1);
+            tc_mma(dcorr, ah_re, rl_re, idesc, 0);
+            tc_mma(dcorr, ah_im, rl_im, idesc, 1);
+            tc_mma(dcorr, al_re, rh_re, idesc, 1);
+            tc_mma(dcorr, al_im, rh_im, idesc, 1);
         }
         tc_commit(ctx.bar);
     }
     const bool ok = mbar_wait_bounded(ctx.bar, ctx.phase);
     ctx.phase ^= 1u;
     tc_fence_after();
-    float y[32];
+    float y[32], yc[32];
     {
         const int warp = tid / 32;
-        const uint32_t taddr = ctx.tmem + ((uint32_t)((warp % 4) * 32) << 16) + (warp / 4) * 32;
+        const uint32_t taddr = ctx.tmem + ((uint32_t)((warp % 4) * 32) << 16) + (warp / 4) * 64;
         tc_ld32(taddr, y);
+        tc_ld32(taddr + 32, yc);
     }
     if (!ok && (tid % 32) == 0) atomicExch(a.err, 1);
 #pragma unroll
-    for (int k = 0; k < 16; ++k) x[k] = make_float2(ldexpf(y[k], e), ldexpf(y[16 + k], e));
+    for (int k = 0; k < 16; ++k) x[k] = make_float2(ldexpf(y[k] + yc[k], e), ldexpf(y[16 + k] + yc[16 + k], e));
     if constexpr (LAST) {
         float2* line = a.dst + base_s[b];
 #pragma unroll
@@ -236,7 +244,7 @@ __global__ void __launch_bounds__(B * PLAN::N / 16, 1) fft_tc_kernel(const PassA
     constexpr int N = PLAN::N;
     constexpr int THREADS = B * N / 16;
     constexpr int NBLK = THREADS / kTcRows;
-    constexpr uint32_t TCOLS = NBLK <= 1 ? 32 : NBLK <= 2 ? 64 : NBLK <= 4 ? 128 : 256;
+    constexpr uint32_t TCOLS = NBLK <= 1 ? 64 : NBLK <= 2 ? 128 : NBLK <= 4 ? 256 : 512;  // 64 per block
     using G = TileGeom<MODE, B, N, sizeof(float2)>;
     constexpr int TWN = PLAN::twtotal();
     constexpr int R0 = PLAN::r[0];
