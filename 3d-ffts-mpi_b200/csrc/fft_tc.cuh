@@ -132,12 +132,15 @@ __device__ __forceinline__ void tc_stage(const PassArgs<float>& a, float2* tile,
 #pragma unroll
         for (int r = 1; r < 16; ++r) x[r] = cmulw<INV>(x[r], tw[TWO + (r - 1) * NS + m]);
     }
-    // scale the row into [-1, 1) by a power of two
+    // scale the row into [-1, 1) by a power of two: e = exponent of the largest
+    // component (as frexp would give it), scale factors built from exponent bits
     float mx = 0.f;
 #pragma unroll
     for (int r = 0; r < 16; ++r) mx = fmaxf(mx, fmaxf(fabsf(x[r].x), fabsf(x[r].y)));
-    int e = 0;
-    if (mx > 0.f) frexpf(mx, &e);
+    int e = ((__float_as_int(mx) >> 23) & 0xFF) - 126;
+    e = mx > 0.f ? min(max(e, -125), 126) : 0;
+    const float down = __int_as_float((127 - e) << 23);  // 2^-e
+    const float up = __int_as_float((127 + e) << 23);    // 2^e
     // A row: chunks 0,1 = hi re; 2,3 = hi im; 4,5 = lo re; 6,7 = lo im
     {
         const int row = tid % kTcRows;
@@ -148,7 +151,7 @@ __device__ __forceinline__ void tc_stage(const PassArgs<float>& a, float2* tile,
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
                 const int r = (part & 1) * 8 + i;
-                const float v = ldexpf((part < 2) ? x[r].x : x[r].y, -e);
+                const float v = ((part < 2) ? x[r].x : x[r].y) * down;
                 split16<FMT>(v, h[i], l[i]);
             }
             uint4 hv, lv;
@@ -207,7 +210,7 @@ __device__ __forceinline__ void tc_stage(const PassArgs<float>& a, float2* tile,
     }
     if (!ok && (tid % 32) == 0) atomicExch(a.err, 1);
 #pragma unroll
-    for (int k = 0; k < 16; ++k) x[k] = make_float2(ldexpf(y[k] + yc[k], e), ldexpf(y[16 + k] + yc[16 + k], e));
+    for (int k = 0; k < 16; ++k) x[k] = make_float2((y[k] + yc[k]) * up, (y[16 + k] + yc[16 + k]) * up);
     if constexpr (LAST) {
         float2* line = a.dst + base_s[b];
 #pragma unroll

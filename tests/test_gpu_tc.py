@@ -29,11 +29,11 @@ def run(pkg, O, cuda, P, shape, method, kind="uniform", tones=0, seed=0):
 
 
 @pytest.mark.parametrize("method", ["split_fp16", "split_bf16"])
-@pytest.mark.parametrize("P,shape", [(4, 64), (16, 128), (16, 256), (4, (64, 128, 256)), (4, (32, 1024, 64)),
-                                     (4, (1024, 32, 64)), (4, (64, 32, 1024))])
+@pytest.mark.parametrize("P,shape", [(4, 64), (16, 128), (16, 256), (4, (64, 128, 256)), (4, (64, 1024, 64)),
+                                     (4, (1024, 64, 64)), (4, (64, 64, 1024))])
 def test_split_vs_fp64_oracle(pkg, oracle, cuda, P, shape, method):
     g, fwd, inv, f = run(pkg, oracle, cuda, P, shape, method)
-    ref = oracle.fft3_global(g)
+    ref = oracle.fft3_global(g, lines=oracle.dft_lines if g.size <= 2 ** 22 else oracle.fft_lines)
     ef, ei = oracle.rel_l2(fwd, ref), oracle.rel_l2(inv, g)
     assert ef <= TOL[method], f"forward rel L2 {ef:.3e}"
     assert ei <= 2 * TOL[method], f"round trip rel L2 {ei:.3e}"
