@@ -156,7 +156,6 @@ A2A_PLANS(double)
     X(double,  256, KIND_PIPE,    8, 256, 1, 1)        \
     X(double,  256, KIND_DIRECT,  4,  64, 1, 1)        \
     X(double,  384, KIND_DIRECT,  8, 256, 1, 1)        \
-    X(double,  384, KIND_PIPE,    8, 384, 1, 1)        \
     X(double,  384, KIND_DIRECT,  4, 128, 1, 1)        \
     X(double,  512, KIND_DIRECT,  8, 256, 1, 1)        \
     X(double,  512, KIND_TMA,     8, 256, 1, 1)        \

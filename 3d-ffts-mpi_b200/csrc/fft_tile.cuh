@@ -265,22 +265,24 @@ template <bool BFAST, int B, int NBL> __device__ __forceinline__ void bf_map(int
 }
 
 // Shared-memory layout of one tile of BV vector lines of ESZ-byte elements.
-// BATCH: [n][bv] (lines fastest).  LINE: line b at b*LS, element n at
-// n + n/32 (one pad slot per 32 elements spreads strided butterfly writes over
-// the banks).  LS is chosen so that a warp walking across lines -- BV lines
-// times 32/BV consecutive elements -- covers every bank evenly:
-// LS == 32/BV modulo the number of elements per 128-byte bank row.
+// A shared access of SLOTS = 128/ESZ lanes (a half warp for 8-byte, a quarter
+// warp for 16-byte elements) is one wavefront when its lanes hit distinct
+// 128-byte bank rows' slots.  BATCH: [n][bv] (lines fastest).  LINE: line b at
+// b*LS, element n at n + n/SLOTS: the pad slot per SLOTS elements makes the
+// stride-R butterfly writes of radix 2..SLOTS land in distinct slots, and
+// LS == SLOTS/BV (mod SLOTS) makes a wavefront that walks across the BV lines
+// (SLOTS/BV consecutive elements each) distinct as well.
 template <int MODE, int BV, int N, int ESZ> struct TileGeom {
     static constexpr int SLOTS = 128 / ESZ;
-    static constexpr int LS0 = N + N / 32;
-    static constexpr int WANT = (32 / BV) % SLOTS;
+    static constexpr int LS0 = N + N / SLOTS;
+    static constexpr int WANT = (SLOTS / (BV < SLOTS ? BV : SLOTS)) % SLOTS;
     static constexpr int LS = LS0 + ((WANT - LS0 % SLOTS) % SLOTS + SLOTS) % SLOTS;
     static constexpr int elems = (MODE == MODE_BATCH) ? N * BV : BV * LS;
     static __device__ __forceinline__ int idx(int b, int n) {
         if constexpr (MODE == MODE_BATCH)
             return n * BV + b;
         else
-            return b * LS + n + (n >> 5);
+            return b * LS + n + n / SLOTS;
     }
 };
 
