@@ -221,7 +221,7 @@ cudaError_t launch_slot(const Dist& d, int slot, bool inv, int c, void* p, doubl
     const SlotGeom g = slot_geom(d, slot);
     const uint64_t tiles = (uint64_t)g.NU * (g.NV / k.lines);
     uint64_t grid = tiles;
-    if (k.kind == a2a::KIND_PIPE || k.kind == a2a::KIND_TMA) {
+    if (k.kind == a2a::KIND_PIPE || k.kind == a2a::KIND_TMA || k.kind == a2a::KIND_RPIPE) {
         const uint64_t resident = (uint64_t)std::max(ps.occ[c], 1) * d.sms;
         grid = std::min(tiles, resident);
     }
@@ -843,7 +843,9 @@ a2a_status a2a_dfft_plan_report(const a2a_dfft* f, char* buf, size_t len) {
             snprintf(line, sizeof line,
                      "%s pass n=%d %s lines=%d lpt=%d threads=%d smem=%zu occ=%d radix=%d,%d,%d,%d fits=%d "
                      "tuned_ms=%.4f%s\n",
-                     names[p], k.n, k.kind == a2a::KIND_PIPE ? "pipe" : k.kind == a2a::KIND_TMA ? "tma" : "direct", k.lines, k.lpt, k.threads, k.smem,
+                     names[p], k.n,
+                     k.kind == a2a::KIND_PIPE ? "pipe" : k.kind == a2a::KIND_TMA ? "tma"
+                     : k.kind == a2a::KIND_RPIPE ? "rpipe" : "direct", k.lines, k.lpt, k.threads, k.smem,
                      ps.occ[c], k.radix[0], k.radix[1], k.radix[2], k.radix[3], (int)ps.fits[c], ps.tuned_ms[c],
                      c == ps.chosen ? " <- chosen" : "");
             out += line;

@@ -91,6 +91,7 @@ A2A_PLANS(double)
     X(float,  192, KIND_PIPE,   16, 256, 2, 1)         \
     X(float,  192, KIND_DIRECT,  4,  64, 1, 1)         \
     X(float,  256, KIND_DIRECT, 16, 256, 2, 1)         \
+    X(float,  256, KIND_RPIPE,  16, 256, 2, 1)         \
     X(float,  256, KIND_DIRECT, 32, 256, 1, 2)         \
     X(float,  256, KIND_TMA,    16, 256, 2, 1)         \
     X(float,  256, KIND_TMA,    32, 512, 1, 1)         \
@@ -104,6 +105,10 @@ A2A_PLANS(double)
     X(float,  384, KIND_DIRECT,  4,  64, 1, 1)         \
     X(float,  512, KIND_DIRECT, 16, 512, 1, 2)         \
     X(float,  512, KIND_DIRECT,  8, 128, 4, 1)         \
+    X(float,  512, KIND_RPIPE,  16, 512, 1, 2)         \
+    X(float,  512, KIND_RPIPE,  16, 512, 1, 1)         \
+    X(float,  512, KIND_RPIPE,   8, 256, 2, 1)         \
+    X(float,  512, KIND_RPIPE,  16, 256, 1, 2)         \
     X(float,  512, KIND_TMA,    16, 512, 1, 2)         \
     X(float,  512, KIND_TMA,    16, 256, 1, 2)         \
     X(float,  512, KIND_TMA,     8, 256, 2, 2)         \
@@ -118,6 +123,7 @@ A2A_PLANS(double)
     X(float,  768, KIND_PIPE,    8, 384, 1, 1)         \
     X(float,  768, KIND_DIRECT,  4, 128, 1, 1)         \
     X(float, 1024, KIND_DIRECT, 16, 512, 1, 2)         \
+    X(float, 1024, KIND_RPIPE,   8, 512, 1, 1)         \
     X(float, 1024, KIND_TMA,     8, 512, 1, 1)         \
     X(float, 1024, KIND_DIRECT,  8, 256, 1, 1)         \
     X(float, 1024, KIND_DIRECT,  8, 256, 1, 2)         \
@@ -158,6 +164,7 @@ A2A_PLANS(double)
     X(double,  384, KIND_DIRECT,  8, 256, 1, 1)        \
     X(double,  384, KIND_DIRECT,  4, 128, 1, 1)        \
     X(double,  512, KIND_DIRECT,  8, 256, 1, 1)        \
+    X(double,  512, KIND_RPIPE,   8, 512, 1, 1)        \
     X(double,  512, KIND_TMA,     8, 256, 1, 1)        \
     X(double,  512, KIND_DIRECT,  8, 512, 1, 1)        \
     X(double,  512, KIND_PIPE,    8, 512, 1, 1)        \
@@ -176,6 +183,8 @@ PassKernel make_pass_kernel() {
         k.fn = reinterpret_cast<const void*>(&fft_pipe_kernel<T, P, B, TH, MODE, INV, MB, LPT>);
     else if constexpr (KIND == KIND_TMA)
         k.fn = reinterpret_cast<const void*>(&fft_tma_kernel<T, P, B, TH, MODE, INV, MB, LPT>);
+    else if constexpr (KIND == KIND_RPIPE)
+        k.fn = reinterpret_cast<const void*>(&fft_rpipe_kernel<T, P, B, TH, MODE, INV, MB, LPT>);
     else
         k.fn = reinterpret_cast<const void*>(&fft_pass_kernel<T, P, B, TH, MODE, INV, MB, LPT>);
     k.kind = KIND;
@@ -214,7 +223,7 @@ bool make_variant(int mode, bool inv, PassKernel* out) {
 int find_pass_kernels_f32(int n, int mode, bool inverse, PassKernel* out, int max);
 int find_pass_kernels_f64(int n, int mode, bool inverse, PassKernel* out, int max);
 
-constexpr int kMaxVariants = 12;
+constexpr int kMaxVariants = 16;
 
 // fft_tc.cu: the split-precision tensor-core kernel of length n (fmt 0 =
 // fp16, 1 = bf16); false when n has none.

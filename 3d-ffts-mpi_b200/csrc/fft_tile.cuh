@@ -381,7 +381,8 @@ enum PassKind : int {
     KIND_DIRECT = 0,  // one tile per CTA, stage 0 loads global memory into registers
     KIND_PIPE = 1,    // persistent CTAs, next tile prefetched into shared memory (LDGSTS)
     KIND_TMA = 2,     // persistent CTAs, tile rows fetched by TMA bulk copies, mbarrier completion
-    KIND_TC = 3       // radix-16 stages as split-precision tcgen05 GEMMs
+    KIND_TC = 3,      // radix-16 stages as split-precision tcgen05 GEMMs
+    KIND_RPIPE = 4    // persistent CTAs, next tile's stage-0 loads in flight in registers
 };
 
 constexpr int kTmaBuffers = 2;
@@ -491,6 +492,97 @@ __global__ void __launch_bounds__(THREADS, MINB) fft_pass_kernel(const PassArgs<
         }
         __syncthreads();
         run_stage<T, PLAN, B, THREADS, MODE, INV, LPT, 1>(a, tile, tw, offA_s, base_s, tid);
+    }
+}
+
+// KIND_RPIPE: persistent CTAs double-buffer through registers.  Stage 0 of
+// tile t leaves its results in shared memory; its registers then receive the
+// global loads of tile t + gridDim.x, which stay in flight while stages
+// 1..S-1 of tile t run, so each SM keeps HBM reads going through its
+// butterfly phase without a second shared-memory tile.
+template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV, int MINB, int LPT>
+__global__ void __launch_bounds__(THREADS, MINB) fft_rpipe_kernel(const PassArgs<T> a) {
+    using E = typename ElemOf<T, LPT>::type;
+    constexpr int BV = B / LPT;
+    using G = TileGeom<MODE, BV, PLAN::N, sizeof(E)>;
+    constexpr int N = PLAN::N;
+    constexpr int R0 = PLAN::r[0];
+    constexpr int NBL = N / R0;
+    constexpr int NBT = BV * NBL;
+    constexpr int K = (NBT + THREADS - 1) / THREADS;
+    constexpr bool EXACT = (NBT % THREADS) == 0;
+    constexpr int TWN = PLAN::twtotal();
+    constexpr bool BFAST0 = (MODE == MODE_BATCH);
+    static_assert(PLAN::S >= 2, "the pipelined kernel needs at least two stages");
+    static_assert(MODE != MODE_BATCH || THREADS % BV == 0, "batch mode needs THREADS % (B/LPT) == 0");
+    static_assert(LPT == 1 || MODE == MODE_BATCH, "line pairs only in batch mode");
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    E* tile = reinterpret_cast<E*>(smem_raw);
+    cx<T>* tw = reinterpret_cast<cx<T>*>(tile + G::elems);
+    uint32_t* offA_s = reinterpret_cast<uint32_t*>(tw + TWN);
+    size_t* base_s = reinterpret_cast<size_t*>(
+        smem_raw + ((sizeof(E) * (size_t)G::elems + sizeof(cx<T>) * TWN + sizeof(uint32_t) * N + 15) & ~size_t(15)));
+
+    const int tid = threadIdx.x;
+    const int tilesV = a.NV / B;
+    const int ntiles = a.NU * tilesV;
+    uint32_t d0[R0];
+    if (a.split) {
+#pragma unroll
+        for (int r = 0; r < R0; ++r) d0[r] = __ldg(a.offA + r * NBL);
+    }
+    auto load_tile = [&](int t, E (&x)[K][R0]) {
+        const int u = t / tilesV;
+        const int v0 = (t - u * tilesV) * B;
+        const size_t ubase = __ldg(a.offU + u);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int q = tid + k * THREADS;
+            if (EXACT || q < NBT) {
+                int b, j;
+                bf_map<BFAST0, BV, NBL>(q, b, j);
+                const cx<T>* line = a.src + ubase + __ldg(a.offV + v0 + b * LPT);
+                if (a.split) {
+                    const cx<T>* p = line + __ldg(a.offA + j);
+#pragma unroll
+                    for (int r = 0; r < R0; ++r) x[k][r] = ld_stream(reinterpret_cast<const E*>(p + d0[r]));
+                } else {
+#pragma unroll
+                    for (int r = 0; r < R0; ++r)
+                        x[k][r] = ld_stream(reinterpret_cast<const E*>(line + __ldg(a.offA + j + r * NBL)));
+                }
+            }
+        }
+    };
+    int t = blockIdx.x;
+    E x[K][R0];
+    if (t < ntiles) load_tile(t, x);
+    for (int i = tid; i < TWN; i += THREADS) tw[i] = a.tw[i];
+    for (int i = tid; i < N; i += THREADS) offA_s[i] = a.offA[i];
+    for (; t < ntiles; t += gridDim.x) {
+        {
+            const int u = t / tilesV;
+            const int v0 = (t - u * tilesV) * B;
+            const size_t ubase = __ldg(a.offU + u);
+            for (int i = tid; i < BV; i += THREADS) base_s[i] = ubase + __ldg(a.offV + v0 + i * LPT);
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int q = tid + k * THREADS;
+            if (EXACT || q < NBT) {
+                int b, j;
+                bf_map<BFAST0, BV, NBL>(q, b, j);
+                Dft<R0, INV, E>::run(x[k]);
+#pragma unroll
+                for (int r = 0; r < R0; ++r) tile[G::idx(b, j * R0 + r)] = x[k][r];
+            }
+        }
+        const int tn = t + gridDim.x;
+        if (tn < ntiles) load_tile(tn, x);  // in flight through the remaining stages
+        __syncthreads();
+        run_stage<T, PLAN, B, THREADS, MODE, INV, LPT, 1>(a, tile, tw, offA_s, base_s, tid);
+        __syncthreads();  // tile and line bases free for the next tile
     }
 }
 
