@@ -59,121 +59,121 @@ A2A_PLANS(double)
 // buffer and keep the fastest (a2a_dfft_make_plans).  DIRECT tiles are about
 // 32-64 KB so two or three CTAs share an SM; PIPE CTAs hold two tiles.
 #define A2A_VARIANTS_F32(X)                            \
-    X(float,    4, KIND_DIRECT,  4,  32, 1, 1)         \
-    X(float,    8, KIND_DIRECT,  8,  32, 1, 1)         \
-    X(float,    8, KIND_DIRECT,  4,  32, 1, 1)         \
-    X(float,   12, KIND_DIRECT,  4,  32, 1, 1)         \
-    X(float,   16, KIND_DIRECT, 16,  32, 1, 1)         \
-    X(float,   16, KIND_DIRECT,  4,  32, 1, 1)         \
-    X(float,   24, KIND_DIRECT,  8,  32, 1, 1)         \
-    X(float,   24, KIND_DIRECT,  4,  32, 1, 1)         \
-    X(float,   32, KIND_DIRECT, 32,  64, 1, 2)         \
-    X(float,   32, KIND_DIRECT, 32, 128, 1, 1)         \
-    X(float,   32, KIND_DIRECT,  4,  32, 1, 1)         \
-    X(float,   48, KIND_DIRECT, 16,  32, 1, 2)         \
-    X(float,   48, KIND_DIRECT, 16,  64, 1, 1)         \
-    X(float,   48, KIND_DIRECT,  4,  32, 1, 1)         \
-    X(float,   64, KIND_DIRECT, 32, 128, 1, 2)         \
-    X(float,   64, KIND_DIRECT, 32, 128, 1, 1)         \
-    X(float,   64, KIND_PIPE,   32, 128, 4, 1)         \
-    X(float,   64, KIND_DIRECT,  4,  32, 1, 1)         \
-    X(float,   96, KIND_DIRECT, 32, 128, 1, 2)         \
-    X(float,   96, KIND_DIRECT, 32, 128, 1, 1)         \
-    X(float,   96, KIND_PIPE,   32, 128, 2, 1)         \
-    X(float,   96, KIND_DIRECT,  4,  32, 1, 1)         \
-    X(float,  128, KIND_DIRECT, 32, 128, 1, 2)         \
-    X(float,  128, KIND_DIRECT, 16, 128, 4, 1)         \
-    X(float,  128, KIND_DIRECT, 32, 256, 1, 1)         \
-    X(float,  128, KIND_PIPE,   32, 256, 2, 1)         \
-    X(float,  128, KIND_DIRECT,  4,  32, 1, 1)         \
-    X(float,  192, KIND_DIRECT, 32, 256, 1, 2)         \
-    X(float,  192, KIND_DIRECT, 32, 256, 1, 1)         \
-    X(float,  192, KIND_PIPE,   16, 256, 2, 1)         \
-    X(float,  192, KIND_DIRECT,  4,  64, 1, 1)         \
-    X(float,  256, KIND_DIRECT, 16, 256, 2, 1)         \
-    X(float,  256, KIND_RPIPE,  16, 256, 2, 1)         \
-    X(float,  256, KIND_DIRECT, 32, 256, 1, 2)         \
-    X(float,  256, KIND_TMA,    16, 256, 2, 1)         \
-    X(float,  256, KIND_TMA,    32, 512, 1, 1)         \
-    X(float,  256, KIND_DIRECT, 16, 128, 4, 2)         \
-    X(float,  256, KIND_DIRECT, 32, 256, 1, 1)         \
-    X(float,  256, KIND_PIPE,   16, 256, 2, 1)         \
-    X(float,  256, KIND_DIRECT,  4,  64, 1, 1)         \
-    X(float,  384, KIND_DIRECT, 16, 256, 1, 2)         \
-    X(float,  384, KIND_DIRECT, 16, 256, 1, 1)         \
-    X(float,  384, KIND_PIPE,    8, 256, 2, 1)         \
-    X(float,  384, KIND_DIRECT,  4,  64, 1, 1)         \
-    X(float,  512, KIND_DIRECT, 16, 512, 1, 2)         \
-    X(float,  512, KIND_DIRECT,  8, 128, 4, 1)         \
-    X(float,  512, KIND_RPIPE,  16, 512, 1, 2)         \
-    X(float,  512, KIND_RPIPE,  16, 512, 1, 1)         \
-    X(float,  512, KIND_RPIPE,   8, 256, 2, 1)         \
-    X(float,  512, KIND_RPIPE,  16, 256, 1, 2)         \
-    X(float,  512, KIND_TMA,    16, 512, 1, 2)         \
-    X(float,  512, KIND_TMA,    16, 256, 1, 2)         \
-    X(float,  512, KIND_TMA,     8, 256, 2, 2)         \
-    X(float,  512, KIND_DIRECT, 16, 256, 2, 2)         \
-    X(float,  512, KIND_DIRECT, 16, 256, 2, 1)         \
-    X(float,  512, KIND_DIRECT,  8, 128, 4, 2)         \
-    X(float,  512, KIND_PIPE,    8, 256, 2, 1)         \
-    X(float,  512, KIND_DIRECT,  4,  64, 1, 1)         \
-    X(float,  768, KIND_DIRECT,  8, 256, 1, 2)         \
-    X(float,  768, KIND_DIRECT,  8, 256, 1, 1)         \
-    X(float,  768, KIND_DIRECT, 16, 384, 1, 2)         \
-    X(float,  768, KIND_PIPE,    8, 384, 1, 1)         \
-    X(float,  768, KIND_DIRECT,  4, 128, 1, 1)         \
-    X(float, 1024, KIND_DIRECT, 16, 512, 1, 2)         \
-    X(float, 1024, KIND_RPIPE,   8, 512, 1, 1)         \
-    X(float, 1024, KIND_TMA,     8, 512, 1, 1)         \
-    X(float, 1024, KIND_DIRECT,  8, 256, 1, 1)         \
-    X(float, 1024, KIND_DIRECT,  8, 256, 1, 2)         \
-    X(float, 1024, KIND_DIRECT,  8, 512, 1, 1)         \
-    X(float, 1024, KIND_PIPE,    8, 512, 1, 1)         \
-    X(float, 1024, KIND_DIRECT,  4, 128, 1, 1)
+    X(float,    4, KIND_DIRECT,  4,  32, 1, 1)      \
+    X(float,    8, KIND_DIRECT,  8,  32, 1, 1)      \
+    X(float,    8, KIND_DIRECT,  4,  32, 1, 1)      \
+    X(float,   12, KIND_DIRECT,  4,  32, 1, 1)      \
+    X(float,   16, KIND_DIRECT, 16,  32, 1, 1)      \
+    X(float,   16, KIND_DIRECT,  4,  32, 1, 1)      \
+    X(float,   24, KIND_DIRECT,  8,  32, 1, 1)      \
+    X(float,   24, KIND_DIRECT,  4,  32, 1, 1)      \
+    X(float,   32, KIND_DIRECT, 32,  64, 1, 2)      \
+    X(float,   32, KIND_DIRECT, 32, 128, 1, 1)      \
+    X(float,   32, KIND_DIRECT,  4,  32, 1, 1)      \
+    X(float,   48, KIND_DIRECT, 16,  32, 1, 2)      \
+    X(float,   48, KIND_DIRECT, 16,  64, 1, 1)      \
+    X(float,   48, KIND_DIRECT,  4,  32, 1, 1)      \
+    X(float,   64, KIND_DIRECT, 32, 128, 1, 2)      \
+    X(float,   64, KIND_DIRECT, 32, 128, 1, 1)      \
+    X(float,   64, KIND_PIPE,   32, 128, 4, 1)      \
+    X(float,   64, KIND_DIRECT,  4,  32, 1, 1)      \
+    X(float,   96, KIND_DIRECT, 32, 128, 1, 2)      \
+    X(float,   96, KIND_DIRECT, 32, 128, 1, 1)      \
+    X(float,   96, KIND_PIPE,   32, 128, 2, 1)      \
+    X(float,   96, KIND_DIRECT,  4,  32, 1, 1)      \
+    X(float,  128, KIND_DIRECT, 32, 128, 1, 2)      \
+    X(float,  128, KIND_DIRECT, 16, 128, 4, 1)      \
+    X(float,  128, KIND_DIRECT, 32, 256, 1, 1)      \
+    X(float,  128, KIND_PIPE,   32, 256, 2, 1)      \
+    X(float,  128, KIND_DIRECT,  4,  32, 1, 1)      \
+    X(float,  192, KIND_DIRECT, 32, 256, 1, 2)      \
+    X(float,  192, KIND_DIRECT, 32, 256, 1, 1)      \
+    X(float,  192, KIND_PIPE,   16, 256, 2, 1)      \
+    X(float,  192, KIND_DIRECT,  4,  64, 1, 1)      \
+    X(float,  256, KIND_DIRECT, 16, 256, 2, 1)      \
+    X(float,  256, KIND_RPIPE,  16, 256, 2, 1)      \
+    X(float,  256, KIND_DIRECT, 32, 256, 1, 2)      \
+    X(float,  256, KIND_TMA,    16, 256, 2, 1)      \
+    X(float,  256, KIND_TMA,    32, 512, 1, 1)      \
+    X(float,  256, KIND_DIRECT, 16, 128, 4, 2)      \
+    X(float,  256, KIND_DIRECT, 32, 256, 1, 1)      \
+    X(float,  256, KIND_PIPE,   16, 256, 2, 1)      \
+    X(float,  256, KIND_DIRECT,  4,  64, 1, 1)      \
+    X(float,  384, KIND_DIRECT, 16, 256, 1, 2)      \
+    X(float,  384, KIND_DIRECT, 16, 256, 1, 1)      \
+    X(float,  384, KIND_PIPE,    8, 256, 2, 1)      \
+    X(float,  384, KIND_DIRECT,  4,  64, 1, 1)      \
+    X(float,  512, KIND_RPIPE,  16, 512, 1, 2)      \
+    X(float,  512, KIND_RPIPE,   8, 256, 2, 1)      \
+    X(float,  512, KIND_DIRECT, 16, 512, 1, 2)      \
+    X(float,  512, KIND_DIRECT,  8, 128, 4, 1)      \
+    X(float,  512, KIND_RPIPE,  16, 512, 1, 1)      \
+    X(float,  512, KIND_RPIPE,  16, 256, 1, 2)      \
+    X(float,  512, KIND_TMA,    16, 512, 1, 2)      \
+    X(float,  512, KIND_TMA,    16, 256, 1, 2)      \
+    X(float,  512, KIND_TMA,     8, 256, 2, 2)      \
+    X(float,  512, KIND_DIRECT, 16, 256, 2, 2)      \
+    X(float,  512, KIND_DIRECT, 16, 256, 2, 1)      \
+    X(float,  512, KIND_DIRECT,  8, 128, 4, 2)      \
+    X(float,  512, KIND_PIPE,    8, 256, 2, 1)      \
+    X(float,  512, KIND_DIRECT,  4,  64, 1, 1)      \
+    X(float,  768, KIND_DIRECT,  8, 256, 1, 2)      \
+    X(float,  768, KIND_DIRECT,  8, 256, 1, 1)      \
+    X(float,  768, KIND_DIRECT, 16, 384, 1, 2)      \
+    X(float,  768, KIND_PIPE,    8, 384, 1, 1)      \
+    X(float,  768, KIND_DIRECT,  4, 128, 1, 1)      \
+    X(float, 1024, KIND_DIRECT,  8, 512, 1, 1)      \
+    X(float, 1024, KIND_DIRECT, 16, 512, 1, 2)      \
+    X(float, 1024, KIND_RPIPE,   8, 512, 1, 1)      \
+    X(float, 1024, KIND_TMA,     8, 512, 1, 1)      \
+    X(float, 1024, KIND_DIRECT,  8, 256, 1, 1)      \
+    X(float, 1024, KIND_DIRECT,  8, 256, 1, 2)      \
+    X(float, 1024, KIND_PIPE,    8, 512, 1, 1)      \
+    X(float, 1024, KIND_DIRECT,  4, 128, 1, 1)     
 
 #define A2A_VARIANTS_F64(X)                         \
-    X(double,    4, KIND_DIRECT,  4,  32, 1, 1)        \
-    X(double,    8, KIND_DIRECT,  8,  32, 1, 1)        \
-    X(double,    8, KIND_DIRECT,  4,  32, 1, 1)        \
-    X(double,   12, KIND_DIRECT,  4,  32, 1, 1)        \
-    X(double,   16, KIND_DIRECT, 16,  32, 1, 1)        \
-    X(double,   16, KIND_DIRECT,  4,  32, 1, 1)        \
-    X(double,   24, KIND_DIRECT,  8,  32, 1, 1)        \
-    X(double,   24, KIND_DIRECT,  4,  32, 1, 1)        \
-    X(double,   32, KIND_DIRECT, 16, 128, 1, 1)        \
-    X(double,   32, KIND_DIRECT,  4,  32, 1, 1)        \
-    X(double,   48, KIND_DIRECT,  8,  64, 1, 1)        \
-    X(double,   48, KIND_DIRECT,  4,  32, 1, 1)        \
-    X(double,   64, KIND_DIRECT, 32, 128, 1, 1)        \
-    X(double,   64, KIND_DIRECT, 16, 128, 2, 1)        \
-    X(double,   64, KIND_PIPE,   16, 128, 2, 1)        \
-    X(double,   64, KIND_DIRECT,  4,  32, 1, 1)        \
-    X(double,   96, KIND_DIRECT, 16, 128, 1, 1)        \
-    X(double,   96, KIND_PIPE,   16, 128, 2, 1)        \
-    X(double,   96, KIND_DIRECT,  4,  32, 1, 1)        \
-    X(double,  128, KIND_DIRECT, 16, 128, 1, 1)        \
-    X(double,  128, KIND_PIPE,   16, 256, 2, 1)        \
-    X(double,  128, KIND_DIRECT,  4,  32, 1, 1)        \
-    X(double,  192, KIND_DIRECT, 16, 256, 1, 1)        \
-    X(double,  192, KIND_PIPE,    8, 256, 1, 1)        \
-    X(double,  192, KIND_DIRECT,  4,  64, 1, 1)        \
-    X(double,  256, KIND_DIRECT, 16, 256, 1, 1)        \
-    X(double,  256, KIND_DIRECT,  8, 128, 2, 1)        \
-    X(double,  256, KIND_PIPE,    8, 256, 1, 1)        \
-    X(double,  256, KIND_DIRECT,  4,  64, 1, 1)        \
-    X(double,  384, KIND_DIRECT,  8, 256, 1, 1)        \
-    X(double,  384, KIND_DIRECT,  4, 128, 1, 1)        \
-    X(double,  512, KIND_DIRECT,  8, 256, 1, 1)        \
-    X(double,  512, KIND_RPIPE,   8, 512, 1, 1)        \
-    X(double,  512, KIND_TMA,     8, 256, 1, 1)        \
-    X(double,  512, KIND_DIRECT,  8, 512, 1, 1)        \
-    X(double,  512, KIND_PIPE,    8, 512, 1, 1)        \
-    X(double,  512, KIND_DIRECT,  4, 128, 1, 1)        \
-    X(double,  768, KIND_DIRECT,  8, 384, 1, 1)        \
-    X(double,  768, KIND_DIRECT,  4, 192, 1, 1)        \
-    X(double, 1024, KIND_DIRECT,  8, 512, 1, 1)        \
-    X(double, 1024, KIND_DIRECT,  4, 256, 1, 1)
-// clang-format on
+    X(double,    4, KIND_DIRECT,  4,  32, 1, 1)     \
+    X(double,    8, KIND_DIRECT,  8,  32, 1, 1)     \
+    X(double,    8, KIND_DIRECT,  4,  32, 1, 1)     \
+    X(double,   12, KIND_DIRECT,  4,  32, 1, 1)     \
+    X(double,   16, KIND_DIRECT, 16,  32, 1, 1)     \
+    X(double,   16, KIND_DIRECT,  4,  32, 1, 1)     \
+    X(double,   24, KIND_DIRECT,  8,  32, 1, 1)     \
+    X(double,   24, KIND_DIRECT,  4,  32, 1, 1)     \
+    X(double,   32, KIND_DIRECT, 16, 128, 1, 1)     \
+    X(double,   32, KIND_DIRECT,  4,  32, 1, 1)     \
+    X(double,   48, KIND_DIRECT,  8,  64, 1, 1)     \
+    X(double,   48, KIND_DIRECT,  4,  32, 1, 1)     \
+    X(double,   64, KIND_DIRECT, 32, 128, 1, 1)     \
+    X(double,   64, KIND_DIRECT, 16, 128, 2, 1)     \
+    X(double,   64, KIND_PIPE,   16, 128, 2, 1)     \
+    X(double,   64, KIND_DIRECT,  4,  32, 1, 1)     \
+    X(double,   96, KIND_DIRECT, 16, 128, 1, 1)     \
+    X(double,   96, KIND_PIPE,   16, 128, 2, 1)     \
+    X(double,   96, KIND_DIRECT,  4,  32, 1, 1)     \
+    X(double,  128, KIND_DIRECT, 16, 128, 1, 1)     \
+    X(double,  128, KIND_PIPE,   16, 256, 2, 1)     \
+    X(double,  128, KIND_DIRECT,  4,  32, 1, 1)     \
+    X(double,  192, KIND_DIRECT, 16, 256, 1, 1)     \
+    X(double,  192, KIND_PIPE,    8, 256, 1, 1)     \
+    X(double,  192, KIND_DIRECT,  4,  64, 1, 1)     \
+    X(double,  256, KIND_DIRECT, 16, 256, 1, 1)     \
+    X(double,  256, KIND_DIRECT,  8, 128, 2, 1)     \
+    X(double,  256, KIND_PIPE,    8, 256, 1, 1)     \
+    X(double,  256, KIND_DIRECT,  4,  64, 1, 1)     \
+    X(double,  384, KIND_DIRECT,  8, 256, 1, 1)     \
+    X(double,  384, KIND_DIRECT,  4, 128, 1, 1)     \
+    X(double,  512, KIND_RPIPE,   8, 512, 1, 1)     \
+    X(double,  512, KIND_DIRECT,  8, 256, 1, 1)     \
+    X(double,  512, KIND_TMA,     8, 256, 1, 1)     \
+    X(double,  512, KIND_DIRECT,  8, 512, 1, 1)     \
+    X(double,  512, KIND_PIPE,    8, 512, 1, 1)     \
+    X(double,  512, KIND_DIRECT,  4, 128, 1, 1)     \
+    X(double,  768, KIND_DIRECT,  4, 192, 1, 1)     \
+    X(double,  768, KIND_DIRECT,  8, 384, 1, 1)     \
+    X(double, 1024, KIND_DIRECT,  8, 512, 1, 1)     \
+    X(double, 1024, KIND_DIRECT,  4, 256, 1, 1)     \
+// clang-format on                                 
 
 template <typename T, int N, int KIND, int B, int TH, int MB, int LPT, int MODE, bool INV>
 PassKernel make_pass_kernel() {
