@@ -48,14 +48,29 @@ __all__ = [
     "scale_fft",
     "fast_copy_fft",
     "version",
+    "write_dims",
+    "write_rank_dumps",
 ]
 
+_KERNELS = {"d_z_a2a_to_z_pencils", "d_z_pencils_to_z_a2a", "d_x_a2a_to_x_pencils", "d_x_pencils_to_x_a2a",
+            "d_y_a2a_to_y_pencils", "d_y_pencils_to_y_a2a", "d_fast_z_to_x", "d_fast_x_to_y", "d_fast_y_to_z"}
 _PREC = {"c128": C128, "complex128": C128, "double": C128, "c64": C64, "complex64": C64, "float": C64}
 _METHODS = {"plain": METHOD_PLAIN, "split_bf16": METHOD_SPLIT_BF16, "split_fp16": METHOD_SPLIT_FP16}
 
 
 def version() -> int:
     return lib().a2a_version()
+
+
+def _host_ptr(a) -> int:
+    """Address of a contiguous host array (numpy array or CPU tensor)."""
+    if hasattr(a, "data_ptr"):
+        if a.is_cuda or not a.is_contiguous():
+            raise ValueError("host buffers must be contiguous CPU tensors")
+        return a.data_ptr()
+    if not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("host buffers must be C-contiguous")
+    return a.ctypes.data
 
 
 def _torch_dtype(prec: int):
@@ -161,6 +176,23 @@ class a2aDistribution:
     def returnYPencils(self, d_Buff1, d_Buff2):
         call("a2a_return_y_pencils", self._h, self._buf(d_Buff1), self._buf(d_Buff2))
 
+    # -- the individual kernels (distribution/kernels/kernels.h:3-17) -------
+    def alltoall(self, source, dest):
+        """``MPI_Alltoall`` of ``nsends`` complexes per peer over the virtual ranks."""
+        call("a2a_alltoall", self._h, self._buf(source), self._buf(dest))
+
+    def launch(self, kernel: str, source, dest):
+        """One remap kernel by its reference name: ``d_z_a2a_to_z_pencils``,
+        ``d_z_pencils_to_z_a2a``, ``d_x_...``, ``d_y_...``, ``d_fast_z_to_x``,
+        ``d_fast_x_to_y``, ``d_fast_y_to_z``."""
+        if kernel not in _KERNELS:
+            raise ValueError(f"unknown kernel {kernel!r}; one of {sorted(_KERNELS)}")
+        call("a2a_" + kernel, self._h, self._buf(source), self._buf(dest))
+
+    def write_dims(self, path: str) -> None:
+        """The reference's ``dims`` file (``a2adistribution.cpp:142-151``)."""
+        write_dims(self.Ng, self.world_size, path)
+
     def finalize(self) -> None:
         """``a2aDistribution::finalize`` (``a2adistribution.cpp:258-265``)."""
         if self._h:
@@ -172,6 +204,33 @@ class a2aDistribution:
             self.finalize()
         except Exception:
             pass
+
+
+def write_dims(Ng: int, world_size: int, path: str) -> None:
+    """Write the reference's ``dims`` file: nine int32 (world_size, Ng,
+    nlocal, dims[3], local_grid_size[3]); host only."""
+    call("a2a_write_dims", int(Ng), int(world_size), str(path).encode())
+
+
+def write_rank_dumps(Ng: int, world_size: int, folder: str, inp, fwd, inv) -> None:
+    """Write ``<folder>/proc<r>`` for every rank: its brick of ``inp``,
+    ``fwd`` and ``inv`` (rank-major host arrays or CUDA tensors, complex128
+    or complex64), the layout of the reference test's dumps
+    (``tests/test.cpp:69-125``)."""
+    import numpy as np
+
+    arrs = []
+    for a in (inp, fwd, inv):
+        if hasattr(a, "detach"):
+            a = a.detach().cpu().numpy()
+        arrs.append(np.ascontiguousarray(a).ravel())
+    dt = arrs[0].dtype
+    if dt not in (np.complex128, np.complex64) or any(a.dtype != dt for a in arrs):
+        raise TypeError("dumps are complex128 or complex64, all three the same")
+    prec = C128 if dt == np.complex128 else C64
+    call("a2a_write_rank_dumps", int(Ng), int(world_size), prec, str(folder).encode(),
+         arrs[0].ctypes.data_as(ctypes.c_void_p), arrs[1].ctypes.data_as(ctypes.c_void_p),
+         arrs[2].ctypes.data_as(ctypes.c_void_p))
 
 
 # -- dfft/kernels/kernels.h:5-11 --------------------------------------------
@@ -271,6 +330,17 @@ class a2adfft:
             call("a2a_dfft_inverse_async", self._h, self.distribution._buf(d_data), ctypes.c_void_p(handle))
 
     backward = inverse
+
+    def forward_host(self, host_data, d_buffer) -> None:
+        """Host-staged forward (``fft_demo/fft_3d/fft_3d.c:6-96``): host array
+        -> ``d_buffer`` -> transform -> back into the host array."""
+        call("a2a_dfft_forward_host", self._h, ctypes.c_void_p(_host_ptr(host_data)),
+             self.distribution._buf(d_buffer))
+
+    def inverse_host(self, host_data, d_buffer) -> None:
+        """Host-staged inverse (``fft_demo/fft_3d/fft_3d.c:98-189``)."""
+        call("a2a_dfft_inverse_host", self._h, ctypes.c_void_p(_host_ptr(host_data)),
+             self.distribution._buf(d_buffer))
 
     def execute_pass(self, d_data, pass_index: int, inverse: bool, stream) -> None:
         """Enqueue one of the three fused passes (0 = Z, 1 = X, 2 = Y)."""

@@ -66,6 +66,16 @@ SIGNATURES = {
     "a2a_get_y_pencils": [_P, _PP, _PP],
     "a2a_return_y_pencils": [_P, _PP, _PP],
     "a2a_distribution_finalize": [_P],
+    "a2a_alltoall": [_P, _PP, _PP],
+    "a2a_d_z_a2a_to_z_pencils": [_P, _PP, _PP],
+    "a2a_d_z_pencils_to_z_a2a": [_P, _PP, _PP],
+    "a2a_d_x_a2a_to_x_pencils": [_P, _PP, _PP],
+    "a2a_d_x_pencils_to_x_a2a": [_P, _PP, _PP],
+    "a2a_d_y_a2a_to_y_pencils": [_P, _PP, _PP],
+    "a2a_d_y_pencils_to_y_a2a": [_P, _PP, _PP],
+    "a2a_d_fast_z_to_x": [_P, _PP, _PP],
+    "a2a_d_fast_x_to_y": [_P, _PP, _PP],
+    "a2a_d_fast_y_to_z": [_P, _PP, _PP],
     "a2a_forward_1d_fft": [_P, _PP],
     "a2a_inverse_1d_fft": [_P, _PP],
     "a2a_scale_fft": [_P, _PP, _PP],
@@ -86,6 +96,10 @@ SIGNATURES = {
     "a2a_dfft_execute_pass_async": [_P, _PP, _I, _I, _P],
     "a2a_dfft_launches_per_transform": [_P, ctypes.POINTER(_I)],
     "a2a_dfft_destroy": [_P],
+    "a2a_dfft_forward_host": [_P, _P, _PP],
+    "a2a_dfft_inverse_host": [_P, _P, _PP],
+    "a2a_write_dims": [_I, _I, ctypes.c_char_p],
+    "a2a_write_rank_dumps": [_I, _I, _I, ctypes.c_char_p, _P, _P, _P],
     "a2a_status_string": [_I],
     "a2a_last_error": [],
     "a2a_version": [],

@@ -682,6 +682,58 @@ a2a_status a2a_return_y_pencils(a2a_distribution* h, void** b1, void** b2) {
     });
 }
 
+// ---- the individual launchers of distribution/kernels/kernels.h:3-17 ----
+
+static a2a_status one_kernel(a2a_distribution* h, void** src, void** dst, cudaError_t (*body)(Dist&, void*, void*)) {
+    if (!h) return fail(A2A_ERROR_INVALID_VALUE, "distribution is NULL");
+    Dist& d = h->d;
+    a2a_status s;
+    if ((s = need_cube(d, "the remap kernels")) != A2A_SUCCESS) return s;
+    if ((s = check_buf(src, "source")) != A2A_SUCCESS) return s;
+    if ((s = check_buf(dst, "dest")) != A2A_SUCCESS) return s;
+    if (src[0] == dst[0]) return fail(A2A_ERROR_INVALID_VALUE, "source and dest must be distinct buffers");
+    const cudaError_t e = body(d, src[0], dst[0]);
+    if (e != cudaSuccess) return cuda_fail(e, "remap launch");
+    return finish(d, d.stream, true);
+}
+
+a2a_status a2a_alltoall(a2a_distribution* h, void** src, void** dst) {
+    return one_kernel(h, src, dst, [](Dist& d, void* a, void* b) { return a2a::launch_alltoall(d, a, b, d.stream); });
+}
+a2a_status a2a_d_z_a2a_to_z_pencils(a2a_distribution* h, void** src, void** dst) {
+    return one_kernel(h, src, dst,
+                      [](Dist& d, void* a, void* b) { return a2a::launch_pencil_remap(d, 2, true, a, b, d.stream); });
+}
+a2a_status a2a_d_z_pencils_to_z_a2a(a2a_distribution* h, void** src, void** dst) {
+    return one_kernel(h, src, dst,
+                      [](Dist& d, void* a, void* b) { return a2a::launch_pencil_remap(d, 2, false, a, b, d.stream); });
+}
+a2a_status a2a_d_x_a2a_to_x_pencils(a2a_distribution* h, void** src, void** dst) {
+    return one_kernel(h, src, dst,
+                      [](Dist& d, void* a, void* b) { return a2a::launch_pencil_remap(d, 0, true, a, b, d.stream); });
+}
+a2a_status a2a_d_x_pencils_to_x_a2a(a2a_distribution* h, void** src, void** dst) {
+    return one_kernel(h, src, dst,
+                      [](Dist& d, void* a, void* b) { return a2a::launch_pencil_remap(d, 0, false, a, b, d.stream); });
+}
+a2a_status a2a_d_y_a2a_to_y_pencils(a2a_distribution* h, void** src, void** dst) {
+    return one_kernel(h, src, dst,
+                      [](Dist& d, void* a, void* b) { return a2a::launch_pencil_remap(d, 1, true, a, b, d.stream); });
+}
+a2a_status a2a_d_y_pencils_to_y_a2a(a2a_distribution* h, void** src, void** dst) {
+    return one_kernel(h, src, dst,
+                      [](Dist& d, void* a, void* b) { return a2a::launch_pencil_remap(d, 1, false, a, b, d.stream); });
+}
+a2a_status a2a_d_fast_z_to_x(a2a_distribution* h, void** src, void** dst) {
+    return one_kernel(h, src, dst, [](Dist& d, void* a, void* b) { return a2a::launch_fast_axis(d, 0, a, b, d.stream); });
+}
+a2a_status a2a_d_fast_x_to_y(a2a_distribution* h, void** src, void** dst) {
+    return one_kernel(h, src, dst, [](Dist& d, void* a, void* b) { return a2a::launch_fast_axis(d, 1, a, b, d.stream); });
+}
+a2a_status a2a_d_fast_y_to_z(a2a_distribution* h, void** src, void** dst) {
+    return one_kernel(h, src, dst, [](Dist& d, void* a, void* b) { return a2a::launch_fast_axis(d, 2, a, b, d.stream); });
+}
+
 a2a_status a2a_distribution_finalize(a2a_distribution* h) {
     if (!h) return A2A_SUCCESS;
     release(h->d);
@@ -901,6 +953,92 @@ a2a_status a2a_dfft_destroy(a2a_dfft* f) {
     if (f && f->d_tc) cudaFree(f->d_tc);
     delete f;
     return A2A_SUCCESS;
+}
+
+// ---- dump files (a2adistribution.cpp:142-151, tests/test.cpp:69-125) ----
+
+static a2a_status host_decomp(int ng, int P, int dims[3], int local[3], long long* nlocal) {
+    if (ng < 1 || P < 1) return fail(A2A_ERROR_INVALID_VALUE, "ng and world_size must be >= 1");
+    dims_create(P, dims);
+    for (int a = 0; a < 3; ++a)
+        if (ng % dims[a] || P % dims[a])
+            return fail(A2A_ERROR_DECOMPOSITION, "Ng=%d / world_size=%d do not divide by dims[%d]=%d", ng, P, a,
+                        dims[a]);
+    for (int a = 0; a < 3; ++a) local[a] = ng / dims[a];
+    const long long lx = local[0], ly = local[1], lz = local[2];
+    if ((lx * ly) % P || (lx * lz) % P || (ly * lz) % P)
+        return fail(A2A_ERROR_DECOMPOSITION, "a face of the brick is not divisible by world_size=%d", P);
+    *nlocal = lx * ly * lz;
+    return A2A_SUCCESS;
+}
+
+a2a_status a2a_write_dims(int ng, int world_size, const char* path) {
+    int dims[3], local[3];
+    long long nlocal;
+    a2a_status s;
+    if (!path) return fail(A2A_ERROR_INVALID_VALUE, "path is NULL");
+    if ((s = host_decomp(ng, world_size, dims, local, &nlocal)) != A2A_SUCCESS) return s;
+    if (nlocal > 2147483647LL) return fail(A2A_ERROR_UNSUPPORTED, "nlocal does not fit the 32-bit field");
+    FILE* fh = fopen(path, "wb");
+    if (!fh) return fail(A2A_ERROR_INVALID_VALUE, "cannot open %s", path);
+    const int head[3] = {world_size, ng, (int)nlocal};
+    size_t w = fwrite(head, sizeof(int), 3, fh);
+    w += fwrite(dims, sizeof(int), 3, fh);
+    w += fwrite(local, sizeof(int), 3, fh);
+    fclose(fh);
+    if (w != 9) return fail(A2A_ERROR_INVALID_VALUE, "short write to %s", path);
+    return A2A_SUCCESS;
+}
+
+a2a_status a2a_write_rank_dumps(int ng, int world_size, a2a_precision precision, const char* folder,
+                                const void* host_input, const void* host_forward, const void* host_inverse) {
+    int dims[3], local[3];
+    long long nlocal;
+    a2a_status s;
+    if (!folder || !host_input || !host_forward || !host_inverse)
+        return fail(A2A_ERROR_INVALID_VALUE, "NULL argument");
+    if (precision != A2A_C128 && precision != A2A_C64)
+        return fail(A2A_ERROR_INVALID_VALUE, "unknown precision %d", (int)precision);
+    if ((s = host_decomp(ng, world_size, dims, local, &nlocal)) != A2A_SUCCESS) return s;
+    const size_t eb = precision == A2A_C128 ? 16 : 8;
+    const size_t rank_bytes = (size_t)nlocal * eb;
+    const void* parts[3] = {host_input, host_forward, host_inverse};
+    for (int r = 0; r < world_size; ++r) {
+        char path[4096];
+        snprintf(path, sizeof path, "%s/proc%d", folder, r);
+        FILE* fh = fopen(path, "wb");
+        if (!fh) return fail(A2A_ERROR_INVALID_VALUE, "cannot open %s", path);
+        for (const void* part : parts) {
+            if (fwrite(static_cast<const char*>(part) + (size_t)r * rank_bytes, 1, rank_bytes, fh) != rank_bytes) {
+                fclose(fh);
+                return fail(A2A_ERROR_INVALID_VALUE, "short write to %s", path);
+            }
+        }
+        fclose(fh);
+    }
+    return A2A_SUCCESS;
+}
+
+// ---- host-staged transforms (fft_demo/fft_3d/fft_3d.c:6-189) ----
+
+static a2a_status host_staged(a2a_dfft* f, void* host, void** d_buf, bool inv) {
+    if (!f || !host) return fail(A2A_ERROR_INVALID_VALUE, "NULL argument");
+    a2a_status s;
+    if ((s = check_dfft(f, d_buf)) != A2A_SUCCESS) return s;
+    const Dist& d = f->dist->d;
+    const size_t bytes = (size_t)d.P * d.nlocal * d.elem_bytes;
+    A2A_CUDA(cudaMemcpyAsync(d_buf[0], host, bytes, cudaMemcpyHostToDevice, d.stream), "cudaMemcpyAsync(H2D)");
+    if ((s = fused(f, d_buf, inv, d.stream, false)) != A2A_SUCCESS) return s;
+    A2A_CUDA(cudaMemcpyAsync(host, d_buf[0], bytes, cudaMemcpyDeviceToHost, d.stream), "cudaMemcpyAsync(D2H)");
+    A2A_CUDA(cudaStreamSynchronize(d.stream), "cudaStreamSynchronize");
+    return check_device_flag(d);
+}
+
+a2a_status a2a_dfft_forward_host(a2a_dfft* f, void* host_data, void** d_buffer) {
+    return host_staged(f, host_data, d_buffer, false);
+}
+a2a_status a2a_dfft_inverse_host(a2a_dfft* f, void* host_data, void** d_buffer) {
+    return host_staged(f, host_data, d_buffer, true);
 }
 
 const char* a2a_status_string(a2a_status s) {

@@ -118,6 +118,25 @@ a2a_status a2a_return_x_pencils(a2a_distribution* dist, void** d_buff1, void** d
 a2a_status a2a_get_y_pencils(a2a_distribution* dist, void** d_buff1, void** d_buff2);    /* :222-238 */
 a2a_status a2a_return_y_pencils(a2a_distribution* dist, void** d_buff1, void** d_buff2); /* :240-256 */
 
+/* The individual kernels the steps are made of, as the reference exposes
+ * them in distribution/kernels/kernels.h:3-17 (each synchronous; source and
+ * dest are distinct buffers of world_size * nlocal elements):
+ * MPI_Alltoall with nsends = nlocal / world_size over the virtual ranks
+ * (a2adistribution.cpp:158-165); the pack/unpack remaps
+ * (distribution/kernels/a2apencils.cu:5-226; the Y pack is the true inverse
+ * of the Y unpack, see above); the fast-axis changes
+ * (distribution/kernels/a2achangefastaxis.cu:4-93). */
+a2a_status a2a_alltoall(a2a_distribution* dist, void** source, void** dest);
+a2a_status a2a_d_z_a2a_to_z_pencils(a2a_distribution* dist, void** source, void** dest);
+a2a_status a2a_d_z_pencils_to_z_a2a(a2a_distribution* dist, void** source, void** dest);
+a2a_status a2a_d_x_a2a_to_x_pencils(a2a_distribution* dist, void** source, void** dest);
+a2a_status a2a_d_x_pencils_to_x_a2a(a2a_distribution* dist, void** source, void** dest);
+a2a_status a2a_d_y_a2a_to_y_pencils(a2a_distribution* dist, void** source, void** dest);
+a2a_status a2a_d_y_pencils_to_y_a2a(a2a_distribution* dist, void** source, void** dest);
+a2a_status a2a_d_fast_z_to_x(a2a_distribution* dist, void** source, void** dest);
+a2a_status a2a_d_fast_x_to_y(a2a_distribution* dist, void** source, void** dest);
+a2a_status a2a_d_fast_y_to_z(a2a_distribution* dist, void** source, void** dest);
+
 /* a2aDistribution::finalize (a2adistribution.cpp:258-265); also frees the
  * object.  NULL is accepted. */
 a2a_status a2a_distribution_finalize(a2a_distribution* dist);
@@ -199,6 +218,31 @@ a2a_status a2a_dfft_execute_pass_async(a2a_dfft* dfft, void** d_data, int pass, 
 a2a_status a2a_dfft_launches_per_transform(const a2a_dfft* dfft, int* out);
 
 a2a_status a2a_dfft_destroy(a2a_dfft* dfft);
+
+/* ---- host-staged transforms -------------------------------------------- */
+
+/* The FP32 demo driver's pattern (src/fft_demo/fft_3d/fft_3d.c:6-189): the
+ * data lives in host memory; it is copied to d_buffer[0] (a device buffer
+ * of the plan's size), transformed there and copied back, synchronously. */
+a2a_status a2a_dfft_forward_host(a2a_dfft* dfft, void* host_data, void** d_buffer);
+a2a_status a2a_dfft_inverse_host(a2a_dfft* dfft, void* host_data, void** d_buffer);
+
+/* ---- dump files ---------------------------------------------------------- */
+
+/* The reference's `dims` file (distribution/a2adistribution.cpp:142-151):
+ * nine int32 -- world_size, Ng, nlocal, dims[3], local_grid_size[3].  Host
+ * only; needs no device. */
+a2a_status a2a_write_dims(int ng, int world_size, const char* path);
+
+/* The reference test's per-rank dumps (tests/test.cpp:69-125): for every
+ * rank r, file `<folder>/proc<r>` holding that rank's brick of the input,
+ * the forward result and the inverse result, one after the other (complex
+ * double for A2A_C128 as in src/a2afft, complex float for A2A_C64 as in
+ * src/fft_demo).  The three host buffers are rank-major (world_size *
+ * nlocal elements each).  The reference names files `proc<digit>` and so
+ * stops at 10 ranks; here r is written in full.  Host only. */
+a2a_status a2a_write_rank_dumps(int ng, int world_size, a2a_precision precision, const char* folder,
+                                const void* host_input, const void* host_forward, const void* host_inverse);
 
 /* ---- misc --------------------------------------------------------------- */
 

@@ -75,3 +75,27 @@ def test_invalid_arguments_without_gpu(pkg):
 def test_python_mirror_rejects_bad_precision(pkg):
     with pytest.raises(ValueError):
         pkg.a2aDistribution(4, 8, 64, precision="bf16")
+
+
+def test_dims_and_rank_dumps_roundtrip_on_cpu(pkg, oracle, tmp_path):
+    """The reference's dims / proc<r> files written by the C ABI read back
+    with the reference checker's semantics (no GPU: host-only calls)."""
+    import importlib
+
+    import numpy as np
+
+    dumps = importlib.import_module(pkg.__name__ + ".dumps")
+    for P, ng in [(8, 8), (6, 12), (16, 32)]:
+        d = oracle.Decomp(ng, P)
+        pkg.write_dims(ng, P, str(tmp_path / "dims"))
+        prm = dumps.read_dims(str(tmp_path / "dims"))
+        assert prm == {"world_size": P, "Ng": ng, "nlocal": d.nlocal, "dims": d.dims, "local_grid_size": list(d.local)}
+        g = oracle.make_input("uniform", (ng,) * 3, seed=1, dtype=np.complex128)
+        b = oracle.global_to_bricks(g, d)
+        fwd = oracle.global_to_bricks(np.fft.fftn(g), d)
+        pkg.write_rank_dumps(ng, P, str(tmp_path), b, fwd, b)
+        assert dumps.check(str(tmp_path)) == (True, True)
+        raw = dumps.read_rank_dumps(str(tmp_path), prm)
+        assert np.array_equal(dumps.stitch(raw[:, 0], prm), g)
+    with pytest.raises(pkg.A2AError):
+        pkg.write_dims(10, 4, str(tmp_path / "bad"))
