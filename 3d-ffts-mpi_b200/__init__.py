@@ -48,6 +48,7 @@ __all__ = [
     "scale_fft",
     "fast_copy_fft",
     "version",
+    "decompose",
     "write_dims",
     "write_rank_dumps",
 ]
@@ -111,7 +112,16 @@ class a2aDistribution:
         self.blockSize = d.block_size
         self.element_bytes = int(d.element_bytes)
         self.buffer_bytes = int(d.buffer_bytes)
+        self.first_rank = int(d.first_rank)
+        self.local_ranks = int(d.local_ranks)
         self._stream = None
+
+    def set_rank_range(self, first: int, count: int) -> None:
+        """Hold only virtual ranks [first, first+count) in the buffers passed to
+        the per-rank kernels (remaps, fast-axis changes, 1D transforms, scale,
+        copy) -- the layout of one process of a distributed run."""
+        call("a2a_distribution_set_rank_range", self._h, int(first), int(count))
+        self.first_rank, self.local_ranks = int(first), int(count)
 
     # -- reference public fields per rank (a2adistribution.h:8-17) ----------
     def coords(self, rank: int) -> list[int]:
@@ -133,10 +143,11 @@ class a2aDistribution:
         return _torch_dtype(self.precision)
 
     def empty(self, device="cuda"):
-        """A device buffer of ``world_size * nlocal`` elements."""
+        """A device buffer of ``local_ranks * nlocal`` elements (all ranks by
+        default)."""
         import torch
 
-        return torch.empty(self.world_size * self.nlocal, dtype=self.dtype, device=device)
+        return torch.empty(self.local_ranks * self.nlocal, dtype=self.dtype, device=device)
 
     def set_stream(self, stream) -> None:
         """CUDA stream for the calls that take none (a ``torch.cuda.Stream``,
@@ -152,9 +163,9 @@ class a2aDistribution:
             raise ValueError("buffers must be CUDA tensors (or raw device pointers)")
         if t.dtype != self.dtype:
             raise TypeError(f"buffer dtype {t.dtype} does not match the distribution's {self.dtype}")
-        if not t.is_contiguous() or t.numel() != self.world_size * self.nlocal:
-            raise ValueError(f"buffer must be contiguous with world_size*nlocal = {self.world_size * self.nlocal} "
-                             "elements")
+        n = getattr(self, "local_ranks", self.world_size) * self.nlocal
+        if not t.is_contiguous() or t.numel() != n:
+            raise ValueError(f"buffer must be contiguous with local_ranks*nlocal = {n} elements")
         return bufptr(t.data_ptr())
 
     # -- the six steps (a2adistribution.cpp:156-256) -------------------------
@@ -204,6 +215,14 @@ class a2aDistribution:
             self.finalize()
         except Exception:
             pass
+
+
+def decompose(Ng: int, world_size: int) -> dict:
+    """Host-only decomposition: dims, local_grid_size, nlocal (raises
+    A2AError where the reference asserts)."""
+    dims, loc, n = (ctypes.c_int * 3)(), (ctypes.c_int * 3)(), ctypes.c_int64()
+    call("a2a_decompose", int(Ng), int(world_size), dims, loc, ctypes.byref(n))
+    return {"dims": list(dims), "local_grid_size": list(loc), "nlocal": int(n.value)}
 
 
 def write_dims(Ng: int, world_size: int, path: str) -> None:

@@ -44,6 +44,8 @@ class Desc(ctypes.Structure):
         ("precision", ctypes.c_int),
         ("element_bytes", ctypes.c_size_t),
         ("buffer_bytes", ctypes.c_size_t),
+        ("first_rank", ctypes.c_int),
+        ("local_ranks", ctypes.c_int),
     ]
 
 
@@ -59,6 +61,7 @@ SIGNATURES = {
     "a2a_distribution_describe": [_P, ctypes.POINTER(Desc)],
     "a2a_rank_coords": [_P, _I, _I3, _I3],
     "a2a_distribution_set_stream": [_P, _P],
+    "a2a_distribution_set_rank_range": [_P, _I, _I],
     "a2a_get_z_pencils": [_P, _PP, _PP],
     "a2a_return_z_pencils": [_P, _PP, _PP],
     "a2a_get_x_pencils": [_P, _PP, _PP],
@@ -98,6 +101,7 @@ SIGNATURES = {
     "a2a_dfft_destroy": [_P],
     "a2a_dfft_forward_host": [_P, _P, _PP],
     "a2a_dfft_inverse_host": [_P, _P, _PP],
+    "a2a_decompose": [_I, _I, _I3, _I3, ctypes.POINTER(ctypes.c_int64)],
     "a2a_write_dims": [_I, _I, ctypes.c_char_p],
     "a2a_write_rank_dumps": [_I, _I, _I, ctypes.c_char_p, _P, _P, _P],
     "a2a_status_string": [_I],

@@ -116,9 +116,10 @@ SlotGeom slot_geom(const Dist& d, int slot) {
         case a2a::SLOT_Y:  // lines (x, z), element y
             return {d.off[1], d.off[0], d.off[2], d.tw[1], d.ng[1], d.ng[0], d.ng[2], a2a::MODE_BATCH,
                     &d.h_off[1], &d.h_off[0], &d.h_off[2]};
-        default:  // contiguous length-Ng lines of a pencil buffer (cubes)
-            return {d.iota, d.pen_u, d.pen_v, d.tw[0], d.ng[0], d.ng[0], d.ng[0], a2a::MODE_LINE, nullptr, nullptr,
-                    nullptr};
+        default:  // contiguous length-Ng lines of the held ranks' pencil buffers (cubes)
+            return {d.iota, d.pen_u, d.pen_v, d.tw[0], d.ng[0],
+                    int((uint64_t)d.local_ranks * d.nlocal / ((uint64_t)d.ng[0] * d.ng[0])), d.ng[0],
+                    a2a::MODE_LINE, nullptr, nullptr, nullptr};
     }
 }
 
@@ -244,6 +245,8 @@ a2a_status setup_distribution(Dist& d, int nx, int ny, int nz, int P, int block_
     d.ng[1] = ny;
     d.ng[2] = nz;
     d.P = P;
+    d.first_rank = 0;
+    d.local_ranks = P;
     d.block_size = block_size;
     d.prec = prec;
     d.elem_bytes = prec == A2A_C128 ? 16 : 8;
@@ -446,9 +449,20 @@ cudaError_t run_tc_pass(const a2a_dfft* f, int pass, bool inv, void* p, cudaStre
     return cudaLaunchKernel(k.fn, dim3(grid), dim3(k.threads), args, k.smem, st);
 }
 
+a2a_status need_all_ranks(const Dist& d, const char* what) {
+    if (d.local_ranks != d.P)
+        return fail(A2A_ERROR_NOT_IMPLEMENTED,
+                    "%s needs every virtual rank in one buffer; this distribution holds %d of %d (the exchange "
+                    "between processes is the distributed layer's)",
+                    what, d.local_ranks, d.P);
+    return A2A_SUCCESS;
+}
+
 a2a_status check_dfft(a2a_dfft* f, void** data) {
     if (!f) return fail(A2A_ERROR_INVALID_VALUE, "dfft is NULL");
     if (!f->plans_made) return fail(A2A_ERROR_NO_PLANS, "make_plans has not been called");
+    a2a_status s;
+    if ((s = need_all_ranks(f->dist->d, "the fused transform")) != A2A_SUCCESS) return s;
     return check_buf(data, "d_data");
 }
 
@@ -482,6 +496,7 @@ template <typename F> a2a_status step(a2a_distribution* h, void** b1, void** b2,
     if (!h) return fail(A2A_ERROR_INVALID_VALUE, "distribution is NULL");
     Dist& d = h->d;
     a2a_status s;
+    if ((s = need_all_ranks(d, "the pencil steps")) != A2A_SUCCESS) return s;
     if ((s = need_cube(d, "the pencil steps")) != A2A_SUCCESS) return s;
     if ((s = check_buf(b1, "d_buff1")) != A2A_SUCCESS) return s;
     if ((s = check_buf(b2, "d_buff2")) != A2A_SUCCESS) return s;
@@ -609,7 +624,9 @@ a2a_status a2a_distribution_describe(const a2a_distribution* h, a2a_distribution
     o->block_size = d.block_size;
     o->precision = (int)d.prec;
     o->element_bytes = d.elem_bytes;
-    o->buffer_bytes = (size_t)d.P * d.nlocal * d.elem_bytes;
+    o->buffer_bytes = (size_t)d.local_ranks * d.nlocal * d.elem_bytes;
+    o->first_rank = d.first_rank;
+    o->local_ranks = d.local_ranks;
     return A2A_SUCCESS;
 }
 
@@ -698,7 +715,23 @@ static a2a_status one_kernel(a2a_distribution* h, void** src, void** dst, cudaEr
 }
 
 a2a_status a2a_alltoall(a2a_distribution* h, void** src, void** dst) {
+    if (h) {
+        const a2a_status s = need_all_ranks(h->d, "the alltoall");
+        if (s != A2A_SUCCESS) return s;
+    }
     return one_kernel(h, src, dst, [](Dist& d, void* a, void* b) { return a2a::launch_alltoall(d, a, b, d.stream); });
+}
+
+a2a_status a2a_distribution_set_rank_range(a2a_distribution* h, int first, int count) {
+    if (!h) return fail(A2A_ERROR_INVALID_VALUE, "distribution is NULL");
+    Dist& d = h->d;
+    if (first < 0 || count < 1 || first + count > d.P)
+        return fail(A2A_ERROR_INVALID_VALUE, "rank range [%d, %d) outside [0, %d)", first, first + count, d.P);
+    if (d.cube && ((uint64_t)count * d.nlocal) % ((uint64_t)d.ng[0] * d.ng[0]))
+        return fail(A2A_ERROR_UNSUPPORTED, "%d ranks do not hold whole sets of Ng pencils of length Ng", count);
+    d.first_rank = first;
+    d.local_ranks = count;
+    return A2A_SUCCESS;
 }
 a2a_status a2a_d_z_a2a_to_z_pencils(a2a_distribution* h, void** src, void** dst) {
     return one_kernel(h, src, dst,
@@ -762,7 +795,7 @@ a2a_status a2a_fast_copy_fft(a2a_distribution* h, void** d_out, void** d_data) {
     a2a_status s;
     if ((s = check_buf(d_out, "d_out")) != A2A_SUCCESS) return s;
     if ((s = check_buf(d_data, "d_data")) != A2A_SUCCESS) return s;
-    A2A_CUDA(cudaMemcpyAsync(d_out[0], d_data[0], (size_t)d.P * d.nlocal * d.elem_bytes, cudaMemcpyDeviceToDevice,
+    A2A_CUDA(cudaMemcpyAsync(d_out[0], d_data[0], (size_t)d.local_ranks * d.nlocal * d.elem_bytes, cudaMemcpyDeviceToDevice,
                              d.stream),
              "cudaMemcpyAsync");
     return finish(d, d.stream, true);
@@ -970,6 +1003,14 @@ static a2a_status host_decomp(int ng, int P, int dims[3], int local[3], long lon
         return fail(A2A_ERROR_DECOMPOSITION, "a face of the brick is not divisible by world_size=%d", P);
     *nlocal = lx * ly * lz;
     return A2A_SUCCESS;
+}
+
+a2a_status a2a_decompose(int ng, int world_size, int dims[3], int local_grid_size[3], int64_t* nlocal) {
+    if (!dims || !local_grid_size || !nlocal) return fail(A2A_ERROR_INVALID_VALUE, "NULL argument");
+    long long n = 0;
+    const a2a_status s = host_decomp(ng, world_size, dims, local_grid_size, &n);
+    *nlocal = (int64_t)n;
+    return s;
 }
 
 a2a_status a2a_write_dims(int ng, int world_size, const char* path) {

@@ -29,6 +29,10 @@ enum SlotId { SLOT_Z = 0, SLOT_X = 1, SLOT_Y = 2, SLOT_LINES = 3, NSLOTS = 4 };
 struct Dist {
     int ng[3] = {0, 0, 0};
     int P = 0;
+    // virtual ranks held in the caller's buffers: [first_rank, first_rank +
+    // local_ranks); all P unless a2a_distribution_set_rank_range narrowed it
+    int first_rank = 0;
+    int local_ranks = 0;
     int dims[3] = {0, 0, 0};
     int local[3] = {0, 0, 0};
     uint64_t nlocal = 0;

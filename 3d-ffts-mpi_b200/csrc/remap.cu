@@ -144,7 +144,7 @@ static PencilGeom pencil_geom(const Dist& d, int axis) {
 template <typename V>
 static cudaError_t remap_t(const Dist& d, int axis, bool unpack, const void* src, void* dst, cudaStream_t st) {
     const PencilGeom g = pencil_geom(d, axis);
-    const uint64_t total = uint64_t(d.P) * d.nlocal;
+    const uint64_t total = uint64_t(d.local_ranks) * d.nlocal;
     const int grid = grid_for(total, 256, d.sms);
     if (unpack)
         pencil_remap_kernel<V, true><<<grid, 256, 0, st>>>(static_cast<const V*>(src), static_cast<V*>(dst), g, total);
@@ -161,7 +161,7 @@ cudaError_t launch_pencil_remap(const Dist& d, int axis, bool unpack, const void
 
 template <typename V>
 static cudaError_t transpose_t(const Dist& d, const TransposeGeom& t, const void* src, void* dst, cudaStream_t st) {
-    dim3 grid(unsigned(((t.A + 31) / 32) * ((t.C + 31) / 32)), unsigned(t.M), unsigned(d.P));
+    dim3 grid(unsigned(((t.A + 31) / 32) * ((t.C + 31) / 32)), unsigned(t.M), unsigned(d.local_ranks));
     transpose_kernel<V><<<grid, 256, 0, st>>>(static_cast<const V*>(src), static_cast<V*>(dst), t);
     return cudaGetLastError();
 }
@@ -187,7 +187,7 @@ cudaError_t launch_fast_axis(const Dist& d, int which, const void* src, void* ds
 }
 
 cudaError_t launch_scale(const Dist& d, const void* src, void* dst, double divisor, cudaStream_t st) {
-    const uint64_t n = uint64_t(d.P) * d.nlocal;
+    const uint64_t n = uint64_t(d.local_ranks) * d.nlocal;
     const int grid = grid_for(n, 256, d.sms);
     if (d.prec == A2A_C128)
         scale_kernel<double2, double><<<grid, 256, 0, st>>>(static_cast<const double2*>(src),

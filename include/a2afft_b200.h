@@ -73,7 +73,9 @@ typedef struct a2a_distribution_desc {
     int block_size;         /* the reference's CUDA block size argument */
     int precision;          /* a2a_precision */
     size_t element_bytes;   /* 16 (C128) or 8 (C64) */
-    size_t buffer_bytes;    /* world_size * nlocal * element_bytes */
+    size_t buffer_bytes;    /* local_ranks * nlocal * element_bytes */
+    int first_rank;         /* virtual ranks held in the caller's buffers: */
+    int local_ranks;        /* [first_rank, first_rank + local_ranks), all by default */
 } a2a_distribution_desc;
 
 typedef struct a2a_distribution a2a_distribution; /* a2aDistribution */
@@ -99,6 +101,17 @@ a2a_status a2a_distribution_describe(const a2a_distribution* dist, a2a_distribut
 
 /* rank2coords + get_local_grid_start (a2adistribution.cpp:55-83). */
 a2a_status a2a_rank_coords(const a2a_distribution* dist, int rank, int coords[3], int local_start[3]);
+
+/* Narrows the buffers this process passes to the per-rank kernels (the
+ * remaps, fast-axis changes, 1D transforms, scale, copy) to virtual ranks
+ * [first, first + count): the layout when the P ranks are spread over
+ * several processes/GPUs, each holding a contiguous block (the per-rank
+ * kernels are identical for every rank).  The alltoall, the six steps and the
+ * fused transform need all P ranks in one buffer and then return
+ * A2A_ERROR_NOT_IMPLEMENTED; the exchange between processes is done by the
+ * caller (see 3d-ffts-mpi_b200/distributed.py).  No reference counterpart:
+ * there every process is one rank. */
+a2a_status a2a_distribution_set_rank_range(a2a_distribution* dist, int first, int count);
 
 /* Stream used by the calls below that take no stream (NULL = default). */
 a2a_status a2a_distribution_set_stream(a2a_distribution* dist, void* cuda_stream);
@@ -226,6 +239,14 @@ a2a_status a2a_dfft_destroy(a2a_dfft* dfft);
  * of the plan's size), transformed there and copied back, synchronously. */
 a2a_status a2a_dfft_forward_host(a2a_dfft* dfft, void* host_data, void** d_buffer);
 a2a_status a2a_dfft_inverse_host(a2a_dfft* dfft, void* host_data, void** d_buffer);
+
+/* ---- host-only decomposition -------------------------------------------- */
+
+/* The decomposition a2a_distribution_create would make (dims =
+ * MPI_Dims_create(world_size, 3), local brick, nlocal) and its validation,
+ * on the host only: for processes that have no device or have not created
+ * one yet.  No reference counterpart as a separate call. */
+a2a_status a2a_decompose(int ng, int world_size, int dims[3], int local_grid_size[3], int64_t* nlocal);
 
 /* ---- dump files ---------------------------------------------------------- */
 
