@@ -43,6 +43,8 @@ __all__ = [
     "A2AError",
     "a2aDistribution",
     "a2adfft",
+    "a2aBatch",
+    "batch_shapes",
     "forward_1d_fft",
     "inverse_1d_fft",
     "scale_fft",
@@ -383,3 +385,141 @@ class a2adfft:
             self.destroy()
         except Exception:
             pass
+
+
+BATCH_EDGES = (32, 48, 64, 96, 128, 192)
+
+
+def batch_shapes(cubes: int = 96, seed: int = 3, boxes=((128, 256, 512), (128, 256, 512))):
+    """Shapes of the measured batch workload: ``cubes`` cubes whose edges are
+    drawn uniformly from 32 48 64 96 128 192 with a seeded generator, then
+    the fixed anisotropic boxes."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    edges = rng.choice(np.array(BATCH_EDGES), size=cubes)
+    return [(int(e),) * 3 for e in edges] + [tuple(int(v) for v in b) for b in boxes]
+
+
+class a2aBatch:
+    """Many independent boxes transformed together: one persistent kernel
+    launch per direction, replayed from a CUDA graph.  No reference
+    counterpart (the reference plans one grid at a time); box ``b`` has the
+    layout ``a2aDistribution(world_size, shapes[b])`` gives it and its
+    transform equals that distribution's ``a2adfft`` forward / inverse.
+
+    ``shapes``: list of ``(nx, ny, nz)`` (or ints for cubes); every edge one of
+    32 48 64 96 128 192 256 512."""
+
+    def __init__(self, shapes, world_size: int = 4, precision: str = "c64"):
+        self.shapes = [tuple(int(v) for v in ((s,) * 3 if isinstance(s, int) else s)) for s in shapes]
+        self.world_size = int(world_size)
+        self.precision = precision
+        if precision not in _PREC:
+            raise ValueError(f"precision must be one of {sorted(_PREC)}")
+        self._prec = _PREC[precision]
+        flat = [v for s in self.shapes for v in s]
+        arr = (ctypes.c_int * len(flat))(*flat)
+        h = ctypes.c_void_p()
+        call("a2a_batch_create", len(self.shapes), arr, self.world_size, self._prec, ctypes.byref(h))
+        self._h = h
+        self.elements = []
+        for b in range(len(self.shapes)):
+            n = ctypes.c_int64()
+            call("a2a_batch_box_elements", self._h, b, ctypes.byref(n))
+            self.elements.append(n.value)
+
+    @property
+    def nboxes(self) -> int:
+        return len(self.shapes)
+
+    @property
+    def dtype(self):
+        return _torch_dtype(self._prec)
+
+    def offsets(self, align_elems: int = 32) -> list[int]:
+        """Element offsets of the boxes packed into one flat buffer, each
+        rounded up to ``align_elems`` (256 bytes for complex64 at 32)."""
+        out, pos = [], 0
+        for n in self.elements:
+            out.append(pos)
+            pos += (n + align_elems - 1) // align_elems * align_elems
+        return out + [pos]
+
+    def empty(self, device="cuda"):
+        """(flat tensor, per-box views): every box in one allocation."""
+        import torch
+
+        offs = self.offsets()
+        flat = torch.empty(offs[-1], dtype=self.dtype, device=device)
+        views = [flat[offs[b]:offs[b] + self.elements[b]] for b in range(self.nboxes)]
+        return flat, views
+
+    def _ptrs(self, bufs):
+        if len(bufs) != self.nboxes:
+            raise ValueError(f"expected {self.nboxes} buffers, got {len(bufs)}")
+        vals = []
+        for b, t in enumerate(bufs):
+            if isinstance(t, int):
+                vals.append(t)
+                continue
+            if not t.is_cuda or t.dtype != self.dtype or t.numel() < self.elements[b] or not t.is_contiguous():
+                raise ValueError(f"box {b}: expected a contiguous CUDA {self.dtype} tensor of >= "
+                                 f"{self.elements[b]} elements")
+            vals.append(t.data_ptr())
+        return (ctypes.c_void_p * self.nboxes)(*vals)
+
+    def make_plans(self, d_scratch=None) -> None:
+        call("a2a_batch_make_plans", self._h, None if d_scratch is None else self._ptrs(d_scratch))
+
+    def set_schedule(self, fused: bool = True, claim: int = 2) -> None:
+        call("a2a_batch_set_schedule", self._h, int(bool(fused)), int(claim))
+
+    def select_variant(self, length: int, batch_mode: bool, variant: int) -> None:
+        call("a2a_batch_select_variant", self._h, int(length), int(bool(batch_mode)), int(variant))
+
+    def set_graph(self, enable: bool) -> None:
+        call("a2a_batch_set_graph", self._h, int(bool(enable)))
+
+    def inject_stall(self, enable: bool) -> None:
+        call("a2a_batch_inject_stall", self._h, int(bool(enable)))
+
+    def plan_report(self) -> str:
+        buf = ctypes.create_string_buffer(1 << 16)
+        call("a2a_batch_plan_report", self._h, buf, len(buf))
+        return buf.value.decode()
+
+    def forward(self, d_data, stream=None) -> None:
+        if stream is None:
+            call("a2a_batch_forward", self._h, self._ptrs(d_data))
+        else:
+            handle = getattr(stream, "cuda_stream", stream)
+            call("a2a_batch_forward_async", self._h, self._ptrs(d_data), ctypes.c_void_p(handle))
+
+    def inverse(self, d_data, stream=None) -> None:
+        if stream is None:
+            call("a2a_batch_inverse", self._h, self._ptrs(d_data))
+        else:
+            handle = getattr(stream, "cuda_stream", stream)
+            call("a2a_batch_inverse_async", self._h, self._ptrs(d_data), ctypes.c_void_p(handle))
+
+    def check_device(self) -> None:
+        call("a2a_batch_check_device", self._h)
+
+    @property
+    def launches_per_transform(self) -> int:
+        n = ctypes.c_int()
+        call("a2a_batch_launches_per_transform", self._h, ctypes.byref(n))
+        return n.value
+
+    def destroy(self) -> None:
+        if self._h:
+            call("a2a_batch_destroy", self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+

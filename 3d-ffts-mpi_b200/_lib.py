@@ -104,6 +104,21 @@ SIGNATURES = {
     "a2a_decompose": [_I, _I, _I3, _I3, ctypes.POINTER(ctypes.c_int64)],
     "a2a_write_dims": [_I, _I, ctypes.c_char_p],
     "a2a_write_rank_dumps": [_I, _I, _I, ctypes.c_char_p, _P, _P, _P],
+    "a2a_batch_create": [_I, ctypes.POINTER(_I), _I, _I, ctypes.POINTER(_P)],
+    "a2a_batch_box_elements": [_P, _I, ctypes.POINTER(ctypes.c_int64)],
+    "a2a_batch_make_plans": [_P, _PP],
+    "a2a_batch_set_schedule": [_P, _I, _I],
+    "a2a_batch_select_variant": [_P, _I, _I, _I],
+    "a2a_batch_set_graph": [_P, _I],
+    "a2a_batch_inject_stall": [_P, _I],
+    "a2a_batch_plan_report": [_P, ctypes.c_char_p, ctypes.c_size_t],
+    "a2a_batch_forward": [_P, _PP],
+    "a2a_batch_inverse": [_P, _PP],
+    "a2a_batch_forward_async": [_P, _PP, _P],
+    "a2a_batch_inverse_async": [_P, _PP, _P],
+    "a2a_batch_check_device": [_P],
+    "a2a_batch_launches_per_transform": [_P, ctypes.POINTER(_I)],
+    "a2a_batch_destroy": [_P],
     "a2a_status_string": [_I],
     "a2a_last_error": [],
     "a2a_version": [],

@@ -16,6 +16,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include "batch.cuh"
 #include "fft_tc.cuh"
 #include "internal.h"
 
@@ -1101,5 +1102,505 @@ const char* a2a_status_string(a2a_status s) {
 const char* a2a_last_error(void) { return g_last_error.c_str(); }
 
 int a2a_version(void) { return A2AFFT_B200_VERSION; }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched form: many independent boxes (each decomposed over its own virtual
+// ranks, as a2a_distribution_create_box lays them out) transformed by one
+// persistent kernel launch per direction, replayed from a CUDA graph.  No
+// counterpart in the reference, which transforms one grid per plan.
+// ---------------------------------------------------------------------------
+
+struct a2a_batch {
+    a2a_precision prec = A2A_C64;
+    int P = 0;
+    int nboxes = 0;
+    int sms = 148;
+    std::vector<a2a_distribution*> dists;  // one per distinct box shape (offset tables, twiddles)
+    std::vector<int> box_dist;             // box -> index into dists
+    std::vector<a2a::BatchBox> hbox;
+    std::vector<int2> items;               // (box * 4 + pass, tile), pass-major
+    int pass_start[4] = {0, 0, 0, 0};
+    a2a::BatchBox* d_boxes = nullptr;
+    int2* d_items = nullptr;
+    size_t items_cap = 0;
+    // queue scratch: [0] abort, [1..3] items taken per launch, [4..] tiles
+    // done per (box, pass); then the error flag (outside the cleared range)
+    int* d_queue = nullptr;
+    size_t queue_ints = 0;
+    int var[2][a2a::kBatchNumLengths] = {};  // tile variant per (mode, length)
+    bool used[2][a2a::kBatchNumLengths] = {};
+    float tuned_ms[2][a2a::kBatchNumLengths][2] = {};
+    int fused = 1;   // 1: one launch per direction; 0: one launch per pass
+    int claim = 2;
+    int wait_extra = 0;
+    bool use_graph = true;
+    size_t smem = 0;
+    int grid = 0;
+    cudaStream_t cap = nullptr;
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    std::vector<void*> bound;  // data pointers held in d_boxes
+};
+
+namespace {
+
+int batch_len_index(int n) {
+    for (int i = 0; i < a2a::kBatchNumLengths; ++i)
+        if (a2a::kBatchLengths[i] == n) return i;
+    return -1;
+}
+
+void batch_drop_graphs(a2a_batch* b) {
+    for (auto& e : b->exec)
+        if (e) {
+            cudaGraphExecDestroy(e);
+            e = nullptr;
+        }
+}
+
+// Per-pass geometry of box i: transform length, lines NU x NV (as slot_geom).
+void batch_pass_geom(const a2a_batch* b, int i, int pass, int& n, int& NU, int& NV) {
+    const Dist& d = b->dists[b->box_dist[i]]->d;
+    if (pass == 0) { n = d.ng[2]; NU = d.ng[0]; NV = d.ng[1]; }
+    else if (pass == 1) { n = d.ng[0]; NU = d.ng[1]; NV = d.ng[2]; }
+    else { n = d.ng[1]; NU = d.ng[0]; NV = d.ng[2]; }
+}
+
+// Tiles per pass, the item list, launch shared memory and grid from the
+// current variants; uploads the box table and the items.
+a2a_status batch_layout(a2a_batch* b) {
+    batch_drop_graphs(b);
+    b->items.clear();
+    size_t smem = 0;
+    for (int p = 0; p < 3; ++p) {
+        b->pass_start[p] = (int)b->items.size();
+        for (int i = 0; i < b->nboxes; ++i) {
+            int n, NU, NV;
+            batch_pass_geom(b, i, p, n, NU, NV);
+            const int mode = p == 0 ? a2a::MODE_LINE : a2a::MODE_BATCH;
+            const int li = batch_len_index(n);
+            const int v = b->var[mode][li];
+            const int lines = a2a::batch_tile_lines(b->prec, n, v);
+            if (lines <= 0 || NV % lines)
+                return fail(A2A_ERROR_UNSUPPORTED, "box %d: %d lines per tile do not divide %d", i, lines, NV);
+            a2a::BatchBox& bx = b->hbox[i];
+            bx.var[p] = v;
+            bx.tiles[p] = NU * (NV / lines);
+            smem = std::max(smem, a2a::batch_tile_smem(b->prec, n, v, mode));
+            if ((int64_t)b->items.size() + bx.tiles[p] >= (int64_t(1) << 30))
+                return fail(A2A_ERROR_UNSUPPORTED, "the batch has too many tiles");
+            for (int t = 0; t < bx.tiles[p]; ++t) b->items.push_back(make_int2(i * 4 + p, t));
+        }
+    }
+    b->pass_start[3] = (int)b->items.size();
+    b->smem = smem;
+    const void* fn = a2a::batch_kernel(b->prec, false);
+    int occ = 0;
+    A2A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, a2a::kBatchThreads, smem),
+             "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    if (occ < 1) return fail(A2A_ERROR_UNSUPPORTED, "the batched kernel does not fit an SM with %zu bytes", smem);
+    b->grid = std::max(1, std::min(b->pass_start[3], occ * b->sms));
+    if (b->items.size() > b->items_cap) {
+        if (b->d_items) cudaFree(b->d_items);
+        b->d_items = nullptr;
+        b->items_cap = 0;
+        A2A_CUDA(cudaMalloc(&b->d_items, b->items.size() * sizeof(int2)), "cudaMalloc(batch items)");
+        b->items_cap = b->items.size();
+    }
+    if (!b->items.empty())
+        A2A_CUDA(cudaMemcpy(b->d_items, b->items.data(), b->items.size() * sizeof(int2), cudaMemcpyHostToDevice),
+                 "cudaMemcpy(batch items)");
+    A2A_CUDA(cudaMemcpy(b->d_boxes, b->hbox.data(), b->hbox.size() * sizeof(a2a::BatchBox), cudaMemcpyHostToDevice),
+             "cudaMemcpy(batch boxes)");
+    return A2A_SUCCESS;
+}
+
+// Enqueues one direction: clear the queue counters, then the persistent
+// launch (or one launch per pass).
+cudaError_t batch_launches(a2a_batch* b, bool inv, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(b->d_queue, 0, b->queue_ints * sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    const void* fn = a2a::batch_kernel(b->prec, inv);
+    a2a::BatchArgs a;
+    a.boxes = b->d_boxes;
+    a.items = b->d_items;
+    a.claim = b->claim;
+    a.fused = b->fused;
+    a.wait_extra = b->wait_extra;
+    a.abort = b->d_queue;
+    a.done = b->d_queue + 4;
+    a.err = b->d_queue + b->queue_ints;
+    const int launches = b->fused ? 1 : 3;
+    for (int k = 0; k < launches && e == cudaSuccess; ++k) {
+        a.item_lo = b->fused ? 0 : b->pass_start[k];
+        a.item_hi = b->fused ? b->pass_start[3] : b->pass_start[k + 1];
+        a.taken = b->d_queue + 1 + k;
+        const int grid = std::max(1, std::min(a.item_hi - a.item_lo, b->grid));
+        void* args[] = {&a};
+        e = cudaLaunchKernel(fn, dim3(grid), dim3(a2a::kBatchThreads), args, b->smem, st);
+    }
+    return e;
+}
+
+a2a_status batch_capture(a2a_batch* b) {
+    batch_drop_graphs(b);
+    if (!b->use_graph) return A2A_SUCCESS;
+    for (int inv = 0; inv < 2; ++inv) {
+        cudaGraph_t g = nullptr;
+        A2A_CUDA(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+        const cudaError_t e = batch_launches(b, inv != 0, b->cap);
+        const cudaError_t e2 = cudaStreamEndCapture(b->cap, &g);
+        if (e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return cuda_fail(e, "batched launch (capture)");
+        }
+        A2A_CUDA(e2, "cudaStreamEndCapture");
+        const cudaError_t e3 = cudaGraphInstantiate(&b->exec[inv], g, 0);
+        cudaGraphDestroy(g);
+        A2A_CUDA(e3, "cudaGraphInstantiate");
+    }
+    return A2A_SUCCESS;
+}
+
+// Points the device box table at the caller's buffers (only when they changed).
+a2a_status batch_bind(a2a_batch* b, void** data, cudaStream_t st) {
+    if (!data) return fail(A2A_ERROR_INVALID_VALUE, "d_data is NULL");
+    bool changed = false;
+    for (int i = 0; i < b->nboxes; ++i) {
+        if (!data[i]) return fail(A2A_ERROR_INVALID_VALUE, "d_data[%d] is NULL", i);
+        if (reinterpret_cast<uintptr_t>(data[i]) % 16)
+            return fail(A2A_ERROR_MISALIGNED, "d_data[%d] is not 16-byte aligned", i);
+        if (b->bound[i] != data[i]) changed = true;
+    }
+    if (!changed) return A2A_SUCCESS;
+    for (int i = 0; i < b->nboxes; ++i) {
+        b->bound[i] = data[i];
+        b->hbox[i].data = data[i];
+    }
+    // pageable source: the call returns once the table is staged, and the
+    // copy is ordered before the launches that follow on `st`
+    A2A_CUDA(cudaMemcpyAsync(b->d_boxes, b->hbox.data(), b->hbox.size() * sizeof(a2a::BatchBox),
+                             cudaMemcpyHostToDevice, st),
+             "cudaMemcpyAsync(batch boxes)");
+    return A2A_SUCCESS;
+}
+
+a2a_status batch_check_flag(a2a_batch* b) {
+    int flag = 0;
+    int* err = b->d_queue + b->queue_ints;
+    A2A_CUDA(cudaMemcpy(&flag, err, sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy(error flag)");
+    if (flag) {
+        A2A_CUDA(cudaMemset(err, 0, sizeof(int)), "cudaMemset(error flag)");
+        return fail(A2A_ERROR_TIMEOUT, "a batched work item's bounded wait for the previous pass of its box gave up");
+    }
+    return A2A_SUCCESS;
+}
+
+a2a_status batch_run(a2a_batch* b, void** data, bool inv, cudaStream_t st, bool sync) {
+    if (!b) return fail(A2A_ERROR_INVALID_VALUE, "batch is NULL");
+    a2a_status s;
+    if ((s = batch_bind(b, data, st)) != A2A_SUCCESS) return s;
+    if (b->use_graph) {
+        if (!b->exec[0] && (s = batch_capture(b)) != A2A_SUCCESS) return s;
+        A2A_CUDA(cudaGraphLaunch(b->exec[inv ? 1 : 0], st), "cudaGraphLaunch");
+    } else {
+        A2A_CUDA(batch_launches(b, inv, st), "batched launch");
+    }
+    if (!sync) return A2A_SUCCESS;
+    A2A_CUDA(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+    return batch_check_flag(b);
+}
+
+void batch_free(a2a_batch* b) {
+    if (!b) return;
+    batch_drop_graphs(b);
+    if (b->cap) cudaStreamDestroy(b->cap);
+    if (b->d_boxes) cudaFree(b->d_boxes);
+    if (b->d_items) cudaFree(b->d_items);
+    if (b->d_queue) cudaFree(b->d_queue);
+    for (a2a_distribution* h : b->dists) {
+        release(h->d);
+        delete h;
+    }
+    delete b;
+}
+
+}  // namespace
+
+extern "C" {
+
+a2a_status a2a_batch_create(int nboxes, const int* shapes, int world_size, a2a_precision precision,
+                            a2a_batch** out) {
+    if (!out) return fail(A2A_ERROR_INVALID_VALUE, "out is NULL");
+    *out = nullptr;
+    if (!shapes) return fail(A2A_ERROR_INVALID_VALUE, "shapes is NULL");
+    if (nboxes < 1 || nboxes > a2a::kBatchMaxBoxes)
+        return fail(A2A_ERROR_INVALID_VALUE, "nboxes must be in [1, %d]", a2a::kBatchMaxBoxes);
+    if (precision != A2A_C128 && precision != A2A_C64)
+        return fail(A2A_ERROR_INVALID_VALUE, "unknown precision %d", (int)precision);
+    for (int i = 0; i < 3 * nboxes; ++i)
+        if (batch_len_index(shapes[i]) < 0)
+            return fail(A2A_ERROR_UNSUPPORTED,
+                        "box %d: edge %d has no batched tile code (supported: 32 48 64 96 128 192 256 512)", i / 3,
+                        shapes[i]);
+    auto* b = new (std::nothrow) a2a_batch();
+    if (!b) return fail(A2A_ERROR_OUT_OF_MEMORY, "host allocation failed");
+    b->prec = precision;
+    b->P = world_size;
+    b->nboxes = nboxes;
+    a2a_status s = A2A_SUCCESS;
+    for (int i = 0; i < nboxes && s == A2A_SUCCESS; ++i) {
+        int k = 0;
+        for (; k < (int)b->dists.size(); ++k) {
+            const Dist& d = b->dists[k]->d;
+            if (d.ng[0] == shapes[3 * i] && d.ng[1] == shapes[3 * i + 1] && d.ng[2] == shapes[3 * i + 2]) break;
+        }
+        if (k == (int)b->dists.size()) {
+            a2a_distribution* h = nullptr;
+            s = create_common(shapes[3 * i], shapes[3 * i + 1], shapes[3 * i + 2], world_size, 64, precision, &h);
+            if (s != A2A_SUCCESS) {
+                const std::string why = g_last_error;
+                s = fail(s, "box %d (%dx%dx%d): %s", i, shapes[3 * i], shapes[3 * i + 1], shapes[3 * i + 2],
+                         why.c_str());
+                break;
+            }
+            b->dists.push_back(h);
+        }
+        b->box_dist.push_back(k);
+    }
+    if (s != A2A_SUCCESS) {
+        batch_free(b);
+        return s;
+    }
+    b->sms = b->dists[0]->d.sms;
+    b->hbox.resize(nboxes);
+    b->bound.assign(nboxes, nullptr);
+    for (int i = 0; i < nboxes; ++i) {
+        const Dist& d = b->dists[b->box_dist[i]]->d;
+        a2a::BatchBox& bx = b->hbox[i];
+        bx.data = nullptr;
+        for (int a = 0; a < 3; ++a) {
+            bx.off[a] = d.off[a];
+            bx.tw[a] = d.tw[a];
+            bx.n[a] = d.ng[a];
+        }
+        for (int p = 0; p < 3; ++p) {
+            const int sl = p;  // SLOT_Z, SLOT_X, SLOT_Y
+            const int axis = p == 0 ? 2 : p == 1 ? 0 : 1;
+            bx.split[p] = split_ok(d.local[axis], d.slot[sl][0].cand[0]);
+            int n, NU, NV;
+            batch_pass_geom(b, i, p, n, NU, NV);
+            b->used[p == 0 ? a2a::MODE_LINE : a2a::MODE_BATCH][batch_len_index(n)] = true;
+        }
+        bx.inv_scale = 1.0 / ((double)d.ng[0] * d.ng[1] * d.ng[2]);
+    }
+    // default variants: the first tile height that divides every pass using it
+    for (int m = 0; m < 2; ++m)
+        for (int li = 0; li < a2a::kBatchNumLengths; ++li) {
+            if (!b->used[m][li]) continue;
+            const int n = a2a::kBatchLengths[li];
+            int pick = -1;
+            for (int v = 0; v < 2 && pick < 0; ++v) {
+                const int lines = a2a::batch_tile_lines(precision, n, v);
+                bool ok = true;
+                for (int i = 0; i < nboxes && ok; ++i)
+                    for (int p = 0; p < 3; ++p) {
+                        int pn, NU, NV;
+                        batch_pass_geom(b, i, p, pn, NU, NV);
+                        const int pm = p == 0 ? a2a::MODE_LINE : a2a::MODE_BATCH;
+                        if (pn == n && pm == m && NV % lines) ok = false;
+                    }
+                if (ok) pick = v;
+            }
+            if (pick < 0) {
+                batch_free(b);
+                return fail(A2A_ERROR_UNSUPPORTED, "no batched tile of length %d divides the boxes' line counts", n);
+            }
+            b->var[m][li] = pick;
+        }
+    const size_t max_smem = a2a::batch_smem(precision);
+    cudaError_t e = cudaSuccess;
+    for (int inv = 0; inv < 2 && e == cudaSuccess; ++inv)
+        e = cudaFuncSetAttribute(a2a::batch_kernel(precision, inv != 0), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)max_smem);
+    b->queue_ints = 4 + 3 * (size_t)nboxes;
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_boxes, sizeof(a2a::BatchBox) * nboxes);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_queue, (b->queue_ints + 1) * sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(b->d_queue, 0, (b->queue_ints + 1) * sizeof(int));
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        batch_free(b);
+        return cuda_fail(e, "batch set-up");
+    }
+    if ((s = batch_layout(b)) != A2A_SUCCESS) {
+        batch_free(b);
+        return s;
+    }
+    *out = b;
+    return A2A_SUCCESS;
+}
+
+a2a_status a2a_batch_box_elements(const a2a_batch* b, int box, int64_t* elements) {
+    if (!b || !elements) return fail(A2A_ERROR_INVALID_VALUE, "NULL argument");
+    if (box < 0 || box >= b->nboxes) return fail(A2A_ERROR_INVALID_VALUE, "box %d outside [0, %d)", box, b->nboxes);
+    const Dist& d = b->dists[b->box_dist[box]]->d;
+    *elements = (int64_t)d.nlocal * d.P;
+    return A2A_SUCCESS;
+}
+
+a2a_status a2a_batch_set_schedule(a2a_batch* b, int fused, int claim) {
+    if (!b) return fail(A2A_ERROR_INVALID_VALUE, "batch is NULL");
+    if (fused != 0 && fused != 1) return fail(A2A_ERROR_INVALID_VALUE, "fused must be 0 or 1");
+    if (claim < 1 || claim > 64) return fail(A2A_ERROR_INVALID_VALUE, "claim must be in [1, 64]");
+    b->fused = fused;
+    b->claim = claim;
+    batch_drop_graphs(b);
+    return A2A_SUCCESS;
+}
+
+a2a_status a2a_batch_select_variant(a2a_batch* b, int length, int batch_mode, int variant) {
+    if (!b) return fail(A2A_ERROR_INVALID_VALUE, "batch is NULL");
+    const int li = batch_len_index(length);
+    if (li < 0 || (batch_mode != 0 && batch_mode != 1) || (variant != 0 && variant != 1))
+        return fail(A2A_ERROR_INVALID_VALUE, "length %d / mode %d / variant %d out of range", length, batch_mode,
+                    variant);
+    const int m = batch_mode ? a2a::MODE_BATCH : a2a::MODE_LINE;
+    const int old = b->var[m][li];
+    b->var[m][li] = variant;
+    const a2a_status s = batch_layout(b);
+    if (s != A2A_SUCCESS) {
+        b->var[m][li] = old;
+        batch_layout(b);
+    }
+    return s;
+}
+
+a2a_status a2a_batch_set_graph(a2a_batch* b, int enable) {
+    if (!b) return fail(A2A_ERROR_INVALID_VALUE, "batch is NULL");
+    b->use_graph = enable != 0;
+    batch_drop_graphs(b);
+    return A2A_SUCCESS;
+}
+
+a2a_status a2a_batch_inject_stall(a2a_batch* b, int enable) {
+    if (!b) return fail(A2A_ERROR_INVALID_VALUE, "batch is NULL");
+    b->wait_extra = enable ? 1 : 0;
+    batch_drop_graphs(b);
+    return A2A_SUCCESS;
+}
+
+a2a_status a2a_batch_make_plans(a2a_batch* b, void** d_scratch) {
+    if (!b) return fail(A2A_ERROR_INVALID_VALUE, "batch is NULL");
+    if (!d_scratch) return A2A_SUCCESS;  // defaults
+    a2a_status s;
+    cudaStream_t st = b->cap;
+    if ((s = batch_bind(b, d_scratch, st)) != A2A_SUCCESS) return s;
+    cudaEvent_t e0, e1;
+    A2A_CUDA(cudaEventCreate(&e0), "cudaEventCreate");
+    A2A_CUDA(cudaEventCreate(&e1), "cudaEventCreate");
+    const bool graph = b->use_graph;
+    b->use_graph = false;
+    // forward + inverse per trial (the inverse keeps the scratch values bounded)
+    auto timed = [&](float* out) -> a2a_status {
+        cudaError_t e = cudaSuccess;
+        float best = 1e30f;
+        for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {
+            e = cudaEventRecord(e0, st);
+            if (e == cudaSuccess) e = batch_launches(b, false, st);
+            if (e == cudaSuccess) e = batch_launches(b, true, st);
+            if (e == cudaSuccess) e = cudaEventRecord(e1, st);
+            if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+            float t = 0.f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+            if (e == cudaSuccess && rep > 0) best = std::min(best, t);
+        }
+        if (e != cudaSuccess) return cuda_fail(e, "batched autotune launch");
+        *out = best;
+        return batch_check_flag(b);
+    };
+    float cur = 0.f;
+    s = timed(&cur);
+    // one sweep over the knobs in use: each length's tile height per mode,
+    // then the schedule (one launch, or one per pass)
+    for (int m = 0; m < 2 && s == A2A_SUCCESS; ++m)
+        for (int li = 0; li < a2a::kBatchNumLengths && s == A2A_SUCCESS; ++li) {
+            if (!b->used[m][li]) continue;
+            const int old = b->var[m][li];
+            b->tuned_ms[m][li][old] = cur;
+            b->var[m][li] = 1 - old;
+            if (batch_layout(b) != A2A_SUCCESS) {  // the other tile does not divide
+                b->var[m][li] = old;
+                s = batch_layout(b);
+                continue;
+            }
+            float t = 0.f;
+            if ((s = timed(&t)) != A2A_SUCCESS) break;
+            b->tuned_ms[m][li][1 - old] = t;
+            if (t < cur) {
+                cur = t;
+            } else {
+                b->var[m][li] = old;
+                s = batch_layout(b);
+            }
+        }
+    if (s == A2A_SUCCESS) {
+        const int old = b->fused;
+        b->fused = 1 - old;
+        float t = 0.f;
+        s = timed(&t);
+        if (s == A2A_SUCCESS && !(t < cur)) b->fused = old;
+    }
+    b->use_graph = graph;
+    batch_drop_graphs(b);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return s;
+}
+
+a2a_status a2a_batch_plan_report(const a2a_batch* b, char* buf, size_t len) {
+    if (!b || !buf || len == 0) return fail(A2A_ERROR_INVALID_VALUE, "NULL argument");
+    std::string r;
+    char line[256];
+    snprintf(line, sizeof line, "boxes=%d world_size=%d precision=%s schedule=%s claim=%d grid=%d smem=%zu items=%d\n",
+             b->nboxes, b->P, b->prec == A2A_C128 ? "c128" : "c64", b->fused ? "one-launch" : "per-pass", b->claim,
+             b->grid, b->smem, b->pass_start[3]);
+    r += line;
+    for (int m = 0; m < 2; ++m)
+        for (int li = 0; li < a2a::kBatchNumLengths; ++li) {
+            if (!b->used[m][li]) continue;
+            const int n = a2a::kBatchLengths[li];
+            snprintf(line, sizeof line, "  N=%d %s lines=%d (tuned ms: %.4f / %.4f)\n", n, m ? "batch" : "line",
+                     a2a::batch_tile_lines(b->prec, n, b->var[m][li]), b->tuned_ms[m][li][0], b->tuned_ms[m][li][1]);
+            r += line;
+        }
+    snprintf(buf, len, "%s", r.c_str());
+    return A2A_SUCCESS;
+}
+
+a2a_status a2a_batch_forward(a2a_batch* b, void** d_data) { return batch_run(b, d_data, false, nullptr, true); }
+a2a_status a2a_batch_inverse(a2a_batch* b, void** d_data) { return batch_run(b, d_data, true, nullptr, true); }
+a2a_status a2a_batch_forward_async(a2a_batch* b, void** d_data, void* stream) {
+    return batch_run(b, d_data, false, static_cast<cudaStream_t>(stream), false);
+}
+a2a_status a2a_batch_inverse_async(a2a_batch* b, void** d_data, void* stream) {
+    return batch_run(b, d_data, true, static_cast<cudaStream_t>(stream), false);
+}
+
+a2a_status a2a_batch_check_device(a2a_batch* b) {
+    if (!b) return fail(A2A_ERROR_INVALID_VALUE, "batch is NULL");
+    return batch_check_flag(b);
+}
+
+a2a_status a2a_batch_launches_per_transform(const a2a_batch* b, int* out) {
+    if (!b || !out) return fail(A2A_ERROR_INVALID_VALUE, "NULL argument");
+    *out = b->fused ? 1 : 3;
+    return A2A_SUCCESS;
+}
+
+a2a_status a2a_batch_destroy(a2a_batch* b) {
+    batch_free(b);
+    return A2A_SUCCESS;
+}
 
 }  // extern "C"

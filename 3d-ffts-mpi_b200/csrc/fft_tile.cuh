@@ -402,12 +402,14 @@ __host__ __device__ constexpr size_t pass_smem_bytes() {
     return bytes;
 }
 
-// KIND_DIRECT: one CTA = one tile of B lines (u, v0 .. v0+B-1).  Stage 0
-// reads global memory straight into registers (j fastest in LINE mode, so
-// the loads coalesce along the line).  With LPT = 2 (BATCH, complex float) a
-// thread moves the same element of two adjacent lines as one 16-byte access.
-template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV, int MINB, int LPT>
-__global__ void __launch_bounds__(THREADS, MINB) fft_pass_kernel(const PassArgs<T> a) {
+// One tile of B lines (u, v0 .. v0+B-1), tile index t = u * (NV/B) + v0/B,
+// in the CTA's dynamic shared memory.  Stage 0 reads global memory straight
+// into registers (j fastest in LINE mode, so the loads coalesce along the
+// line).  With LPT = 2 (BATCH, complex float) a thread moves the same
+// element of two adjacent lines as one 16-byte access.  CG: read through L2
+// only (for data another CTA of the same launch has just written).
+template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV, int LPT, bool CG = false>
+__device__ __forceinline__ void direct_tile(const PassArgs<T>& a, int t, unsigned char* smem_raw, int tid) {
     using E = typename ElemOf<T, LPT>::type;
     constexpr int BV = B / LPT;
     using G = TileGeom<MODE, BV, PLAN::N, sizeof(E)>;
@@ -422,17 +424,15 @@ __global__ void __launch_bounds__(THREADS, MINB) fft_pass_kernel(const PassArgs<
     static_assert(MODE != MODE_BATCH || THREADS % BV == 0, "batch mode needs THREADS % (B/LPT) == 0");
     static_assert(LPT == 1 || MODE == MODE_BATCH, "line pairs only in batch mode");
 
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     E* tile = reinterpret_cast<E*>(smem_raw);
     cx<T>* tw = reinterpret_cast<cx<T>*>(tile + G::elems);
     uint32_t* offA_s = reinterpret_cast<uint32_t*>(tw + TWN);
     size_t* base_s = reinterpret_cast<size_t*>(
         smem_raw + ((sizeof(E) * (size_t)G::elems + sizeof(cx<T>) * TWN + sizeof(uint32_t) * N + 15) & ~size_t(15)));
 
-    const int tid = threadIdx.x;
     const int tilesV = a.NV / B;
-    const int u = blockIdx.x / tilesV;
-    const int v0 = (blockIdx.x - u * tilesV) * B;
+    const int u = t / tilesV;
+    const int v0 = (t - u * tilesV) * B;
     const size_t ubase = a.offU[u];
 
     uint32_t d0[R0];
@@ -451,11 +451,16 @@ __global__ void __launch_bounds__(THREADS, MINB) fft_pass_kernel(const PassArgs<
             if (a.split) {
                 const cx<T>* p = line + __ldg(a.offA + j);
 #pragma unroll
-                for (int r = 0; r < R0; ++r) x[k][r] = ld_stream(reinterpret_cast<const E*>(p + d0[r]));
+                for (int r = 0; r < R0; ++r) {
+                    const E* ptr = reinterpret_cast<const E*>(p + d0[r]);
+                    x[k][r] = CG ? __ldcg(ptr) : ld_stream(ptr);
+                }
             } else {
 #pragma unroll
-                for (int r = 0; r < R0; ++r)
-                    x[k][r] = ld_stream(reinterpret_cast<const E*>(line + __ldg(a.offA + j + r * NBL)));
+                for (int r = 0; r < R0; ++r) {
+                    const E* ptr = reinterpret_cast<const E*>(line + __ldg(a.offA + j + r * NBL));
+                    x[k][r] = CG ? __ldcg(ptr) : ld_stream(ptr);
+                }
             }
         }
     }
@@ -493,6 +498,13 @@ __global__ void __launch_bounds__(THREADS, MINB) fft_pass_kernel(const PassArgs<
         __syncthreads();
         run_stage<T, PLAN, B, THREADS, MODE, INV, LPT, 1>(a, tile, tw, offA_s, base_s, tid);
     }
+}
+
+// KIND_DIRECT: one CTA = one tile.
+template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV, int MINB, int LPT>
+__global__ void __launch_bounds__(THREADS, MINB) fft_pass_kernel(const PassArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    direct_tile<T, PLAN, B, THREADS, MODE, INV, LPT>(a, blockIdx.x, smem_raw, threadIdx.x);
 }
 
 // KIND_RPIPE: persistent CTAs double-buffer through registers.  Stage 0 of

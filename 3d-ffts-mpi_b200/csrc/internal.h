@@ -69,4 +69,12 @@ cudaError_t launch_pencil_remap(const Dist& d, int axis, bool unpack, const void
 cudaError_t launch_fast_axis(const Dist& d, int which, const void* src, void* dst, cudaStream_t st);
 cudaError_t launch_scale(const Dist& d, const void* src, void* dst, double divisor, cudaStream_t st);
 
+// batch.cu: the batched persistent kernel per (precision, direction), its
+// dynamic shared memory, and the tile height of a length's variant (0: the
+// length has no batched tile code)
+const void* batch_kernel(a2a_precision prec, bool inverse);
+size_t batch_smem(a2a_precision prec);
+int batch_tile_lines(a2a_precision prec, int n, int variant);
+size_t batch_tile_smem(a2a_precision prec, int n, int variant, int mode);
+
 }  // namespace a2a

@@ -265,6 +265,55 @@ a2a_status a2a_write_dims(int ng, int world_size, const char* path);
 a2a_status a2a_write_rank_dumps(int ng, int world_size, a2a_precision precision, const char* folder,
                                 const void* host_input, const void* host_forward, const void* host_inverse);
 
+/* ---- batched form --------------------------------------------------------- */
+
+/* Many independent boxes transformed together: one persistent kernel launch
+ * per direction (replayed from a CUDA graph) works through every tile of
+ * every box, the X and Y tiles of a box starting once the box's previous
+ * pass is done.  No counterpart in the reference, which plans one grid at a
+ * time; each box has exactly the layout a2a_distribution_create_box(nx, ny,
+ * nz, world_size, ...) gives it (world_size virtual ranks, rank-major
+ * bricks), and its transform equals that distribution's a2a_dfft_forward /
+ * a2a_dfft_inverse (the inverse scaled by 1/(nx ny nz)). */
+typedef struct a2a_batch a2a_batch;
+
+/* shapes: nboxes triples (nx, ny, nz); every edge one of 32 48 64 96 128 192
+ * 256 512.  Boxes of one shape share their offset tables. */
+a2a_status a2a_batch_create(int nboxes, const int* shapes, int world_size, a2a_precision precision,
+                            a2a_batch** out);
+/* Complex elements of box `box`'s buffer (world_size * nlocal). */
+a2a_status a2a_batch_box_elements(const a2a_batch* batch, int box, int64_t* elements);
+/* Optional tuning on caller buffers d_scratch[0..nboxes) (clobbered): for
+ * each transform length in use, the tile height per access mode, then the
+ * schedule.  NULL keeps the defaults. */
+a2a_status a2a_batch_make_plans(a2a_batch* batch, void** d_scratch);
+/* fused = 1: one launch per direction (later passes wait, device-side, for
+ * the earlier pass of their box); 0: one launch per pass.  claim: work items
+ * a CTA takes per queue access (1..64). */
+a2a_status a2a_batch_set_schedule(a2a_batch* batch, int fused, int claim);
+/* Tile height choice (0 or 1) for one length in line (batch_mode = 0, the Z
+ * pass) or batch mode (the X and Y passes). */
+a2a_status a2a_batch_select_variant(a2a_batch* batch, int length, int batch_mode, int variant);
+/* 1 (default): replay a captured CUDA graph; 0: plain launches. */
+a2a_status a2a_batch_set_graph(a2a_batch* batch, int enable);
+/* Test hook for the timeout path: every device-side wait asks for one tile
+ * more than its pass has, so it gives up (after about a second) and the next
+ * synchronising call returns A2A_ERROR_TIMEOUT.  0 restores normal runs. */
+a2a_status a2a_batch_inject_stall(a2a_batch* batch, int enable);
+a2a_status a2a_batch_plan_report(const a2a_batch* batch, char* buf, size_t len);
+/* d_data[b]: box b's device buffer (16-byte aligned).  Synchronous forms
+ * check the device error flag; the _async forms only enqueue on `stream`.
+ * Calls of one batch object share its queue scratch: calls that overlap on
+ * the GPU race. */
+a2a_status a2a_batch_forward(a2a_batch* batch, void** d_data);
+a2a_status a2a_batch_inverse(a2a_batch* batch, void** d_data);
+a2a_status a2a_batch_forward_async(a2a_batch* batch, void** d_data, void* stream);
+a2a_status a2a_batch_inverse_async(a2a_batch* batch, void** d_data, void* stream);
+/* Reads and clears the batch's device error flag (A2A_ERROR_TIMEOUT if set). */
+a2a_status a2a_batch_check_device(a2a_batch* batch);
+a2a_status a2a_batch_launches_per_transform(const a2a_batch* batch, int* out);
+a2a_status a2a_batch_destroy(a2a_batch* batch);
+
 /* ---- misc --------------------------------------------------------------- */
 
 const char* a2a_status_string(a2a_status status);

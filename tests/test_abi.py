@@ -70,6 +70,17 @@ def test_invalid_arguments_without_gpu(pkg):
     assert lib.a2a_dfft_make_plans(None, None) == 1
     assert lib.a2a_distribution_finalize(None) == 0
     assert lib.a2a_dfft_destroy(None) == 0
+    # batched form: shape validation happens before any device work
+    shapes = (ctypes.c_int * 6)(32, 32, 32, 64, 40, 64)
+    assert lib.a2a_batch_create(2, shapes, 4, 1, ctypes.byref(h)) == 3  # edge 40: no batched tile
+    assert b"edge 40" in lib.a2a_last_error()
+    assert lib.a2a_batch_create(0, shapes, 4, 1, ctypes.byref(h)) == 1
+    assert lib.a2a_batch_create(1, None, 4, 1, ctypes.byref(h)) == 1
+    assert lib.a2a_batch_create(1, shapes, 4, 5, ctypes.byref(h)) == 1
+    assert lib.a2a_batch_create(1, shapes, 3, 1, ctypes.byref(h)) == 2  # 32 over dims [3,1,1]
+    assert b"box 0" in lib.a2a_last_error()
+    assert lib.a2a_batch_forward(None, None) == 1
+    assert lib.a2a_batch_destroy(None) == 0
 
 
 def test_python_mirror_rejects_bad_precision(pkg):
