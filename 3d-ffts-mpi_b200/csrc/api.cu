@@ -598,6 +598,12 @@ a2a_status setup_tc(a2a_dfft* f, a2a_method m) {
 
 }  // namespace
 
+namespace a2a {
+a2a_status record_error(a2a_status s, const char* what, const char* detail) {
+    return fail(s, "%s: %s", what, detail);
+}
+}  // namespace a2a
+
 extern "C" {
 
 a2a_status a2a_distribution_create(int ng, int world_size, int block_size, a2a_precision precision,

@@ -69,6 +69,9 @@ cudaError_t launch_pencil_remap(const Dist& d, int axis, bool unpack, const void
 cudaError_t launch_fast_axis(const Dist& d, int which, const void* src, void* dst, cudaStream_t st);
 cudaError_t launch_scale(const Dist& d, const void* src, void* dst, double divisor, cudaStream_t st);
 
+// api.cu: records "<what>: <detail>" for a2a_last_error and returns s
+a2a_status record_error(a2a_status s, const char* what, const char* detail);
+
 // batch.cu: the batched persistent kernel per (precision, direction), its
 // dynamic shared memory, and the tile height of a length's variant (0: the
 // length has no batched tile code)

@@ -162,6 +162,25 @@ a2a_status a2a_distribution_finalize(a2a_distribution* dist);
 a2a_status a2a_forward_1d_fft(a2a_distribution* dist, void** d_data);
 a2a_status a2a_inverse_1d_fft(a2a_distribution* dist, void** d_data);
 
+/* No counterpart in the reference.  The same in-place, unnormalised
+ * transform of `nlines` contiguous lines of length n (n one of 4 8 12 16 24
+ * 32 48 64 96 128 192 256 384 512 768 1024; nlines a multiple of 4) without
+ * any distribution object, for callers that cannot allocate device memory:
+ * an application whose memory manager reserved the device's memory up front,
+ * or a latency-bound path that cannot take cudaMalloc's implicit
+ * synchronisation.  It allocates nothing: its offset and twiddle tables live
+ * in a fixed file-scope device array of A2A_LINES_NOALLOC_SCRATCH_BYTES,
+ * which every GPU that loads the library holds until the process exits.
+ * The first call on a device resolves that array's address (with the device
+ * current); make that first call before any stream capture.  Each call
+ * rebuilds the tables on `stream` and then transforms; calls share the array,
+ * so calls that overlap on the GPU race.  Sizes whose tables exceed the
+ * array (more than about 64K groups of up to 1024 lines) return
+ * A2A_ERROR_UNSUPPORTED.  Enqueue only: the caller synchronises. */
+#define A2A_LINES_NOALLOC_SCRATCH_BYTES (256u * 1024u)
+a2a_status a2a_lines_fft_noalloc(void* data, int n, int64_t nlines, a2a_precision precision, int inverse,
+                                 void* stream);
+
 /* launch_scale_fft (a2affts.cu:78-92, 108-116): out = data / Ng^3. */
 a2a_status a2a_scale_fft(a2a_distribution* dist, void** d_out, void** d_data);
 /* launch_fast_copy_fft (a2affts.cu:94-106, 118-125): out = data. */
