@@ -108,7 +108,7 @@ SIGNATURES = {
     "a2a_batch_create": [_I, ctypes.POINTER(_I), _I, _I, ctypes.POINTER(_P)],
     "a2a_batch_box_elements": [_P, _I, ctypes.POINTER(ctypes.c_int64)],
     "a2a_batch_make_plans": [_P, _PP],
-    "a2a_batch_set_schedule": [_P, _I, _I],
+    "a2a_batch_set_schedule": [_P, _I, _I, _I],
     "a2a_batch_select_variant": [_P, _I, _I, _I],
     "a2a_batch_set_graph": [_P, _I],
     "a2a_batch_inject_stall": [_P, _I],

@@ -1139,8 +1139,9 @@ struct a2a_batch {
     bool used[2][a2a::kBatchNumLengths] = {};
     float tuned_ms[2][a2a::kBatchNumLengths][2] = {};
     int fused = 1;   // 1: one launch per direction; 0: one launch per pass
-    int claim = 2;
+    int claim = 16;
     int wait_extra = 0;
+    int prefetch = 1;
     bool use_graph = true;
     size_t smem = 0;
     int grid = 0;
@@ -1192,6 +1193,7 @@ a2a_status batch_layout(a2a_batch* b) {
                 return fail(A2A_ERROR_UNSUPPORTED, "box %d: %d lines per tile do not divide %d", i, lines, NV);
             a2a::BatchBox& bx = b->hbox[i];
             bx.var[p] = v;
+            bx.lines[p] = lines;
             bx.tiles[p] = NU * (NV / lines);
             smem = std::max(smem, a2a::batch_tile_smem(b->prec, n, v, mode));
             if ((int64_t)b->items.size() + bx.tiles[p] >= (int64_t(1) << 30))
@@ -1234,6 +1236,7 @@ cudaError_t batch_launches(a2a_batch* b, bool inv, cudaStream_t st) {
     a.claim = b->claim;
     a.fused = b->fused;
     a.wait_extra = b->wait_extra;
+    a.prefetch = b->prefetch;
     a.abort = b->d_queue;
     a.done = b->d_queue + 4;
     a.err = b->d_queue + b->queue_ints;
@@ -1400,6 +1403,17 @@ a2a_status a2a_batch_create(int nboxes, const int* shapes, int world_size, a2a_p
             b->used[p == 0 ? a2a::MODE_LINE : a2a::MODE_BATCH][batch_len_index(n)] = true;
         }
         bx.inv_scale = 1.0 / ((double)d.ng[0] * d.ng[1] * d.ng[2]);
+        // the offset tables' closed form (setup_distribution)
+        const uint32_t nl = (uint32_t)d.nlocal;
+        bx.lext[0] = d.local[0];
+        bx.rstride[0] = (uint32_t)(d.dims[1] * d.dims[2]) * nl;
+        bx.lstride[0] = (uint32_t)(d.local[1] * d.local[2]);
+        bx.lext[1] = d.local[1];
+        bx.rstride[1] = (uint32_t)d.dims[2] * nl;
+        bx.lstride[1] = (uint32_t)d.local[2];
+        bx.lext[2] = d.local[2];
+        bx.rstride[2] = nl;
+        bx.lstride[2] = 1;
     }
     // default variants: the first tile height that divides every pass using it
     for (int m = 0; m < 2; ++m)
@@ -1455,12 +1469,14 @@ a2a_status a2a_batch_box_elements(const a2a_batch* b, int box, int64_t* elements
     return A2A_SUCCESS;
 }
 
-a2a_status a2a_batch_set_schedule(a2a_batch* b, int fused, int claim) {
+a2a_status a2a_batch_set_schedule(a2a_batch* b, int fused, int claim, int prefetch) {
     if (!b) return fail(A2A_ERROR_INVALID_VALUE, "batch is NULL");
     if (fused != 0 && fused != 1) return fail(A2A_ERROR_INVALID_VALUE, "fused must be 0 or 1");
     if (claim < 1 || claim > 64) return fail(A2A_ERROR_INVALID_VALUE, "claim must be in [1, 64]");
+    if (prefetch != 0 && prefetch != 1) return fail(A2A_ERROR_INVALID_VALUE, "prefetch must be 0 or 1");
     b->fused = fused;
     b->claim = claim;
+    b->prefetch = prefetch;
     batch_drop_graphs(b);
     return A2A_SUCCESS;
 }
@@ -1550,13 +1566,22 @@ a2a_status a2a_batch_make_plans(a2a_batch* b, void** d_scratch) {
                 s = batch_layout(b);
             }
         }
-    if (s == A2A_SUCCESS) {
-        const int old = b->fused;
-        b->fused = 1 - old;
+    // the schedule: one launch or one per pass, items per queue access, L2
+    // prefetch of the next tile
+    auto try_knob = [&](int* knob, int value) {
+        if (s != A2A_SUCCESS || *knob == value) return;
+        const int old = *knob;
+        *knob = value;
         float t = 0.f;
         s = timed(&t);
-        if (s == A2A_SUCCESS && !(t < cur)) b->fused = old;
-    }
+        if (s == A2A_SUCCESS && t < cur)
+            cur = t;
+        else
+            *knob = old;
+    };
+    try_knob(&b->fused, 1 - b->fused);
+    for (int c : {4, 8, 16, 32, 64}) try_knob(&b->claim, c);
+    try_knob(&b->prefetch, 1 - b->prefetch);
     b->use_graph = graph;
     batch_drop_graphs(b);
     cudaEventDestroy(e0);
@@ -1568,9 +1593,10 @@ a2a_status a2a_batch_plan_report(const a2a_batch* b, char* buf, size_t len) {
     if (!b || !buf || len == 0) return fail(A2A_ERROR_INVALID_VALUE, "NULL argument");
     std::string r;
     char line[256];
-    snprintf(line, sizeof line, "boxes=%d world_size=%d precision=%s schedule=%s claim=%d grid=%d smem=%zu items=%d\n",
+    snprintf(line, sizeof line,
+             "boxes=%d world_size=%d precision=%s schedule=%s claim=%d prefetch=%d grid=%d smem=%zu items=%d\n",
              b->nboxes, b->P, b->prec == A2A_C128 ? "c128" : "c64", b->fused ? "one-launch" : "per-pass", b->claim,
-             b->grid, b->smem, b->pass_start[3]);
+             b->prefetch, b->grid, b->smem, b->pass_start[3]);
     r += line;
     for (int m = 0; m < 2; ++m)
         for (int li = 0; li < a2a::kBatchNumLengths; ++li) {

@@ -40,7 +40,12 @@ struct BatchBox {
     const void* tw[3];       // stage twiddles per axis (forward sign)
     int n[3];                // edges
     int var[3];              // tile variant per pass (Z, X, Y)
+    int lines[3];            // tile height per pass
     int tiles[3];            // tiles per pass
+    // off[a][x] = (x / lext[a]) * rstride[a] + (x % lext[a]) * lstride[a]
+    // (brick extent, rank stride, in-brick stride): prefetch addresses
+    // without table loads
+    uint32_t lext[3], rstride[3], lstride[3];
     int split[3];            // split addressing usable per pass
     double inv_scale;        // 1 / (nx ny nz)
 };
@@ -52,21 +57,106 @@ struct BatchArgs {
     const BatchBox* boxes;
     const int2* items;
     int item_lo, item_hi;
-    int claim;               // items a CTA takes per queue access
+    int claim;               // most items a CTA takes per queue access
     int fused;               // 1: later passes wait for the earlier pass of their box
     int wait_extra;          // 0; > 0 makes every wait unsatisfiable (tests of the timeout path)
+    int prefetch;            // 1: prefetch the CTA's next tile into L2 while running the current one
     int* taken;              // items taken so far
     int* abort;              // raised when a wait gave up: every CTA stops
     int* done;               // tiles finished per (box, pass), 3 ints per box
     int* err;                // set to 1 when a wait gave up (not cleared by launches)
 };
 
-// One tile of one configuration, compiled as its own function so that each
+// A run of m consecutive tiles t0 .. t0+m-1 of one pass of one box, with the
+// register double-buffering of the persistent pass kernel: stage 0 of tile t
+// leaves its results in shared memory, then its registers receive the global
+// loads of tile t+1, which stay in flight through stages 1..S-1 of tile t.
+// Loads read through L2 only (__ldcg): other CTAs of this launch wrote the
+// data (earlier passes).
+template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV>
+__device__ __forceinline__ void rpipe_run(const PassArgs<T>& a, int t0, int m, unsigned char* smem_raw, int tid) {
+    using E = cx<T>;
+    using G = TileGeom<MODE, B, PLAN::N, sizeof(E)>;
+    constexpr int N = PLAN::N;
+    constexpr int R0 = PLAN::r[0];
+    constexpr int NBL = N / R0;
+    constexpr int NBT = B * NBL;
+    constexpr int K = (NBT + THREADS - 1) / THREADS;
+    constexpr bool EXACT = (NBT % THREADS) == 0;
+    constexpr int TWN = PLAN::twtotal();
+    constexpr bool BFAST0 = (MODE == MODE_BATCH);
+    static_assert(PLAN::S >= 2, "the pipelined run needs at least two stages");
+    static_assert(MODE != MODE_BATCH || THREADS % B == 0, "batch mode needs THREADS % B == 0");
+
+    E* tile = reinterpret_cast<E*>(smem_raw);
+    cx<T>* tw = reinterpret_cast<cx<T>*>(tile + G::elems);
+    uint32_t* offA_s = reinterpret_cast<uint32_t*>(tw + TWN);
+    size_t* base_s = reinterpret_cast<size_t*>(
+        smem_raw + ((sizeof(E) * (size_t)G::elems + sizeof(cx<T>) * TWN + sizeof(uint32_t) * N + 15) & ~size_t(15)));
+
+    const int tilesV = a.NV / B;
+    uint32_t d0[R0];
+    if (a.split) {
+#pragma unroll
+        for (int r = 0; r < R0; ++r) d0[r] = __ldg(a.offA + r * NBL);
+    }
+    auto load_tile = [&](int t, E (&x)[K][R0]) {
+        const int u = t / tilesV;
+        const int v0 = (t - u * tilesV) * B;
+        const size_t ubase = __ldg(a.offU + u);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int q = tid + k * THREADS;
+            if (EXACT || q < NBT) {
+                int b, j;
+                bf_map<BFAST0, B, NBL>(q, b, j);
+                const cx<T>* line = a.src + ubase + __ldg(a.offV + v0 + b);
+                if (a.split) {
+                    const cx<T>* p = line + __ldg(a.offA + j);
+#pragma unroll
+                    for (int r = 0; r < R0; ++r) x[k][r] = __ldcg(p + d0[r]);
+                } else {
+#pragma unroll
+                    for (int r = 0; r < R0; ++r) x[k][r] = __ldcg(line + __ldg(a.offA + j + r * NBL));
+                }
+            }
+        }
+    };
+    E x[K][R0];
+    load_tile(t0, x);
+    for (int i = tid; i < TWN; i += THREADS) tw[i] = a.tw[i];
+    for (int i = tid; i < N; i += THREADS) offA_s[i] = a.offA[i];
+    for (int t = t0; t < t0 + m; ++t) {
+        {
+            const int u = t / tilesV;
+            const int v0 = (t - u * tilesV) * B;
+            const size_t ubase = __ldg(a.offU + u);
+            for (int i = tid; i < B; i += THREADS) base_s[i] = ubase + __ldg(a.offV + v0 + i);
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int q = tid + k * THREADS;
+            if (EXACT || q < NBT) {
+                int b, j;
+                bf_map<BFAST0, B, NBL>(q, b, j);
+                Dft<R0, INV, E>::run(x[k]);
+#pragma unroll
+                for (int r = 0; r < R0; ++r) tile[G::idx(b, j * R0 + r)] = x[k][r];
+            }
+        }
+        if (t + 1 < t0 + m) load_tile(t + 1, x);  // in flight through the remaining stages
+        __syncthreads();
+        run_stage<T, PLAN, B, THREADS, MODE, INV, 1, 1>(a, tile, tw, offA_s, base_s, tid);
+        __syncthreads();  // tile and line bases free for the next tile
+    }
+}
+
+// A run of one configuration, compiled as its own function so that each
 // configuration gets its own register allocation (inlined into one body they
 // would share the worst case and spill).
 template <typename T, bool INV, int N, int V, int MODE>
 __device__ __noinline__ void batch_tile(cx<T>* data, const uint32_t* offA, const uint32_t* offU, const uint32_t* offV,
-                                        const cx<T>* tw, int NU, int NV, T scale, int split, int tile,
+                                        const cx<T>* tw, int NU, int NV, T scale, int split, int tile, int count,
                                         unsigned char* smem, int tid) {
     using P = typename PassPlan<T, N>::Plan;
     PassArgs<T> pa;
@@ -82,14 +172,15 @@ __device__ __noinline__ void batch_tile(cx<T>* data, const uint32_t* offA, const
     pa.split = split;
     pa.err = nullptr;
     pa.tcb = nullptr;
-    direct_tile<T, P, batch_lines<T>(N, V), kBatchThreads, MODE, INV, 1, true>(pa, tile, smem, tid);
+    rpipe_run<T, P, batch_lines<T>(N, V), kBatchThreads, MODE, INV>(pa, tile, count, smem, tid);
 }
 
 template <typename T, bool INV, int N>
 __device__ __forceinline__ void batch_len(cx<T>* data, const uint32_t* offA, const uint32_t* offU,
                                           const uint32_t* offV, const cx<T>* tw, int NU, int NV, T scale, int split,
-                                          int mode, int var, int tile, unsigned char* smem, int tid) {
-#define A2A_BT(V_, M_) batch_tile<T, INV, N, V_, M_>(data, offA, offU, offV, tw, NU, NV, scale, split, tile, smem, tid)
+                                          int mode, int var, int tile, int count, unsigned char* smem, int tid) {
+#define A2A_BT(V_, M_) \
+    batch_tile<T, INV, N, V_, M_>(data, offA, offU, offV, tw, NU, NV, scale, split, tile, count, smem, tid)
     if (mode == MODE_LINE) {
         if (var == 0) A2A_BT(0, MODE_LINE); else A2A_BT(1, MODE_LINE);
     } else {
@@ -113,36 +204,98 @@ __device__ __forceinline__ bool wait_count(const int* ctr, int target, const int
     return false;
 }
 
-// The persistent kernel.  Thread 0 takes `claim` consecutive items per queue
-// access and, in the fused schedule, checks an item's dependency (every tile
-// of the previous pass of its box done) once per (box, pass) change, with an
-// acquire fence after the wait; a finished tile is published by a release
-// (fence, then the counter increment) after the CTA barrier.  An item waits
-// only on items taken before it, so the lowest unfinished taken item always
-// runs and the waits end.
+__device__ __forceinline__ uint32_t box_off(const BatchBox& bx, int a, uint32_t x) {
+    const uint32_t q = x / bx.lext[a];
+    return q * bx.rstride[a] + (x - q * bx.lext[a]) * bx.lstride[a];
+}
+
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p));
+}
+
+// Asks L2 for the 128-byte lines of one tile (every address is an element of
+// the tile, so nothing outside the box is touched).
+template <typename T>
+__device__ __forceinline__ void prefetch_tile(const BatchBox& bx, int pass, int tile, int tid) {
+    constexpr int EPL = 128 / (int)sizeof(cx<T>);  // elements per 128-byte line
+    const int ax = pass == 0 ? 2 : pass == 1 ? 0 : 1;
+    const int au = pass == 1 ? 1 : 0;
+    const int av = pass == 0 ? 1 : 2;
+    const int N = bx.n[ax], B = bx.lines[pass];
+    const int tilesV = bx.n[av] / B;
+    const int u = tile / tilesV, v0 = (tile - u * tilesV) * B;
+    const cx<T>* base = static_cast<const cx<T>*>(bx.data) + box_off(bx, au, u);
+    if (pass == 0) {  // B lines, contiguous along the transform axis
+        const int cpl = (N + EPL - 1) / EPL;
+        for (int q = tid; q < B * cpl; q += kBatchThreads) {
+            const int b = q / cpl, c = q - b * cpl;
+            prefetch_l2(base + box_off(bx, av, v0 + b) + box_off(bx, ax, c * EPL));
+        }
+    } else {  // N rows of B adjacent lines
+        const int cpr = (B + EPL - 1) / EPL;
+        for (int q = tid; q < N * cpr; q += kBatchThreads) {
+            const int j = q / cpr, c = q - j * cpr;
+            prefetch_l2(base + box_off(bx, ax, j) + box_off(bx, av, v0 + c * EPL));
+        }
+    }
+}
+
+// The persistent kernel.  Thread 0 takes up to `claim` consecutive items per
+// queue access (fewer as the queue drains); the CTA runs them as runs of consecutive tiles of one (box, pass).
+// In the fused schedule thread 0 checks a run's dependency (every tile of the
+// previous pass of its box done) once per (box, pass) change, with an acquire
+// fence after the wait, and publishes finished tiles per (box, pass) with a
+// release (fence, then one counter increment).  It
+// publishes before it waits and before it takes more items, so a CTA never
+// waits while holding unpublished tiles; an item waits only on items taken
+// before it, so the lowest unfinished taken item always runs and the waits
+// end.
 template <typename T, bool INV>
 __global__ void __launch_bounds__(kBatchThreads, 2) fft_batch_kernel(const BatchArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ int s_box, s_pass, s_tile, s_go;
+    __shared__ int s_box, s_pass, s_tile, s_count, s_nbox, s_npass, s_ntile;
     const int tid = threadIdx.x;
-    int next = 0, held = 0;          // thread 0: taken items not yet run
+    int next = 0, end = 0;           // thread 0: taken items not yet run
     int ok_box = -1, ok_pass = -1;   // thread 0: last dependency seen complete
+    int pend_box = 0, pend_pass = 0, pend = 0;  // thread 0: finished, unpublished tiles
+    auto publish = [&]() {
+        if (pend) {
+            __threadfence();
+            atomicAdd(a.done + 3 * pend_box + pend_pass, pend);
+            pend = 0;
+        }
+    };
     for (;;) {
         if (tid == 0) {
-            int go = -1, box = 0, pass = 0, tile = 0;
-            if (held == 0) {
-                next = a.item_lo + atomicAdd(a.taken, a.claim);
-                held = a.claim;
+            int count = -1, box = 0, pass = 0, tile = 0, nbox = -1, npass = 0, ntile = 0;
+            if (next >= end) {
+                if (a.fused) publish();
+                // guided claims: up to `claim` items, fewer as the queue
+                // drains, so the last runs end close together
+                const int left = (a.item_hi - a.item_lo) - *reinterpret_cast<volatile int*>(a.taken);
+                const int c = max(1, min(a.claim, left / (2 * (int)gridDim.x)));
+                next = a.item_lo + atomicAdd(a.taken, c);
+                end = next + c;
             }
-            const int i = next++;
-            --held;
+            const int i = next;
             if (i < a.item_hi && !*reinterpret_cast<volatile int*>(a.abort)) {
                 const int2 it = a.items[i];
                 box = it.x >> 2;
                 pass = it.x & 3;
                 tile = it.y;
-                go = 1;
+                // the run: taken items of the same (box, pass), whose tiles
+                // are consecutive in the item list
+                const int stop = min(min(end, a.item_hi), i - tile + a.boxes[box].tiles[pass]);
+                count = stop - i;
+                next = stop;
+                if (a.prefetch && next < end && next < a.item_hi) {
+                    const int2 nt = a.items[next];
+                    nbox = nt.x >> 2;
+                    npass = nt.x & 3;
+                    ntile = nt.y;
+                }
                 if (a.fused && pass > 0 && (box != ok_box || pass != ok_pass)) {
+                    publish();
                     if (wait_count(a.done + 3 * box + pass - 1, a.boxes[box].tiles[pass - 1] + a.wait_extra,
                                    a.abort)) {
                         __threadfence();
@@ -151,18 +304,24 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fft_batch_kernel(const Batch
                     } else {
                         atomicExch(a.err, 1);
                         atomicExch(a.abort, 1);
-                        go = -1;
+                        count = -1;
                     }
                 }
             }
-            s_go = go;
+            if (count < 0 && a.fused) publish();
+            s_count = count;
             s_box = box;
             s_pass = pass;
             s_tile = tile;
+            s_nbox = nbox;
+            s_npass = npass;
+            s_ntile = ntile;
         }
         __syncthreads();
-        if (s_go < 0) break;
+        const int count = s_count;
+        if (count < 0) break;
         const int box = s_box, pass = s_pass, tile = s_tile;
+        if (s_nbox >= 0) prefetch_tile<T>(a.boxes[s_nbox], s_npass, s_ntile, tid);
         {
             const BatchBox& bx = a.boxes[box];
             // pass 0 = Z (lines (x, y)), 1 = X (lines (y, z)), 2 = Y (lines (x, z))
@@ -178,7 +337,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fft_batch_kernel(const Batch
 #define A2A_BATCH_CASE(N_)                                                                                         \
     case N_:                                                                                                       \
         batch_len<T, INV, N_>(data, bx.off[ax], bx.off[au], bx.off[av], tw, bx.n[au], bx.n[av], scale,             \
-                              bx.split[pass], mode, var, tile, smem, tid);                                         \
+                              bx.split[pass], mode, var, tile, count, smem, tid);                                  \
         break;
                 A2A_BATCH_FOR_EACH_N(A2A_BATCH_CASE)
 #undef A2A_BATCH_CASE
@@ -188,8 +347,10 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fft_batch_kernel(const Batch
         }
         __syncthreads();
         if (tid == 0 && a.fused) {
-            __threadfence();
-            atomicAdd(a.done + 3 * box + pass, 1);
+            if (pend && (box != pend_box || pass != pend_pass)) publish();
+            pend_box = box;
+            pend_pass = pass;
+            pend += count;
         }
     }
 }

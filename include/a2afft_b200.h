@@ -304,12 +304,14 @@ a2a_status a2a_batch_create(int nboxes, const int* shapes, int world_size, a2a_p
 a2a_status a2a_batch_box_elements(const a2a_batch* batch, int box, int64_t* elements);
 /* Optional tuning on caller buffers d_scratch[0..nboxes) (clobbered): for
  * each transform length in use, the tile height per access mode, then the
- * schedule.  NULL keeps the defaults. */
+ * schedule (one launch or one per pass, claim 4..64, prefetch).  NULL keeps
+ * the defaults. */
 a2a_status a2a_batch_make_plans(a2a_batch* batch, void** d_scratch);
 /* fused = 1: one launch per direction (later passes wait, device-side, for
- * the earlier pass of their box); 0: one launch per pass.  claim: work items
- * a CTA takes per queue access (1..64). */
-a2a_status a2a_batch_set_schedule(a2a_batch* batch, int fused, int claim);
+ * the earlier pass of their box); 0: one launch per pass.  claim: most work
+ * items a CTA takes per queue access (1..64; fewer as the queue drains).  prefetch = 1: each CTA asks L2 for
+ * its next tile while it transforms the current one. */
+a2a_status a2a_batch_set_schedule(a2a_batch* batch, int fused, int claim, int prefetch);
 /* Tile height choice (0 or 1) for one length in line (batch_mode = 0, the Z
  * pass) or batch mode (the X and Y passes). */
 a2a_status a2a_batch_select_variant(a2a_batch* batch, int length, int batch_mode, int variant);

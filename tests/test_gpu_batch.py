@@ -73,8 +73,9 @@ def test_batch_matches_single_grid_plan(pkg, oracle, cuda):
     torch.cuda.synchronize()
 
 
-@pytest.mark.parametrize("fused,claim,graph", [(1, 1, True), (1, 4, True), (0, 2, True), (1, 2, False), (0, 1, False)])
-def test_batch_schedules_agree_bitwise(pkg, oracle, cuda, fused, claim, graph):
+@pytest.mark.parametrize("fused,claim,prefetch,graph", [(1, 1, 1, True), (1, 4, 0, True), (0, 2, 1, True),
+                                                        (1, 8, 1, False), (0, 1, 0, False)])
+def test_batch_schedules_agree_bitwise(pkg, oracle, cuda, fused, claim, prefetch, graph):
     """The schedule only orders the same tiles: results are bit-identical."""
     import torch
 
@@ -86,7 +87,7 @@ def test_batch_schedules_agree_bitwise(pkg, oracle, cuda, fused, claim, graph):
     ref_b.forward(views)
     ref_b.inverse(views)
     b = pkg.a2aBatch(SMALL, P, prec)
-    b.set_schedule(fused=bool(fused), claim=claim)
+    b.set_schedule(fused=bool(fused), claim=claim, prefetch=bool(prefetch))
     b.set_graph(graph)
     assert b.launches_per_transform == (1 if fused else 3)
     s = torch.cuda.Stream()
