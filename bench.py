@@ -67,17 +67,24 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg")
     ap.add_argument("--no-check", action="store_true", help="skip the accuracy check (profiling runs)")
     ap.add_argument("--workload", choices=["cube", "batch"], default="cube")
+    ap.add_argument("--batch-cubes", type=int, default=96, help="batch workload: number of drawn cubes")
+    ap.add_argument("--batch-big", type=int, default=2, help="batch workload: number of 128x256x512 boxes")
+    ap.add_argument("--no-tune", action="store_true", help="batch workload: default plan, no make_plans timing "
+                    "(profiling runs)")
+    ap.add_argument("--precision", choices=["c64", "c128"], default="c64", help="cube workload element type")
+    ap.add_argument("--seed", type=int, default=None, help="cube workload seed (default 2; 4 for the large sizes)")
     ap.add_argument("--variants", default=None,
                     help="Z,X,Y launch-variant indices instead of timing them all in make_plans (profiling runs)")
     return ap.parse_args()
 
 
-def workload_name(ng, ranks, dims):
-    return (f"{ng}^3 complex64 C2C forward+inverse, {ranks} virtual ranks (dims {dims}), "
-            f"U[-1,1)+3 tones x100 seed {SEED}")
+def workload_name(ng, ranks, dims, precision="c64", seed=SEED, tones=3):
+    cname = "complex128" if precision == "c128" else "complex64"
+    inp = f"U[-1,1)+{tones} tones x100" if tones else "U[-1,1)"
+    return f"{ng}^3 {cname} C2C forward+inverse, {ranks} virtual ranks (dims {dims}), {inp} seed {seed}"
 
 
-def cpu_pipeline_ms(ng_sample, ranks, ng_target, reps=1):
+def cpu_pipeline_ms(ng_sample, ranks, ng_target, reps=1, precision="c64", seed=SEED, tones=3):
     """The reference's host step sequence (oracle port) on one cube of
     ng_sample^3, best of `reps`, scaled to ng_target^3 by N log N."""
     import numpy as np
@@ -86,19 +93,21 @@ def cpu_pipeline_ms(ng_sample, ranks, ng_target, reps=1):
 
     O = entry.load_oracle()
     cores = os.cpu_count() or 1
+    cdt = np.complex128 if precision == "c128" else np.complex64
     d = O.Decomp(ng_sample, ranks)
-    g = O.make_input("uniform", (ng_sample,) * 3, seed=SEED, dtype=np.complex64, tones=3)
+    g = O.make_input("uniform", (ng_sample,) * 3, seed=seed, dtype=cdt, tones=tones)
     b = O.global_to_bricks(g, d)
     lines = O.scipy_lines(cores)
     best = float("inf")
     for _ in range(reps):
         t0 = time.perf_counter()
-        f = O.forward(b, d, lines, np.complex64)
-        O.inverse(f, d, lines, np.complex64)
+        f = O.forward(b, d, lines, cdt)
+        O.inverse(f, d, lines, cdt)
         best = min(best, time.perf_counter() - t0)
     n_s, n_t = float(ng_sample) ** 3, float(ng_target) ** 3
     scale = (n_t * math.log2(n_t)) / (n_s * math.log2(n_s))
-    sample = (f"one forward+inverse of a {ng_sample}^3 complex64 cube on {ranks} virtual ranks "
+    cname = "complex128" if precision == "c128" else "complex64"
+    sample = (f"one forward+inverse of a {ng_sample}^3 {cname} cube on {ranks} virtual ranks "
               f"(dims {d.dims}), best of {reps}, x{scale:.3f} (N log N) to {ng_target}^3")
     return best * 1e3 * scale, cores, sample, best
 
@@ -192,20 +201,21 @@ def profiled_traffic(kernel_key):
     return None
 
 
-def synth_bricks(torch, ng, dims, seed, device):
-    """Seeded U[-1,1) re/im + 3 tones of amplitude 100, generated on the GPU,
-    returned in the rank-major brick layout."""
+def synth_bricks(torch, ng, dims, seed, device, real=None, tones=3):
+    """Seeded U[-1,1) re/im + `tones` pure tones of amplitude 100, generated
+    on the GPU, returned in the rank-major brick layout."""
+    real = real or torch.float32
     gen = torch.Generator(device=device).manual_seed(seed)
     shape = (ng, ng, ng)
-    re = torch.rand(shape, generator=gen, device=device, dtype=torch.float32) * 2 - 1
-    im = torch.rand(shape, generator=gen, device=device, dtype=torch.float32) * 2 - 1
+    re = torch.rand(shape, generator=gen, device=device, dtype=real) * 2 - 1
+    im = torch.rand(shape, generator=gen, device=device, dtype=real) * 2 - 1
     g = torch.complex(re, im)
     del re, im
-    ks = torch.randint(0, ng, (3, 3), generator=gen, device=device)
+    ks = torch.randint(0, ng, (tones, 3), generator=gen, device=device)
     idx = torch.arange(ng, device=device, dtype=torch.int64)
     for kx, ky, kz in ks.tolist():
         ph = ((kx * idx)[:, None, None] + (ky * idx)[None, :, None] + (kz * idx)[None, None, :]) % ng
-        g += 100.0 * torch.polar(torch.ones((), device=device), ph.to(torch.float32) * (2 * math.pi / ng))
+        g += 100.0 * torch.polar(torch.ones((), device=device, dtype=real), ph.to(real) * (2 * math.pi / ng))
         del ph
     d0, d1, d2 = dims
     lx, ly, lz = ng // d0, ng // d1, ng // d2
@@ -217,6 +227,10 @@ def synth_bricks(torch, ng, dims, seed, device):
 BATCH_METRIC = "batch 96 cubes {32..192}^3 + 2x128x256x512 C2C fwd+inv ms, c64"
 BATCH_RANKS = 4
 BATCH_SEED = 3
+
+
+def batch_shapes(pkg, args):
+    return pkg.batch_shapes(cubes=args.batch_cubes, seed=BATCH_SEED, boxes=[(128, 256, 512)] * args.batch_big)
 
 
 def batch_workload(shapes):
@@ -271,7 +285,7 @@ def run_batch_reference(args, rank, world):
         return
     import __graft_entry__ as entry
 
-    shapes = entry.load_package().batch_shapes(seed=BATCH_SEED)
+    shapes = batch_shapes(entry.load_package(), args)
     times = []
     steps = max(1, min(args.steps, 3))
     for i in range(min(args.warmup, 1) + steps):
@@ -299,12 +313,13 @@ def run_batch(args, rank, world, local_rank):
     pkg = entry.load_package()
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    shapes = pkg.batch_shapes(seed=BATCH_SEED)
+    shapes = batch_shapes(pkg, args)
     b = pkg.a2aBatch(shapes, BATCH_RANKS, "c64")
-    scratch, sviews = b.empty(dev)
-    scratch.normal_()
-    b.make_plans(sviews)  # tile heights per length, schedule, claim, prefetch
-    del scratch, sviews
+    if not args.no_tune:
+        scratch, sviews = b.empty(dev)
+        scratch.normal_()
+        b.make_plans(sviews)  # tile heights per length, schedule, claim, prefetch
+        del scratch, sviews
     plan_report = b.plan_report()
     flat, views = b.empty(dev)
     gen = torch.Generator(device=dev).manual_seed(BATCH_SEED)
@@ -436,6 +451,15 @@ def run_batch(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def cube_input(args):
+    """(seed, tones) of the cube workload: the precision-form input (seed 2,
+    3 tones) at 512^3 and below, plain U[-1,1) with seed 4 for the large
+    sizes."""
+    large = args.ng > 512 or args.precision == "c128"
+    seed = args.seed if args.seed is not None else (4 if large else SEED)
+    return seed, (0 if large else 3)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -443,12 +467,15 @@ def run_reference(args, rank, world):
         run_batch_reference(args, rank, world)
         return
     ng_target = args.ng
+    prec = args.precision
+    seed, tones = cube_input(args)
     # calibrate the sample size so the whole run stays within a few minutes
-    est_ms, cores, _, wall = cpu_pipeline_ms(128, args.ranks, ng_target)
+    est_ms, cores, _, wall = cpu_pipeline_ms(128, args.ranks, ng_target, precision=prec, seed=seed, tones=tones)
     sample_ng = CPU_SAMPLE_NG if wall * 8.5 * (args.steps + args.warmup) < 240 else 128
     times = []
     for i in range(args.warmup + args.steps):
-        ms, cores, sample, _ = cpu_pipeline_ms(sample_ng, args.ranks, ng_target)
+        ms, cores, sample, _ = cpu_pipeline_ms(sample_ng, args.ranks, ng_target, precision=prec, seed=seed,
+                                               tones=tones)
         if i >= args.warmup:
             times.append(ms)
     value = statistics.mean(times)
@@ -458,9 +485,9 @@ def run_reference(args, rank, world):
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "ms", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(value, 3), "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": workload_name(ng_target, args.ranks, dims), "ng": ng_target,
-                   "world_size": args.ranks, "precision": "c64", "sample_ng": sample_ng},
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == "c128" else "f32", "data": "synthetic",
+        "config": {"workload": workload_name(ng_target, args.ranks, dims, prec, seed, tones), "ng": ng_target,
+                   "world_size": args.ranks, "precision": prec, "sample_ng": sample_ng},
         "cpu_baseline": {"value": round(value, 3), "unit": "ms", "cores": cores, "kind": "port",
                          "sample": sample + "; remaps single-threaded numpy, 1D transforms scipy.fft workers=cores"},
         "e2e": {"value": round(value, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -477,7 +504,10 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     ng, ranks = args.ng, args.ranks
-    dist = pkg.a2aDistribution(ranks, ng, 64, precision="c64")
+    prec = args.precision
+    seed, tones = cube_input(args)
+    esz = 16 if prec == "c128" else 8
+    dist = pkg.a2aDistribution(ranks, ng, 64, precision=prec)
     dfft = pkg.a2adfft(dist, method=args.method)
     if args.variants:
         dfft.make_plans()
@@ -488,7 +518,7 @@ def run_ours(args, rank, world, local_rank):
         dfft.make_plans(scratch)
         del scratch
     plan_report = dfft.plan_report()
-    x = synth_bricks(torch, ng, dist.dims, SEED, dev)
+    x = synth_bricks(torch, ng, dist.dims, seed, dev, torch.float64 if prec == "c128" else torch.float32, tones)
     x0 = x.clone()
     stream = torch.cuda.Stream(device=dev)
     nbytes_buf = x.numel() * x.element_size()
@@ -510,13 +540,14 @@ def run_ours(args, rank, world, local_rank):
     if (world == 1 or rank == 0) and not args.no_check:
         x.copy_(x0)
         dfft.forward(x)
-        d64 = pkg.a2aDistribution(ranks, ng, 64, precision="c128")
-        f64 = pkg.a2adfft(d64)
-        f64.make_plans()
-        y = x0.to(torch.complex128)
-        f64.forward(y)
-        rel_err = float(torch.linalg.vector_norm(x.to(torch.complex128) - y) / torch.linalg.vector_norm(y))
-        del y, f64, d64
+        if prec == "c64":  # against our complex128 transform of the same input
+            d64 = pkg.a2aDistribution(ranks, ng, 64, precision="c128")
+            f64 = pkg.a2adfft(d64)
+            f64.make_plans()
+            y = x0.to(torch.complex128)
+            f64.forward(y)
+            rel_err = float(torch.linalg.vector_norm(x.to(torch.complex128) - y) / torch.linalg.vector_norm(y))
+            del y, f64, d64
         dfft.inverse(x)
         rt_err = float(torch.linalg.vector_norm((x - x0).to(torch.complex128)) /
                        torch.linalg.vector_norm(x0.to(torch.complex128)))
@@ -588,20 +619,20 @@ def run_ours(args, rank, world, local_rank):
     names = ["Z_fwd", "X_fwd", "Y_fwd", "Z_inv", "X_inv", "Y_inv"]
     means = [statistics.mean(v) for v in per_pass]
     dom = max(range(6), key=lambda i: means[i])
-    alg_bytes = 2.0 * float(ng) ** 3 * 8  # one read + one write of the cube per pass
+    alg_bytes = 2.0 * float(ng) ** 3 * esz  # one read + one write of the cube per pass
     achieved = alg_bytes / (means[dom] * 1e-3) / 1e9
-    key = ["line", "batch", "batch"][dom % 3] + f"_{ng}_c64"
+    key = ["line", "batch", "batch"][dom % 3] + f"_{ng}_{prec}"
     traffic = profiled_traffic(key)
     alg_total = 6 * alg_bytes
     value = step_ms / world
     line = {
         "metric": METRIC, "value": round(value, 4), "unit": "ms", "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": round(step_ms, 4), "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == "c128" else "f32", "data": "synthetic",
         "impl": "a2afft_b200",
-        "config": {"workload": workload_name(ng, ranks, dist.dims), "ng": ng, "world_size": ranks,
-                   "dims": dist.dims, "precision": "c64", "method": args.method,
-                   "l2": "inputs 1 GiB > 126 MB L2 (no flush)",
+        "config": {"workload": workload_name(ng, ranks, dist.dims, prec, seed, tones), "ng": ng, "world_size": ranks,
+                   "dims": dist.dims, "precision": prec, "method": args.method,
+                   "l2": f"inputs {nbytes_buf / 2**30:.2f} GiB > 126 MB L2 (no flush)",
                    "replicas": world},
         "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": round(achieved, 1), "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
@@ -612,13 +643,14 @@ def run_ours(args, rank, world, local_rank):
         "hbm_frac": round(alg_total / (step_ms * 1e-3) / 1e9 / peak, 4),
         "transforms_per_s": round(2 * 1e3 / step_ms, 2),
         "gflops": round(2 * 5 * float(ng) ** 3 * math.log2(float(ng) ** 3) / (step_ms * 1e-3) / 1e9, 1),
+        "rel_l2_reference": "our complex128 transform" if prec == "c64" else None,
         "rel_l2_vs_fp64": rel_err, "roundtrip_rel_l2": rt_err,
         "clocks": clk.summary(),
         "gpu_launches": 6 * args.steps,
         "e2e": e2e,
     }
     if world == 1 and not args.no_cpu:
-        ms, cores, sample, _ = cpu_pipeline_ms(CPU_SAMPLE_NG, ranks, ng)
+        ms, cores, sample, _ = cpu_pipeline_ms(CPU_SAMPLE_NG, ranks, ng, precision=prec, seed=seed, tones=tones)
         line["cpu_baseline"] = {"value": round(ms, 1), "unit": "ms", "cores": cores, "kind": "port",
                                 "sample": sample + "; remaps single-threaded numpy, 1D transforms scipy.fft "
                                 "workers=cores"}
