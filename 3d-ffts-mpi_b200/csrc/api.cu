@@ -9,6 +9,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -124,12 +125,116 @@ SlotGeom slot_geom(const Dist& d, int slot) {
     }
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the
+// library does not link the driver library itself).
+using TmapEncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+TmapEncodeFn tmap_encoder() {
+    static TmapEncodeFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<TmapEncodeFn>(p);
+    });
+    return fn;
+}
+
+// Largest divisor of `ext` whose box edge (w words per element) is at most 256
+// words and a whole number of 16-byte units when `inner`.
+int tmat_chunk(int ext, int w, bool inner) {
+    for (int c = std::min(ext, 256 / w); c >= 1; --c)
+        if (ext % c == 0 && (!inner || (c * w * 8) % 16 == 0)) return c;
+    return 0;
+}
+
+// The tensor maps of axis pass `slot` (Z, X, Y) for tiles of B lines on
+// buffer `data` (one map per z brick index; the layout is described in
+// fft_tmat.cuh).  False when the geometry has no such description: more than
+// kTmatMaxMaps z bricks, a tile crossing a brick, a box edge that cannot be
+// cut into boxes of at most 256 words, strides or offsets off 16 bytes, or an
+// encoder refusal.
+bool build_tmat(const Dist& d, int slot, int B, const void* data, a2a::TmatMaps* m) {
+    if (slot != a2a::SLOT_Z && slot != a2a::SLOT_X && slot != a2a::SLOT_Y) return false;
+    const TmapEncodeFn enc = tmap_encoder();
+    if (!enc) return false;
+    const int w = d.prec == A2A_C128 ? 2 : 1;
+    const int lx = d.local[0], ly = d.local[1], lz = d.local[2];
+    const int d0 = d.dims[0], d1 = d.dims[1], d2 = d.dims[2];
+    const uint64_t nl = d.nlocal;
+    const uint64_t esz = d.elem_bytes;
+    if (d2 > a2a::kTmatMaxMaps || (w * lz * 8) % 16 || (nl * esz) % 16) return false;
+    if (reinterpret_cast<uintptr_t>(data) % 16) return false;
+    std::memset(m, 0, sizeof(*m));
+    m->pass = slot;
+    m->lx = lx;
+    m->ly = ly;
+    m->lz = lz;
+    m->words = w;
+    m->nmaps = d2;
+    cuuint32_t box[5] = {1, 1, 1, 1, 1};
+    if (slot == a2a::SLOT_Z) {
+        if (B > 256 || ly % B) return false;
+        const int c = tmat_chunk(lz, w, true);
+        if (!c) return false;
+        m->chunk = c;
+        m->nchunk = lz / c;
+        box[0] = (cuuint32_t)(w * c);
+        box[1] = (cuuint32_t)B;
+    } else {
+        if (lz % B || w * B > 256 || (w * B * 8) % 16) return false;
+        const int l = slot == a2a::SLOT_X ? lx : ly;
+        const int dd = slot == a2a::SLOT_X ? d0 : d1;
+        box[0] = (cuuint32_t)(w * B);
+        int c = l;
+        if (l > 256 || dd > 256) {
+            if (dd != 1) return false;
+            c = tmat_chunk(l, 1, false);
+            if (!c) return false;
+        }
+        m->chunk = c;
+        m->nchunk = l / c;
+        if (slot == a2a::SLOT_X) {
+            box[2] = (cuuint32_t)c;
+            box[4] = (cuuint32_t)(m->nchunk == 1 ? d0 : 1);
+        } else {
+            box[1] = (cuuint32_t)c;
+            box[3] = (cuuint32_t)(m->nchunk == 1 ? d1 : 1);
+        }
+    }
+    // every box lands at a 128-byte aligned shared-memory offset
+    if (((size_t)B * m->chunk * esz) % 128) return false;
+    const cuuint64_t dims[5] = {(cuuint64_t)w * lz, (cuuint64_t)ly, (cuuint64_t)lx, (cuuint64_t)d1, (cuuint64_t)d0};
+    const cuuint64_t strides[4] = {(cuuint64_t)lz * esz, (cuuint64_t)ly * lz * esz, (cuuint64_t)d2 * nl * esz,
+                                   (cuuint64_t)d1 * d2 * nl * esz};
+    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    for (int zr = 0; zr < d2; ++zr) {
+        void* base = const_cast<char*>(static_cast<const char*>(data)) + (size_t)zr * nl * esz;
+        if (enc(&m->map[zr], CU_TENSOR_MAP_DATA_TYPE_INT64, 5, base, dims, strides, box, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return false;
+    }
+    return true;
+}
+
+bool is_tmat(const PassKernel& k) { return k.kind == a2a::KIND_TMAT2 || k.kind == a2a::KIND_TMAT3; }
+
 // Does variant k fit the slot's geometry?  Every kernel needs whole tiles.
 // Kernels that move several lines per 16-byte access (the pipelined BATCH
 // kernel: whole tile rows; LPT = 2: line pairs) need those lines contiguous
 // and 16-byte aligned in every tile.
-bool variant_fits(const Dist& d, const SlotGeom& g, const PassKernel& k) {
+bool variant_fits(const Dist& d, int slot, const SlotGeom& g, const PassKernel& k) {
     if (g.NV % k.lines) return false;
+    if (is_tmat(k)) {
+        if (k.lpt > 1 && g.mode != a2a::MODE_BATCH) return false;
+        a2a::TmatMaps probe;  // encoded against a stand-in 256-byte aligned address
+        return build_tmat(d, slot, k.lines, reinterpret_cast<const void*>(uintptr_t(1) << 20), &probe);
+    }
     int vec = 1;  // lines per 16-byte access
     if ((k.kind == a2a::KIND_PIPE || k.kind == a2a::KIND_TMA) && g.mode == a2a::MODE_BATCH) vec = k.lines;
     if (k.kind == a2a::KIND_TMA && g.mode != a2a::MODE_BATCH) return false;
@@ -199,7 +304,7 @@ a2a_status finish(const Dist& d, cudaStream_t st, bool sync) {
 template <typename T>
 cudaError_t launch_pass_t(const PassKernel& k, unsigned grid, const void* src, void* dst, const uint32_t* offA,
                           const uint32_t* offU, const uint32_t* offV, const void* tw, int NU, int NV, double scale,
-                          int split, int* err, cudaStream_t st) {
+                          int split, int* err, cudaStream_t st, const void* maps = nullptr) {
     a2a::PassArgs<T> a;
     a.src = static_cast<const a2a::cx<T>*>(src);
     a.dst = static_cast<a2a::cx<T>*>(dst);
@@ -212,7 +317,7 @@ cudaError_t launch_pass_t(const PassKernel& k, unsigned grid, const void* src, v
     a.scale = T(scale);
     a.split = split;
     a.err = err;
-    void* args[] = {&a};
+    void* args[] = {&a, const_cast<void*>(maps)};
     return cudaLaunchKernel(k.fn, dim3(grid), dim3(k.threads), args, k.smem, st);
 }
 
@@ -223,18 +328,29 @@ cudaError_t launch_slot(const Dist& d, int slot, bool inv, int c, void* p, doubl
     const SlotGeom g = slot_geom(d, slot);
     const uint64_t tiles = (uint64_t)g.NU * (g.NV / k.lines);
     uint64_t grid = tiles;
-    if (k.kind == a2a::KIND_PIPE || k.kind == a2a::KIND_TMA || k.kind == a2a::KIND_RPIPE) {
+    if (k.kind == a2a::KIND_PIPE || k.kind == a2a::KIND_TMA || k.kind == a2a::KIND_RPIPE || is_tmat(k)) {
         const uint64_t resident = (uint64_t)std::max(ps.occ[c], 1) * d.sms;
         grid = std::min(tiles, resident);
+    }
+    const void* maps = nullptr;
+    if (is_tmat(k)) {  // tensor maps of this pass for buffer p (rebuilt when p or the tile height changes)
+        a2a::TmatEntry& ce = d.tmat[slot];
+        if (ce.ptr != p || ce.lines != k.lines) {
+            ce.ptr = nullptr;
+            if (!build_tmat(d, slot, k.lines, p, &ce.maps)) return cudaErrorInvalidValue;
+            ce.ptr = p;
+            ce.lines = k.lines;
+        }
+        maps = &ce.maps;
     }
     const int l = slot == a2a::SLOT_Z ? d.local[2] : slot == a2a::SLOT_X ? d.local[0]
                 : slot == a2a::SLOT_Y ? d.local[1] : d.ng[0];
     const int split = split_ok(l, k);
     if (d.prec == A2A_C128)
         return launch_pass_t<double>(k, unsigned(grid), p, p, g.offA, g.offU, g.offV, g.tw, g.NU, g.NV, scale, split,
-                                     d.d_err, st);
+                                     d.d_err, st, maps);
     return launch_pass_t<float>(k, unsigned(grid), p, p, g.offA, g.offU, g.offV, g.tw, g.NU, g.NV, scale, split,
-                                d.d_err, st);
+                                d.d_err, st, maps);
 }
 
 a2a_status setup_distribution(Dist& d, int nx, int ny, int nz, int P, int block_size, a2a_precision prec) {
@@ -365,7 +481,7 @@ a2a_status setup_distribution(Dist& d, int nx, int ny, int nz, int P, int block_
         for (int inv = 0; inv < 2; ++inv) {
             a2a::PassSlot& ps = d.slot[sl][inv];
             for (int c = 0; c < ps.ncand; ++c) {
-                ps.fits[c] = ps.occ[c] > 0 && variant_fits(d, g, ps.cand[c]);
+                ps.fits[c] = ps.occ[c] > 0 && variant_fits(d, sl, g, ps.cand[c]);
                 if (ps.fits[c] && ps.chosen < 0) ps.chosen = c;
             }
             if (ps.chosen < 0) ps.chosen = 0;  // reported by make_plans / the 1D calls
@@ -937,7 +1053,8 @@ a2a_status a2a_dfft_plan_report(const a2a_dfft* f, char* buf, size_t len) {
                      "tuned_ms=%.4f%s\n",
                      names[p], k.n,
                      k.kind == a2a::KIND_PIPE ? "pipe" : k.kind == a2a::KIND_TMA ? "tma"
-                     : k.kind == a2a::KIND_RPIPE ? "rpipe" : "direct", k.lines, k.lpt, k.threads, k.smem,
+                     : k.kind == a2a::KIND_RPIPE ? "rpipe" : k.kind == a2a::KIND_TMAT2 ? "tmat2"
+                     : k.kind == a2a::KIND_TMAT3 ? "tmat3" : "direct", k.lines, k.lpt, k.threads, k.smem,
                      ps.occ[c], k.radix[0], k.radix[1], k.radix[2], k.radix[3], (int)ps.fits[c], ps.tuned_ms[c],
                      c == ps.chosen ? " <- chosen" : "");
             out += line;

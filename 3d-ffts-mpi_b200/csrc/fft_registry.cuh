@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include "fft_tile.cuh"
+#include "fft_tmat.cuh"
 
 namespace a2a {
 
@@ -129,7 +130,17 @@ A2A_PLANS(double)
     X(float, 1024, KIND_DIRECT,  8, 256, 1, 1)      \
     X(float, 1024, KIND_DIRECT,  8, 256, 1, 2)      \
     X(float, 1024, KIND_PIPE,    8, 512, 1, 1)      \
-    X(float, 1024, KIND_DIRECT,  4, 128, 1, 1)     
+    X(float, 1024, KIND_DIRECT,  4, 128, 1, 1)      \
+    X(float,  128, KIND_TMAT2,  32, 256, 2, 1)      \
+    X(float,  256, KIND_TMAT2,  16, 256, 2, 1)      \
+    X(float,  256, KIND_TMAT3,  16, 256, 1, 1)      \
+    X(float,  512, KIND_TMAT2,   8, 256, 2, 1)      \
+    X(float,  512, KIND_TMAT3,   8, 256, 1, 1)      \
+    X(float,  512, KIND_TMAT2,  16, 512, 1, 2)      \
+    X(float,  768, KIND_TMAT2,   8, 256, 1, 1)      \
+    X(float, 1024, KIND_TMAT2,   4, 256, 2, 1)      \
+    X(float, 1024, KIND_TMAT3,   4, 256, 1, 1)      \
+    X(float, 1024, KIND_TMAT2,   8, 512, 1, 1)
 
 #define A2A_VARIANTS_F64(X)                         \
     X(double,    4, KIND_DIRECT,  4,  32, 1, 1)     \
@@ -173,13 +184,21 @@ A2A_PLANS(double)
     X(double,  768, KIND_DIRECT,  8, 384, 1, 1)     \
     X(double, 1024, KIND_DIRECT,  8, 512, 1, 1)     \
     X(double, 1024, KIND_DIRECT,  4, 256, 1, 1)     \
+    X(double,  256, KIND_TMAT2,   8, 256, 2, 1)     \
+    X(double,  512, KIND_TMAT2,   4, 256, 2, 1)     \
+    X(double,  512, KIND_TMAT2,   8, 512, 1, 1)     \
+    X(double,  768, KIND_TMAT2,   4, 192, 1, 1)     \
+    X(double, 1024, KIND_TMAT2,   4, 256, 1, 1)     \
 // clang-format on                                 
 
 template <typename T, int N, int KIND, int B, int TH, int MB, int LPT, int MODE, bool INV>
 PassKernel make_pass_kernel() {
     using P = typename PassPlan<T, N>::Plan;
     PassKernel k;
-    if constexpr (KIND == KIND_PIPE)
+    if constexpr (KIND == KIND_TMAT2 || KIND == KIND_TMAT3)
+        k.fn = reinterpret_cast<const void*>(
+            &fft_tmat_kernel<T, P, B, TH, MODE, INV, MB, LPT, (KIND == KIND_TMAT3 ? 3 : 2)>);
+    else if constexpr (KIND == KIND_PIPE)
         k.fn = reinterpret_cast<const void*>(&fft_pipe_kernel<T, P, B, TH, MODE, INV, MB, LPT>);
     else if constexpr (KIND == KIND_TMA)
         k.fn = reinterpret_cast<const void*>(&fft_tma_kernel<T, P, B, TH, MODE, INV, MB, LPT>);
@@ -193,7 +212,10 @@ PassKernel make_pass_kernel() {
     k.lines = B;
     k.min_blocks = MB;
     k.lpt = LPT;
-    k.smem = pass_smem_bytes<T, P, B, MODE, KIND, LPT>();
+    if constexpr (KIND == KIND_TMAT2 || KIND == KIND_TMAT3)
+        k.smem = tmat_smem_bytes<T, P, B, MODE, LPT, (KIND == KIND_TMAT3 ? 3 : 2)>();
+    else
+        k.smem = pass_smem_bytes<T, P, B, MODE, KIND, LPT>();
     k.nstages = P::S;
     for (int s = 0; s < P::S; ++s) k.radix[s] = P::r[s];
     k.twtotal = P::twtotal();
@@ -223,7 +245,7 @@ bool make_variant(int mode, bool inv, PassKernel* out) {
 int find_pass_kernels_f32(int n, int mode, bool inverse, PassKernel* out, int max);
 int find_pass_kernels_f64(int n, int mode, bool inverse, PassKernel* out, int max);
 
-constexpr int kMaxVariants = 16;
+constexpr int kMaxVariants = 24;
 
 // fft_tc.cu: the split-precision tensor-core kernel of length n (fmt 0 =
 // fp16, 1 = bf16); false when n has none.

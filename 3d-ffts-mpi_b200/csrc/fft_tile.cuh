@@ -382,7 +382,9 @@ enum PassKind : int {
     KIND_PIPE = 1,    // persistent CTAs, next tile prefetched into shared memory (LDGSTS)
     KIND_TMA = 2,     // persistent CTAs, tile rows fetched by TMA bulk copies, mbarrier completion
     KIND_TC = 3,      // radix-16 stages as split-precision tcgen05 GEMMs
-    KIND_RPIPE = 4    // persistent CTAs, next tile's stage-0 loads in flight in registers
+    KIND_RPIPE = 4,   // persistent CTAs, next tile's stage-0 loads in flight in registers
+    KIND_TMAT2 = 5,   // persistent CTAs, whole tiles fetched by TMA tensor copies into a 2-slot ring
+    KIND_TMAT3 = 6    // the same with a 3-slot ring
 };
 
 constexpr int kTmaBuffers = 2;

@@ -1,0 +1,198 @@
+// Axis pass with whole tiles fetched by TMA tensor copies (KIND_TMAT2/3).
+//
+// The rank-major brick buffer is, seen from one z brick index zr, a 5-D
+// array of 8-byte words  [x_r][y_r][x_l][y_l][z_l]  (dims d0, d1, lx, ly,
+// w*lz; w = 1 word per complex float, 2 per complex double) with strides
+// (d1 d2 nl, d2 nl, ly lz, lz, 1) elements, starting at zr * nl.  One tensor
+// map per zr describes it; a tile of B lines is then one box (X and Y
+// passes) or one box per z brick (Z pass):
+//
+//   Z pass, lines (x, y = v0..v0+B-1): per zr a box [lz, B, 1, 1, 1] at
+//           (0, y_l, x_l, y_r, x_r)  -> shared [zr][b][z_l]
+//   X pass, lines (y, z = v0..v0+B-1): box [B, 1, lx, 1, d0] at
+//           (z_l, y_l, 0, y_r, 0) of map z_r -> shared [x][b]
+//   Y pass, lines (x, z = v0..v0+B-1): box [B, ly, 1, d1, 1] at
+//           (z_l, 0, x_l, 0, x_r) of map z_r -> shared [y][b]
+//
+// (a box edge above 256 words is cut into chunks along that axis).  A
+// persistent CTA keeps NSTG tiles in flight in a ring of shared-memory slots,
+// each completing on its own mbarrier; stage 0 reads its slot into
+// registers and writes the Stockham tile, which frees the slot for the tile
+// NSTG ahead while stages 1..S-1 run.  No copy here uses cluster multicast.
+#pragma once
+
+#include <cuda.h>
+
+#include "fft_tile.cuh"
+
+namespace a2a {
+
+constexpr int kTmatMaxMaps = 8;
+constexpr uint32_t kTmatAlign = 1024;
+
+// Kernel parameter: the tensor maps of one pass and the tile geometry.
+struct TmatMaps {
+    CUtensorMap map[kTmatMaxMaps];  // one per z brick index
+    int pass;                       // 0 = Z, 1 = X, 2 = Y
+    int lx, ly, lz;                 // brick extents (elements)
+    int words;                      // 8-byte words per complex element
+    int chunk;                      // box edge (elements) along the cut axis
+    int nchunk;                     // boxes per z brick (Z) or per tile (X, Y)
+    int nmaps;                      // d2
+};
+
+template <typename T, int B, int N> __host__ __device__ constexpr uint32_t tmat_slot_bytes() {
+    return (uint32_t)((B * N * sizeof(cx<T>) + kTmatAlign - 1) / kTmatAlign * kTmatAlign);
+}
+
+template <typename T, class PLAN, int B, int MODE, int LPT, int NSTG>
+__host__ __device__ constexpr size_t tmat_smem_bytes() {
+    using E = typename ElemOf<T, LPT>::type;
+    constexpr int N = PLAN::N;
+    constexpr int BV = B / LPT;
+    size_t bytes = kTmatAlign;  // room to align the ring
+    bytes += (size_t)NSTG * tmat_slot_bytes<T, B, N>();
+    bytes += sizeof(E) * (size_t)TileGeom<MODE, BV, N, sizeof(E)>::elems;
+    bytes += sizeof(cx<T>) * (size_t)PLAN::twtotal();
+    bytes += sizeof(uint32_t) * (size_t)N;
+    bytes = (bytes + 15) & ~size_t(15);
+    bytes += sizeof(size_t) * (size_t)BV;
+    bytes += sizeof(unsigned long long) * NSTG;
+    return bytes;
+}
+
+__device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3, int c4,
+                                            unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];\n" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// Thread 0: arm the slot's mbarrier for one tile and issue its boxes.
+template <typename T, int B, int N>
+__device__ __forceinline__ void tmat_issue(const TmatMaps& m, int t, int tilesV, unsigned char* dst,
+                                           unsigned long long* bar) {
+    constexpr uint32_t bytes = (uint32_t)(B * N * sizeof(cx<T>));
+    const int u = t / tilesV;
+    const int v0 = (t - u * tilesV) * B;
+    const uint32_t cbytes = (uint32_t)(B * m.chunk * sizeof(cx<T>));
+    mbar_arrive_expect_tx(bar, bytes);
+    if (m.pass == 0) {  // lines (x = u, y = v0 ..)
+        const int xl = u % m.lx, xr = u / m.lx, yl = v0 % m.ly, yr = v0 / m.ly;
+        unsigned char* p = dst;
+        for (int zr = 0; zr < m.nmaps; ++zr)
+            for (int c = 0; c < m.nchunk; ++c, p += cbytes)
+                tma_load_5d(p, &m.map[zr], m.words * c * m.chunk, yl, xl, yr, xr, bar);
+    } else if (m.pass == 1) {  // lines (y = u, z = v0 ..)
+        const int zl = v0 % m.lz, zr = v0 / m.lz, yl = u % m.ly, yr = u / m.ly;
+        for (int c = 0; c < m.nchunk; ++c)
+            tma_load_5d(dst + c * cbytes, &m.map[zr], m.words * zl, yl, c * m.chunk, yr, 0, bar);
+    } else {  // lines (x = u, z = v0 ..)
+        const int zl = v0 % m.lz, zr = v0 / m.lz, xl = u % m.lx, xr = u / m.lx;
+        for (int c = 0; c < m.nchunk; ++c)
+            tma_load_5d(dst + c * cbytes, &m.map[zr], m.words * zl, c * m.chunk, xl, 0, xr, bar);
+    }
+}
+
+template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV, int MINB, int LPT, int NSTG>
+__global__ void __launch_bounds__(THREADS, MINB) fft_tmat_kernel(const PassArgs<T> a, const __grid_constant__ TmatMaps m) {
+    using E = typename ElemOf<T, LPT>::type;
+    constexpr int BV = B / LPT;
+    using G = TileGeom<MODE, BV, PLAN::N, sizeof(E)>;
+    constexpr int N = PLAN::N;
+    constexpr int R0 = PLAN::r[0];
+    constexpr int NBL = N / R0;
+    constexpr int NBT = BV * NBL;
+    constexpr int K = (NBT + THREADS - 1) / THREADS;
+    constexpr bool EXACT = (NBT % THREADS) == 0;
+    constexpr int TWN = PLAN::twtotal();
+    constexpr bool BFAST0 = (MODE == MODE_BATCH);
+    constexpr uint32_t SLOT = tmat_slot_bytes<T, B, N>();
+    static_assert(PLAN::S >= 2, "the ring kernel needs at least two stages");
+    static_assert(MODE != MODE_BATCH || THREADS % BV == 0, "batch mode needs THREADS % (B/LPT) == 0");
+    static_assert(LPT == 1 || MODE == MODE_BATCH, "line pairs only in batch mode");
+    static_assert(NSTG >= 2, "the ring needs at least two slots");
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const uint32_t s0 = smem_u32(smem_raw);
+    unsigned char* ring = smem_raw + (((s0 + kTmatAlign - 1) & ~(kTmatAlign - 1)) - s0);
+    E* tile = reinterpret_cast<E*>(ring + NSTG * SLOT);
+    cx<T>* tw = reinterpret_cast<cx<T>*>(tile + G::elems);
+    uint32_t* offA_s = reinterpret_cast<uint32_t*>(tw + TWN);
+    size_t* base_s = reinterpret_cast<size_t*>(
+        reinterpret_cast<unsigned char*>(tile) +
+        ((sizeof(E) * (size_t)G::elems + sizeof(cx<T>) * TWN + sizeof(uint32_t) * N + 15) & ~size_t(15)));
+    unsigned long long* bar = reinterpret_cast<unsigned long long*>(base_s + BV);
+
+    const int tid = threadIdx.x;
+    const int tilesV = a.NV / B;
+    const int ntiles = a.NU * tilesV;
+    const int mine = (int)blockIdx.x < ntiles ? (ntiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x : 0;
+    if (tid == 0) {
+        for (int i = 0; i < NSTG; ++i) mbar_init(bar + i, 1);
+        fence_mbar_init();
+    }
+    for (int i = tid; i < TWN; i += THREADS) tw[i] = a.tw[i];
+    for (int i = tid; i < N; i += THREADS) offA_s[i] = a.offA[i];
+    __syncthreads();
+    int issued = 0;  // thread 0: tiles of this CTA whose copies were issued
+    if (tid == 0)
+        for (; issued < NSTG && issued < mine; ++issued)
+            tmat_issue<T, B, N>(m, blockIdx.x + issued * gridDim.x, tilesV, ring + issued * SLOT, bar + issued);
+
+    for (int i = 0; i < mine; ++i) {
+        const int t = blockIdx.x + i * gridDim.x;
+        const int s = i % NSTG;
+        {
+            const int u = t / tilesV;
+            const int v0 = (t - u * tilesV) * B;
+            const size_t ubase = __ldg(a.offU + u);
+            for (int b = tid; b < BV; b += THREADS) base_s[b] = ubase + __ldg(a.offV + v0 + b * LPT);
+        }
+        const bool ok = mbar_wait_bounded(bar + s, (uint32_t)((i / NSTG) & 1));
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) {
+                atomicExch(a.err, 1);
+                // wait (bounded) for this CTA's copies still in flight before leaving
+                for (int j = i; j < issued; ++j) mbar_wait_bounded(bar + j % NSTG, (uint32_t)((j / NSTG) & 1));
+            }
+            return;
+        }
+        // stage 0 from the ring slot
+        const E* src = reinterpret_cast<const E*>(ring + s * SLOT);
+        E x[K][R0];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int q = tid + k * THREADS;
+            if (EXACT || q < NBT) {
+                int b, j;
+                bf_map<BFAST0, BV, NBL>(q, b, j);
+#pragma unroll
+                for (int r = 0; r < R0; ++r) {
+                    const int n = j + r * NBL;
+                    if constexpr (MODE == MODE_BATCH) {
+                        x[k][r] = src[n * BV + b];
+                    } else {  // [z chunk][b][z within the chunk]
+                        const int q2 = n / m.chunk;
+                        x[k][r] = src[(q2 * B + b) * m.chunk + (n - q2 * m.chunk)];
+                    }
+                }
+                Dft<R0, INV, E>::run(x[k]);
+#pragma unroll
+                for (int r = 0; r < R0; ++r) tile[G::idx(b, j * R0 + r)] = x[k][r];
+            }
+        }
+        __syncthreads();  // slot s read out; the tile and its line bases are ready
+        if (tid == 0 && issued < mine) {
+            fence_proxy_async_smem();  // the generic reads of slot s come before the async writes
+            tmat_issue<T, B, N>(m, blockIdx.x + issued * gridDim.x, tilesV, ring + s * SLOT, bar + s);
+            ++issued;
+        }
+        run_stage<T, PLAN, B, THREADS, MODE, INV, LPT, 1>(a, tile, tw, offA_s, base_s, tid);
+        __syncthreads();  // tile and line bases free for the next tile
+    }
+}
+
+}  // namespace a2a

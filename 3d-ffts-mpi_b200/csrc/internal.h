@@ -25,6 +25,13 @@ struct PassSlot {
 
 enum SlotId { SLOT_Z = 0, SLOT_X = 1, SLOT_Y = 2, SLOT_LINES = 3, NSLOTS = 4 };
 
+// Tensor maps of one axis pass for the buffer they were last built for.
+struct TmatEntry {
+    const void* ptr = nullptr;
+    int lines = 0;
+    TmatMaps maps;
+};
+
 // Everything an a2aDistribution carries, for all virtual ranks at once.
 struct Dist {
     int ng[3] = {0, 0, 0};
@@ -61,6 +68,8 @@ struct Dist {
     std::vector<uint32_t> h_off[3];
     // pass kernels: [slot][inverse]
     PassSlot slot[NSLOTS][2];
+    // tensor maps of the TMA-ring pass kernels, per axis pass (Z, X, Y)
+    mutable TmatEntry tmat[3];
 };
 
 // remap.cu

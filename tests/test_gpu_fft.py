@@ -108,7 +108,9 @@ def test_box_transform(pkg, oracle, cuda):
 
 VARIANT_CASES = [(4, 64), (16, 128), (4, 96), (16, 192), (16, 256), (64, 512), (4, (1024, 16, 64)),
                  (4, (16, 1024, 64)), (4, (16, 64, 1024)), (4, (768, 16, 32)), (4, (16, 768, 32)),
-                 (4, (16, 32, 768)), (4, (384, 32, 32)), (4, (32, 32, 384))]
+                 (4, (16, 32, 768)), (4, (384, 32, 32)), (4, (32, 32, 384)),
+                 # long X / Y lines inside 256-element bricks (the TMA-ring tiles' single-box case)
+                 (64, (1024, 32, 64)), (64, (32, 1024, 64)), (64, (768, 32, 64)), (64, (32, 768, 64))]
 
 
 @pytest.mark.parametrize("prec", ["c64", "c128"])
