@@ -206,6 +206,9 @@ bool build_tmat(const Dist& d, int slot, int B, const void* data, a2a::TmatMaps*
             box[3] = (cuuint32_t)(m->nchunk == 1 ? d1 : 1);
         }
     }
+    m->chunk_shift = -1;
+    for (int sh = 0; sh < 31; ++sh)
+        if ((1 << sh) == m->chunk) m->chunk_shift = sh;
     // every box lands at a 128-byte aligned shared-memory offset
     if (((size_t)B * m->chunk * esz) % 128) return false;
     const cuuint64_t dims[5] = {(cuuint64_t)w * lz, (cuuint64_t)ly, (cuuint64_t)lx, (cuuint64_t)d1, (cuuint64_t)d0};

@@ -137,10 +137,16 @@ A2A_PLANS(double)
     X(float,  512, KIND_TMAT2,   8, 256, 2, 1)      \
     X(float,  512, KIND_TMAT3,   8, 256, 1, 1)      \
     X(float,  512, KIND_TMAT2,  16, 512, 1, 2)      \
+    X(float,  512, KIND_TMAT2,   4, 128, 4, 1)      \
+    X(float,  512, KIND_TMAT3,   4, 128, 3, 1)      \
+    X(float,  512, KIND_TMAT2,   8, 128, 3, 1)      \
     X(float,  768, KIND_TMAT2,   8, 256, 1, 1)      \
     X(float, 1024, KIND_TMAT2,   4, 256, 2, 1)      \
     X(float, 1024, KIND_TMAT3,   4, 256, 1, 1)      \
-    X(float, 1024, KIND_TMAT2,   8, 512, 1, 1)
+    X(float, 1024, KIND_TMAT2,   8, 512, 1, 1)      \
+    X(float, 1024, KIND_TMAT2,   2, 128, 4, 1)      \
+    X(float, 1024, KIND_TMAT3,   4, 256, 1, 2)      \
+    X(float,  768, KIND_TMAT2,   4, 128, 3, 1)
 
 #define A2A_VARIANTS_F64(X)                         \
     X(double,    4, KIND_DIRECT,  4,  32, 1, 1)     \
@@ -188,6 +194,9 @@ A2A_PLANS(double)
     X(double,  512, KIND_TMAT2,   4, 256, 2, 1)     \
     X(double,  512, KIND_TMAT2,   8, 512, 1, 1)     \
     X(double,  768, KIND_TMAT2,   4, 192, 1, 1)     \
+    X(double,  768, KIND_TMAT2,   2, 128, 3, 1)     \
+    X(double,  768, KIND_TMAT3,   2, 128, 2, 1)     \
+    X(double,  512, KIND_TMAT2,   2, 128, 4, 1)     \
     X(double, 1024, KIND_TMAT2,   4, 256, 1, 1)     \
 // clang-format on                                 
 

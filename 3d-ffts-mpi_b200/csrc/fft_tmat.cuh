@@ -37,6 +37,7 @@ struct TmatMaps {
     int lx, ly, lz;                 // brick extents (elements)
     int words;                      // 8-byte words per complex element
     int chunk;                      // box edge (elements) along the cut axis
+    int chunk_shift;                // log2(chunk) when chunk is a power of two, else -1
     int nchunk;                     // boxes per z brick (Z) or per tile (X, Y)
     int nmaps;                      // d2
 };
@@ -175,8 +176,15 @@ __global__ void __launch_bounds__(THREADS, MINB) fft_tmat_kernel(const PassArgs<
                     if constexpr (MODE == MODE_BATCH) {
                         x[k][r] = src[n * BV + b];
                     } else {  // [z chunk][b][z within the chunk]
-                        const int q2 = n / m.chunk;
-                        x[k][r] = src[(q2 * B + b) * m.chunk + (n - q2 * m.chunk)];
+                        int q2, zl;
+                        if (m.chunk_shift >= 0) {
+                            q2 = n >> m.chunk_shift;
+                            zl = n & (m.chunk - 1);
+                        } else {
+                            q2 = n / m.chunk;
+                            zl = n - q2 * m.chunk;
+                        }
+                        x[k][r] = src[(q2 * B + b) * m.chunk + zl];
                     }
                 }
                 Dft<R0, INV, E>::run(x[k]);
