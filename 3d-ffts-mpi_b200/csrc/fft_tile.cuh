@@ -272,19 +272,44 @@ template <bool BFAST, int B, int NBL> __device__ __forceinline__ void bf_map(int
 // stride-R butterfly writes of radix 2..SLOTS land in distinct slots, and
 // LS == SLOTS/BV (mod SLOTS) makes a wavefront that walks across the BV lines
 // (SLOTS/BV consecutive elements each) distinct as well.
-template <int MODE, int BV, int N, int ESZ> struct TileGeom {
+//
+// SWSH >= 0 (BATCH tiles whose rows are narrower than a 128-byte bank row,
+// RPL = 128 / (BV ESZ) rows per bank row): row n is stored at n ^ ((n >>
+// SWSH) & (RPL - 1)).  With SWSH = log2 of the first radix, the first stage's
+// writes to rows R j + r (R apart for neighbouring threads) and the other
+// stages' accesses to adjacent rows land in distinct bank-row slots.
+template <int MODE, int BV, int N, int ESZ, int SWSH = -1> struct TileGeom {
     static constexpr int SLOTS = 128 / ESZ;
     static constexpr int LS0 = N + N / SLOTS;
     static constexpr int WANT = (SLOTS / (BV < SLOTS ? BV : SLOTS)) % SLOTS;
     static constexpr int LS = LS0 + ((WANT - LS0 % SLOTS) % SLOTS + SLOTS) % SLOTS;
     static constexpr int elems = (MODE == MODE_BATCH) ? N * BV : BV * LS;
+    static constexpr int RPL = (BV * ESZ < 128) ? 128 / (BV * ESZ) : 1;
+    static constexpr bool SWZ = MODE == MODE_BATCH && SWSH >= 0 && RPL >= 2;
     static __device__ __forceinline__ int idx(int b, int n) {
-        if constexpr (MODE == MODE_BATCH)
-            return n * BV + b;
-        else
+        if constexpr (MODE == MODE_BATCH) {
+            if constexpr (SWZ)
+                return (n ^ ((n >> SWSH) & (RPL - 1))) * BV + b;
+            else
+                return n * BV + b;
+        } else {
             return b * LS + n + n / SLOTS;
+        }
     }
 };
+
+// The row swizzle shift for a BATCH tile of plan PLAN with BV vectors of ESZ
+// bytes per row: log2 of the first radix when it is a power of two at least
+// the rows per bank row (the XOR then stays a permutation of the rows), else
+// -1 (no swizzle).
+template <class PLAN, int BV, int ESZ> __host__ __device__ constexpr int tile_swizzle_shift() {
+    constexpr int R0 = PLAN::r[0];
+    constexpr int RPL = (BV * ESZ < 128) ? 128 / (BV * ESZ) : 1;
+    if ((R0 & (R0 - 1)) != 0 || RPL < 2 || RPL > R0 || (128 % (BV * ESZ)) != 0) return -1;
+    int sh = 0;
+    while ((1 << sh) < R0) ++sh;
+    return sh;
+}
 
 // streaming loads/stores: each element is touched once per pass
 template <typename V> __device__ __forceinline__ V ld_stream(const V* p) { return __ldcs(p); }
@@ -306,12 +331,12 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
 // Stages s >= 1 (and stage 0 of the pipelined kernel): shared -> registers,
 // twiddle, DFT_R, then shared (Stockham position) or, for the last stage,
 // global memory at base_s[b] + offA_s[n].  A thread moves LPT lines at once.
-template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV, int LPT, int s>
+template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV, int LPT, int s, int SWSH = -1>
 __device__ __forceinline__ void run_stage(const PassArgs<T>& a, typename ElemOf<T, LPT>::type* tile,
                                           const cx<T>* tw, const uint32_t* offA_s, const size_t* base_s, int tid) {
     using E = typename ElemOf<T, LPT>::type;
     constexpr int BV = B / LPT;
-    using G = TileGeom<MODE, BV, PLAN::N, sizeof(E)>;
+    using G = TileGeom<MODE, BV, PLAN::N, sizeof(E), SWSH>;
     constexpr int N = PLAN::N;
     constexpr int R = PLAN::r[s];
     constexpr int NS = PLAN::ns(s);
@@ -373,7 +398,7 @@ __device__ __forceinline__ void run_stage(const PassArgs<T>& a, typename ElemOf<
     }
     if constexpr (!LAST) {
         __syncthreads();
-        run_stage<T, PLAN, B, THREADS, MODE, INV, LPT, s + 1>(a, tile, tw, offA_s, base_s, tid);
+        run_stage<T, PLAN, B, THREADS, MODE, INV, LPT, s + 1, SWSH>(a, tile, tw, offA_s, base_s, tid);
     }
 }
 

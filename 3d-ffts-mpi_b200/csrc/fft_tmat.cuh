@@ -17,8 +17,9 @@
 // (a box edge above 256 words is cut into chunks along that axis).  A
 // persistent CTA keeps NSTG tiles in flight in a ring of shared-memory slots,
 // each completing on its own mbarrier; stage 0 reads its slot into
-// registers and writes the Stockham tile, which frees the slot for the tile
-// NSTG ahead while stages 1..S-1 run.  No copy here uses cluster multicast.
+// registers and writes the Stockham tile (BATCH rows narrower than a bank
+// row are swizzled, see TileGeom), which frees the slot for the tile NSTG
+// ahead while stages 1..S-1 run.  No copy here uses cluster multicast.
 #pragma once
 
 #include <cuda.h>
@@ -101,7 +102,8 @@ template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV, int MI
 __global__ void __launch_bounds__(THREADS, MINB) fft_tmat_kernel(const PassArgs<T> a, const __grid_constant__ TmatMaps m) {
     using E = typename ElemOf<T, LPT>::type;
     constexpr int BV = B / LPT;
-    using G = TileGeom<MODE, BV, PLAN::N, sizeof(E)>;
+    constexpr int SWSH = MODE == MODE_BATCH ? tile_swizzle_shift<PLAN, BV, (int)sizeof(E)>() : -1;
+    using G = TileGeom<MODE, BV, PLAN::N, sizeof(E), SWSH>;
     constexpr int N = PLAN::N;
     constexpr int R0 = PLAN::r[0];
     constexpr int NBL = N / R0;
@@ -198,7 +200,7 @@ __global__ void __launch_bounds__(THREADS, MINB) fft_tmat_kernel(const PassArgs<
             tmat_issue<T, B, N>(m, blockIdx.x + issued * gridDim.x, tilesV, ring + s * SLOT, bar + s);
             ++issued;
         }
-        run_stage<T, PLAN, B, THREADS, MODE, INV, LPT, 1>(a, tile, tw, offA_s, base_s, tid);
+        run_stage<T, PLAN, B, THREADS, MODE, INV, LPT, 1, SWSH>(a, tile, tw, offA_s, base_s, tid);
         __syncthreads();  // tile and line bases free for the next tile
     }
 }
