@@ -225,7 +225,9 @@ bool build_tmat(const Dist& d, int slot, int B, const void* data, a2a::TmatMaps*
     return true;
 }
 
-bool is_tmat(const PassKernel& k) { return k.kind == a2a::KIND_TMAT2 || k.kind == a2a::KIND_TMAT3; }
+bool is_tmat(const PassKernel& k) {
+    return k.kind == a2a::KIND_TMAT2 || k.kind == a2a::KIND_TMAT3 || k.kind == a2a::KIND_TMAT2W;
+}
 
 // Does variant k fit the slot's geometry?  Every kernel needs whole tiles.
 // Kernels that move several lines per 16-byte access (the pipelined BATCH
@@ -349,10 +351,11 @@ cudaError_t launch_slot(const Dist& d, int slot, bool inv, int c, void* p, doubl
     const int l = slot == a2a::SLOT_Z ? d.local[2] : slot == a2a::SLOT_X ? d.local[0]
                 : slot == a2a::SLOT_Y ? d.local[1] : d.ng[0];
     const int split = split_ok(l, k);
+    const void* tw = ps.tw[c] ? ps.tw[c] : g.tw;  // a candidate with its own radix plan has its own table
     if (d.prec == A2A_C128)
-        return launch_pass_t<double>(k, unsigned(grid), p, p, g.offA, g.offU, g.offV, g.tw, g.NU, g.NV, scale, split,
+        return launch_pass_t<double>(k, unsigned(grid), p, p, g.offA, g.offU, g.offV, tw, g.NU, g.NV, scale, split,
                                      d.d_err, st, maps);
-    return launch_pass_t<float>(k, unsigned(grid), p, p, g.offA, g.offU, g.offV, g.tw, g.NU, g.NV, scale, split,
+    return launch_pass_t<float>(k, unsigned(grid), p, p, g.offA, g.offU, g.offV, tw, g.NU, g.NV, scale, split,
                                 d.d_err, st, maps);
 }
 
@@ -477,6 +480,55 @@ a2a_status setup_distribution(Dist& d, int nx, int ny, int nz, int P, int block_
     }
     for (int a = 0; a < 3; ++a) d.tw[a] = static_cast<const char*>(d.d_tw) + twpos[a] * d.elem_bytes;
 
+    // candidates whose radix plan differs from the slot's first (the wide
+    // two-stage plans) get their own twiddle tables
+    {
+        auto same_plan = [](const PassKernel& x, const PassKernel& y) {
+            if (x.nstages != y.nstages) return false;
+            for (int i = 0; i < x.nstages; ++i)
+                if (x.radix[i] != y.radix[i]) return false;
+            return true;
+        };
+        std::vector<double> ed;
+        std::vector<float> ef;
+        std::vector<size_t> epos;  // per (slot, inv, candidate): offset + 1, or 0
+        for (int sl = 0; sl < a2a::NSLOTS; ++sl)
+            for (int inv = 0; inv < 2; ++inv) {
+                a2a::PassSlot& ps = d.slot[sl][inv];
+                for (int c = 0; c < ps.ncand; ++c) {
+                    ps.tw[c] = nullptr;
+                    if (same_plan(ps.cand[c], ps.cand[0])) {
+                        epos.push_back(0);
+                        continue;
+                    }
+                    epos.push_back(ed.size() / 2 + 1);
+                    gen_twiddles(ps.cand[c], re, im);
+                    for (size_t i = 0; i < re.size(); ++i) {
+                        ed.push_back((double)re[i]);
+                        ed.push_back((double)im[i]);
+                        ef.push_back((float)re[i]);
+                        ef.push_back((float)im[i]);
+                    }
+                }
+            }
+        if (!ed.empty()) {
+            A2A_CUDA(cudaMalloc(&d.d_tw2, (ed.size() / 2) * d.elem_bytes), "cudaMalloc(twiddles)");
+            if (prec == A2A_C128)
+                A2A_CUDA(cudaMemcpy(d.d_tw2, ed.data(), ed.size() * sizeof(double), cudaMemcpyHostToDevice),
+                         "cudaMemcpy");
+            else
+                A2A_CUDA(cudaMemcpy(d.d_tw2, ef.data(), ef.size() * sizeof(float), cudaMemcpyHostToDevice),
+                         "cudaMemcpy");
+            size_t k = 0;
+            for (int sl = 0; sl < a2a::NSLOTS; ++sl)
+                for (int inv = 0; inv < 2; ++inv) {
+                    a2a::PassSlot& ps = d.slot[sl][inv];
+                    for (int c = 0; c < ps.ncand; ++c, ++k)
+                        if (epos[k]) ps.tw[c] = static_cast<const char*>(d.d_tw2) + (epos[k] - 1) * d.elem_bytes;
+                }
+        }
+    }
+
     // default choice: the first variant that fits each slot's geometry
     for (int sl = 0; sl < a2a::NSLOTS; ++sl) {
         if (sl == a2a::SLOT_LINES && !d.cube) continue;
@@ -496,8 +548,10 @@ a2a_status setup_distribution(Dist& d, int nx, int ny, int nz, int P, int block_
 void release(Dist& d) {
     if (d.d_tables) cudaFree(d.d_tables);
     if (d.d_tw) cudaFree(d.d_tw);
+    if (d.d_tw2) cudaFree(d.d_tw2);
     d.d_tables = nullptr;
     d.d_tw = nullptr;
+    d.d_tw2 = nullptr;
 }
 
 a2a_status create_common(int nx, int ny, int nz, int P, int bs, a2a_precision prec, a2a_distribution** out) {
@@ -1057,7 +1111,7 @@ a2a_status a2a_dfft_plan_report(const a2a_dfft* f, char* buf, size_t len) {
                      names[p], k.n,
                      k.kind == a2a::KIND_PIPE ? "pipe" : k.kind == a2a::KIND_TMA ? "tma"
                      : k.kind == a2a::KIND_RPIPE ? "rpipe" : k.kind == a2a::KIND_TMAT2 ? "tmat2"
-                     : k.kind == a2a::KIND_TMAT3 ? "tmat3" : "direct", k.lines, k.lpt, k.threads, k.smem,
+                     : k.kind == a2a::KIND_TMAT3 ? "tmat3" : k.kind == a2a::KIND_TMAT2W ? "tmat2w" : "direct", k.lines, k.lpt, k.threads, k.smem,
                      ps.occ[c], k.radix[0], k.radix[1], k.radix[2], k.radix[3], (int)ps.fits[c], ps.tuned_ms[c],
                      c == ps.chosen ? " <- chosen" : "");
             out += line;

@@ -55,6 +55,23 @@ template <typename T, int N> struct PassPlan;
 A2A_PLANS(float)
 A2A_PLANS(double)
 
+// Two-stage plans with a radix-32 stage, for the lengths where they replace
+// three stages (one shared-memory exchange fewer per tile): kernels of kind
+// KIND_TMAT2W use these, every other kind the plans above.
+template <typename T, int N> struct PassPlan2;
+#define A2A_PLAN2(T_, N_, ...)                                              \
+    template <> struct PassPlan2<T_, N_> {                                  \
+        using Plan = RadixPlan<__VA_ARGS__>;                                \
+        static_assert(Plan::N == N_, "radix plan does not multiply to N");  \
+    };
+A2A_PLAN2(float, 512, 16, 32)
+A2A_PLAN2(float, 1024, 32, 32)
+A2A_PLAN2(double, 512, 16, 32)
+A2A_PLAN2(double, 1024, 32, 32)
+
+template <typename T, int N, int KIND> struct PlanOf { using Plan = typename PassPlan<T, N>::Plan; };
+template <typename T, int N> struct PlanOf<T, N, KIND_TMAT2W> { using Plan = typename PassPlan2<T, N>::Plan; };
+
 // Launch variants X(T, N, KIND, B lines per tile, THREADS, MINB, LPT).  The first
 // entry per N is the default; make_plans can time the others on the scratch
 // buffer and keep the fastest (a2a_dfft_make_plans).  DIRECT tiles are about
@@ -140,12 +157,17 @@ A2A_PLANS(double)
     X(float,  512, KIND_TMAT2,   4, 128, 4, 1)      \
     X(float,  512, KIND_TMAT3,   4, 128, 3, 1)      \
     X(float,  512, KIND_TMAT2,   8, 128, 3, 1)      \
+    X(float,  512, KIND_TMAT2W,  8, 128, 2, 1)      \
+    X(float,  512, KIND_TMAT2W,  8, 256, 2, 1)      \
+    X(float,  512, KIND_TMAT2W, 16, 256, 1, 2)      \
     X(float,  768, KIND_TMAT2,   8, 256, 1, 1)      \
     X(float, 1024, KIND_TMAT2,   4, 256, 2, 1)      \
     X(float, 1024, KIND_TMAT3,   4, 256, 1, 1)      \
     X(float, 1024, KIND_TMAT2,   8, 512, 1, 1)      \
     X(float, 1024, KIND_TMAT2,   2, 128, 4, 1)      \
     X(float, 1024, KIND_TMAT3,   4, 256, 1, 2)      \
+    X(float, 1024, KIND_TMAT2W,  8, 256, 1, 1)      \
+    X(float, 1024, KIND_TMAT2W,  4, 128, 2, 1)      \
     X(float,  768, KIND_TMAT2,   4, 128, 3, 1)
 
 #define A2A_VARIANTS_F64(X)                         \
@@ -197,14 +219,16 @@ A2A_PLANS(double)
     X(double,  768, KIND_TMAT2,   2, 128, 3, 1)     \
     X(double,  768, KIND_TMAT3,   2, 128, 2, 1)     \
     X(double,  512, KIND_TMAT2,   2, 128, 4, 1)     \
+    X(double,  512, KIND_TMAT2W,  4, 128, 2, 1)     \
+    X(double, 1024, KIND_TMAT2W,  4, 128, 1, 1)     \
     X(double, 1024, KIND_TMAT2,   4, 256, 1, 1)     \
 // clang-format on                                 
 
 template <typename T, int N, int KIND, int B, int TH, int MB, int LPT, int MODE, bool INV>
 PassKernel make_pass_kernel() {
-    using P = typename PassPlan<T, N>::Plan;
+    using P = typename PlanOf<T, N, KIND>::Plan;
     PassKernel k;
-    if constexpr (KIND == KIND_TMAT2 || KIND == KIND_TMAT3)
+    if constexpr (KIND == KIND_TMAT2 || KIND == KIND_TMAT3 || KIND == KIND_TMAT2W)
         k.fn = reinterpret_cast<const void*>(
             &fft_tmat_kernel<T, P, B, TH, MODE, INV, MB, LPT, (KIND == KIND_TMAT3 ? 3 : 2)>);
     else if constexpr (KIND == KIND_PIPE)
@@ -221,7 +245,7 @@ PassKernel make_pass_kernel() {
     k.lines = B;
     k.min_blocks = MB;
     k.lpt = LPT;
-    if constexpr (KIND == KIND_TMAT2 || KIND == KIND_TMAT3)
+    if constexpr (KIND == KIND_TMAT2 || KIND == KIND_TMAT3 || KIND == KIND_TMAT2W)
         k.smem = tmat_smem_bytes<T, P, B, MODE, LPT, (KIND == KIND_TMAT3 ? 3 : 2)>();
     else
         k.smem = pass_smem_bytes<T, P, B, MODE, KIND, LPT>();

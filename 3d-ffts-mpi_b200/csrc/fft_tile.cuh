@@ -99,24 +99,40 @@ __host__ __device__ constexpr double root16_cos(int m) {
     }
 }
 __host__ __device__ constexpr double root16_sin(int m) { return root16_cos((m + 12) & 15); }
+// cos(2 pi m / 32) and sin(2 pi m / 32), m = 0..31: the 32nd roots of unity,
+// to 21 significant digits (the even ones equal the sixteenth roots above).
+__host__ __device__ constexpr double root32_cos(int m) {
+    constexpr double c[9] = {1.0,
+                             0.980785280403230449126,
+                             0.923879532511286756128,
+                             0.831469612302545237079,
+                             0.707106781186547524401,
+                             0.555570233019602224743,
+                             0.382683432365089771728,
+                             0.195090322016128267848,
+                             0.0};
+    const int q = m & 31;  // cos is even about 0 and odd about 8: fold to 0..8
+    return q <= 8 ? c[q] : q <= 16 ? -c[16 - q] : q <= 24 ? -c[q - 16] : c[32 - q];
+}
+__host__ __device__ constexpr double root32_sin(int m) { return root32_cos((m + 24) & 31); }
 // sin(2 pi / 3)
 constexpr double kSin60 = 0.866025403784438646763723170753;
 
 // v * W_R^k with W_R = exp(-2 pi i / R) (forward) or its conjugate (INV).
-// R divides 16; k is a compile-time constant once the caller's loops unroll,
+// R divides 32; k is a compile-time constant once the caller's loops unroll,
 // so the switch folds to one case.
 template <int R, bool INV, typename V> __device__ __forceinline__ V twc(V v, int k) {
-    static_assert(16 % R == 0, "in-register twiddles are sixteenth roots of unity");
+    static_assert(32 % R == 0, "in-register twiddles are 32nd roots of unity");
     using T = typename RealOf<V>::type;
-    const int m = ((k % R) + R) % R * (16 / R);
+    const int m = ((k % R) + R) % R * (32 / R);
     switch (m) {
         case 0: return v;
-        case 4: return INV ? mul_pi(v) : mul_mi(v);
-        case 8: return neg(v);
-        case 12: return INV ? mul_mi(v) : mul_pi(v);
+        case 8: return INV ? mul_pi(v) : mul_mi(v);
+        case 16: return neg(v);
+        case 24: return INV ? mul_mi(v) : mul_pi(v);
         default: {
-            const T c = (T)root16_cos(m);
-            const T s = (T)root16_sin(m);
+            const T c = (T)root32_cos(m);
+            const T s = (T)root32_sin(m);
             return cmul(v, c, INV ? s : -s);
         }
     }
@@ -197,6 +213,9 @@ template <bool INV, typename V> struct Dft<8, INV, V> {
 };
 template <bool INV, typename V> struct Dft<16, INV, V> {
     static __device__ __forceinline__ void run(V* v) { dft_split<4, 4, INV>(v); }
+};
+template <bool INV, typename V> struct Dft<32, INV, V> {
+    static __device__ __forceinline__ void run(V* v) { dft_split<8, 4, INV>(v); }
 };
 
 // --------------------------------------------------------------------------
@@ -409,7 +428,8 @@ enum PassKind : int {
     KIND_TC = 3,      // radix-16 stages as split-precision tcgen05 GEMMs
     KIND_RPIPE = 4,   // persistent CTAs, next tile's stage-0 loads in flight in registers
     KIND_TMAT2 = 5,   // persistent CTAs, whole tiles fetched by TMA tensor copies into a 2-slot ring
-    KIND_TMAT3 = 6    // the same with a 3-slot ring
+    KIND_TMAT3 = 6,   // the same with a 3-slot ring
+    KIND_TMAT2W = 7   // the 2-slot ring with the length's two-stage wide-radix plan (radix 16/32)
 };
 
 constexpr int kTmaBuffers = 2;

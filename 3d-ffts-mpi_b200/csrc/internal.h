@@ -18,6 +18,7 @@ struct PassSlot {
     int occ[kMaxVariants] = {0};       // resident CTAs per SM
     bool fits[kMaxVariants] = {false};
     float tuned_ms[kMaxVariants] = {0};  // make_plans timings (0 = not timed)
+    const void* tw[kMaxVariants] = {nullptr};  // own twiddle table (a candidate with another radix plan)
     int ncand = 0;
     int chosen = 0;
     const PassKernel& k() const { return cand[chosen]; }
@@ -64,6 +65,7 @@ struct Dist {
     // precision of the plan
     void* d_tw = nullptr;
     const void* tw[3] = {nullptr, nullptr, nullptr};
+    void* d_tw2 = nullptr;  // twiddle tables of candidates with another radix plan
     // host copies of the offset tables (geometry checks)
     std::vector<uint32_t> h_off[3];
     // pass kernels: [slot][inverse]
