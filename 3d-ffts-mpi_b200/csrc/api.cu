@@ -1019,12 +1019,22 @@ a2a_status a2a_dfft_make_plans(a2a_dfft* f, void** d_scratch) {
         if (reinterpret_cast<uintptr_t>(f->scratch) % 16)
             return fail(A2A_ERROR_MISALIGNED, "d_scratch[0] is not 16-byte aligned");
         // time every fitting variant of each pass on the scratch buffer (its
-        // contents are clobbered, as the reference allows) and keep the fastest
+        // contents are clobbered, as the reference allows) and keep the
+        // fastest: one sweep over the passes, each candidate timed inside a
+        // whole forward + inverse with the other passes' current choices (a
+        // pass alone runs with a different cache and clock state than in the
+        // transform)
         cudaStream_t st = d.stream;
         cudaEvent_t e0, e1;
         A2A_CUDA(cudaEventCreate(&e0), "cudaEventCreate");
         A2A_CUDA(cudaEventCreate(&e1), "cudaEventCreate");
         a2a_status status = A2A_SUCCESS;
+        auto transform = [&]() {
+            cudaError_t e = cudaSuccess;
+            for (int inv = 0; inv < 2 && e == cudaSuccess; ++inv)
+                for (int p = 0; p < 3 && e == cudaSuccess; ++p) e = run_pass(d, p, inv != 0, f->scratch, st);
+            return e;
+        };
         for (int p = 0; p < 3 && status == A2A_SUCCESS; ++p) {
             a2a::PassSlot& ps = d.slot[p][0];
             int best = ps.chosen;
@@ -1032,11 +1042,13 @@ a2a_status a2a_dfft_make_plans(a2a_dfft* f, void** d_scratch) {
             for (int c = 0; c < ps.ncand && status == A2A_SUCCESS; ++c) {
                 ps.tuned_ms[c] = 0.f;
                 if (!ps.fits[c]) continue;
-                cudaError_t e = launch_slot(d, p, false, c, f->scratch, 1.0, st);  // warm-up
+                ps.chosen = c;
+                d.slot[p][1].chosen = c;  // the inverse kernels share the variant list
+                cudaError_t e = transform();  // warm-up
                 float ms = 1e30f;
                 for (int rep = 0; rep < 3 && e == cudaSuccess; ++rep) {
                     e = cudaEventRecord(e0, st);
-                    if (e == cudaSuccess) e = launch_slot(d, p, false, c, f->scratch, 1.0, st);
+                    if (e == cudaSuccess) e = transform();
                     if (e == cudaSuccess) e = cudaEventRecord(e1, st);
                     if (e == cudaSuccess) e = cudaEventSynchronize(e1);
                     float t = 0.f;
@@ -1054,7 +1066,7 @@ a2a_status a2a_dfft_make_plans(a2a_dfft* f, void** d_scratch) {
                 }
             }
             ps.chosen = best;
-            d.slot[p][1].chosen = best;  // the inverse kernels share the variant list
+            d.slot[p][1].chosen = best;
         }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);

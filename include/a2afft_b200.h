@@ -201,7 +201,9 @@ a2a_status a2a_dfft_set_method(a2a_dfft* dfft, a2a_method method);
  * buffer).  The fused transform runs in place and never touches it; when it
  * is given (and autotuning is on, the default), make_plans times every
  * compiled launch variant of each axis pass on it -- clobbering its contents,
- * as the reference's transforms do -- and keeps the fastest.  With NULL the
+ * as the reference's transforms do -- inside a whole forward + inverse with
+ * the other passes' current choices (one sweep Z, X, Y), and keeps the
+ * fastest; the report's tuned_ms is that forward + inverse time.  With NULL the
  * default variant of each pass is used.  The choice is stored in the
  * distribution and shared by every dfft built on it. */
 a2a_status a2a_dfft_make_plans(a2a_dfft* dfft, void** d_scratch);
