@@ -44,6 +44,9 @@ __all__ = [
     "a2aDistribution",
     "a2adfft",
     "a2aBatch",
+    "ipc_export",
+    "ipc_import",
+    "ipc_release",
     "batch_shapes",
     "forward_1d_fft",
     "inverse_1d_fft",
@@ -59,6 +62,28 @@ _KERNELS = {"d_z_a2a_to_z_pencils", "d_z_pencils_to_z_a2a", "d_x_a2a_to_x_pencil
             "d_y_a2a_to_y_pencils", "d_y_pencils_to_y_a2a", "d_fast_z_to_x", "d_fast_x_to_y", "d_fast_y_to_z"}
 _PREC = {"c128": C128, "complex128": C128, "double": C128, "c64": C64, "complex64": C64, "float": C64}
 _METHODS = {"plain": METHOD_PLAIN, "split_bf16": METHOD_SPLIT_BF16, "split_fp16": METHOD_SPLIT_FP16}
+
+
+def ipc_export(buf) -> tuple[bytes, int]:
+    """(handle, offset) that lets another process map this CUDA tensor (or
+    device address)."""
+    ptr = buf if isinstance(buf, int) else buf.data_ptr()
+    h = ctypes.create_string_buffer(64)
+    off = ctypes.c_uint64()
+    call("a2a_ipc_export", ctypes.c_void_p(ptr), h, ctypes.byref(off))
+    return h.raw, off.value
+
+
+def ipc_import(handle: bytes, offset: int) -> int:
+    """Device address, in this process, of a buffer another process exported."""
+    h = ctypes.create_string_buffer(handle, 64)
+    p = ctypes.c_void_p()
+    call("a2a_ipc_import", h, ctypes.c_uint64(offset), ctypes.byref(p))
+    return p.value
+
+
+def ipc_release(ptr: int) -> None:
+    call("a2a_ipc_release", ctypes.c_void_p(ptr))
 
 
 def version() -> int:
@@ -368,6 +393,19 @@ class a2adfft:
         handle = getattr(stream, "cuda_stream", stream)
         call("a2a_dfft_execute_pass_async", self._h, self.distribution._buf(d_data), int(pass_index), int(inverse),
              ctypes.c_void_p(handle))
+
+    def execute_pass_blocks(self, blocks, pass_index: int, inverse: bool, part: int = 0, nparts: int = 1,
+                            stream=None) -> None:
+        """One fused pass over a virtual buffer split into ``len(blocks)``
+        blocks of equal size (block g = virtual ranks ``[g L, (g+1) L)``), each
+        a CUDA tensor of this process or a device address (``int``) mapped
+        from another process with ``ipc_import``; enqueues tile part ``part``
+        of ``nparts``.  The caller orders the passes."""
+        vals = [b if isinstance(b, int) else b.data_ptr() for b in blocks]
+        arr = (ctypes.c_void_p * len(vals))(*vals)
+        handle = 0 if stream is None else getattr(stream, "cuda_stream", stream)
+        call("a2a_dfft_execute_pass_blocks", self._h, arr, len(vals), int(pass_index), int(bool(inverse)), int(part),
+             int(nparts), ctypes.c_void_p(handle))
 
     @property
     def launches_per_transform(self) -> int:

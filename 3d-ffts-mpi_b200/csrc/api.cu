@@ -1169,6 +1169,67 @@ a2a_status a2a_dfft_execute_pass_async(a2a_dfft* f, void** d_data, int pass, int
     return A2A_SUCCESS;
 }
 
+a2a_status a2a_dfft_execute_pass_blocks(a2a_dfft* f, void** blocks, int nblocks, int pass, int inverse, int part,
+                                        int nparts, void* stream) {
+    if (!f) return fail(A2A_ERROR_INVALID_VALUE, "dfft is NULL");
+    const Dist& d = f->dist->d;
+    a2a_status s;
+    if ((s = need_all_ranks(d, "the multi-block pass (its tables are global)")) != A2A_SUCCESS) return s;
+    if (pass < 0 || pass > 2) return fail(A2A_ERROR_INVALID_VALUE, "pass must be 0 (Z), 1 (X) or 2 (Y)");
+    if (nblocks < 1 || nblocks > a2a::kMbMaxBlocks || d.P % nblocks)
+        return fail(A2A_ERROR_INVALID_VALUE, "nblocks must divide world_size=%d and be in [1, %d]", d.P,
+                    a2a::kMbMaxBlocks);
+    if (nparts < 1 || part < 0 || part >= nparts) return fail(A2A_ERROR_INVALID_VALUE, "part must be in [0, nparts)");
+    if (!blocks) return fail(A2A_ERROR_INVALID_VALUE, "blocks is NULL");
+    for (int i = 0; i < nblocks; ++i) {
+        if (!blocks[i]) return fail(A2A_ERROR_INVALID_VALUE, "blocks[%d] is NULL", i);
+        if (reinterpret_cast<uintptr_t>(blocks[i]) % 16)
+            return fail(A2A_ERROR_MISALIGNED, "blocks[%d] is not 16-byte aligned", i);
+    }
+    const SlotGeom g = slot_geom(d, pass);
+    PassKernel k;
+    if (!a2a::find_mb_kernel(d.prec, g.n, g.mode, inverse != 0, &k))
+        return fail(A2A_ERROR_UNSUPPORTED, "no multi-block pass kernel of length %d (lengths 4, 8, 16 have none)",
+                    g.n);
+    if (g.NV % k.lines && !(a2a::find_mb_kernel_small(d.prec, g.n, g.mode, inverse != 0, &k) && g.NV % k.lines == 0))
+        return fail(A2A_ERROR_UNSUPPORTED, "%d lines are not a multiple of a 4-line tile", g.NV);
+    A2A_CUDA(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem),
+             "cudaFuncSetAttribute");
+    const int64_t tiles = (int64_t)g.NU * (g.NV / k.lines);
+    const int64_t t0 = tiles * part / nparts, t1 = tiles * (part + 1) / nparts;
+    if (t1 <= t0) return A2A_SUCCESS;
+    const double scale = (inverse && pass == 2) ? 1.0 / ((double)d.ng[0] * d.ng[1] * d.ng[2]) : 1.0;
+    const uint32_t block_elems = (uint32_t)((uint64_t)(d.P / nblocks) * d.nlocal);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e;
+    auto launch = [&](auto tag) {
+        using T = decltype(tag);
+        a2a::PassArgs<T> a;
+        a.src = nullptr;
+        a.dst = nullptr;
+        a.offA = g.offA;
+        a.offU = g.offU;
+        a.offV = g.offV;
+        a.tw = static_cast<const a2a::cx<T>*>(g.tw);
+        a.NU = g.NU;
+        a.NV = g.NV;
+        a.scale = T(scale);
+        a.split = 0;
+        a.err = d.d_err;
+        a.tcb = nullptr;
+        a2a::MbArgs<T> mb;
+        for (int i = 0; i < a2a::kMbMaxBlocks; ++i) mb.blk[i] = static_cast<a2a::cx<T>*>(blocks[i < nblocks ? i : 0]);
+        mb.fbe = a2a::FastDiv(block_elems);
+        mb.nblk = nblocks;
+        mb.tile0 = (int)t0;
+        void* args[] = {&a, &mb};
+        return cudaLaunchKernel(k.fn, dim3((unsigned)(t1 - t0)), dim3(k.threads), args, k.smem, st);
+    };
+    e = d.prec == A2A_C128 ? launch(double()) : launch(float());
+    A2A_CUDA(e, "multi-block pass launch");
+    return A2A_SUCCESS;
+}
+
 a2a_status a2a_dfft_launches_per_transform(const a2a_dfft* f, int* out) {
     if (!f || !out) return fail(A2A_ERROR_INVALID_VALUE, "NULL argument");
     *out = 3;
@@ -1273,6 +1334,71 @@ a2a_status a2a_dfft_forward_host(a2a_dfft* f, void* host_data, void** d_buffer) 
 }
 a2a_status a2a_dfft_inverse_host(a2a_dfft* f, void* host_data, void** d_buffer) {
     return host_staged(f, host_data, d_buffer, true);
+}
+
+// ---- CUDA IPC for the multi-block pass ----
+
+static std::mutex g_ipc_mutex;
+static std::vector<std::pair<void*, void*>> g_ipc_maps;  // (imported address, allocation base)
+
+using MemRangeFn = CUresult (*)(CUdeviceptr*, size_t*, CUdeviceptr);
+
+static MemRangeFn mem_range_fn() {
+    static MemRangeFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<MemRangeFn>(p);
+    });
+    return fn;
+}
+
+a2a_status a2a_ipc_export(const void* dev_ptr, void* handle, uint64_t* offset) {
+    if (!dev_ptr || !handle || !offset) return fail(A2A_ERROR_INVALID_VALUE, "NULL argument");
+    static_assert(sizeof(cudaIpcMemHandle_t) <= A2A_IPC_HANDLE_BYTES, "IPC handle size");
+    const MemRangeFn range = mem_range_fn();
+    if (!range) return fail(A2A_ERROR_CUDA, "cuMemGetAddressRange is not available");
+    CUdeviceptr base = 0;
+    size_t size = 0;
+    if (range(&base, &size, reinterpret_cast<CUdeviceptr>(dev_ptr)) != CUDA_SUCCESS)
+        return fail(A2A_ERROR_INVALID_VALUE, "dev_ptr is not device memory of this process");
+    cudaIpcMemHandle_t h;
+    A2A_CUDA(cudaIpcGetMemHandle(&h, reinterpret_cast<void*>(base)), "cudaIpcGetMemHandle");
+    std::memset(handle, 0, A2A_IPC_HANDLE_BYTES);
+    std::memcpy(handle, &h, sizeof(h));
+    *offset = (uint64_t)(reinterpret_cast<CUdeviceptr>(dev_ptr) - base);
+    return A2A_SUCCESS;
+}
+
+a2a_status a2a_ipc_import(const void* handle, uint64_t offset, void** dev_ptr) {
+    if (!handle || !dev_ptr) return fail(A2A_ERROR_INVALID_VALUE, "NULL argument");
+    cudaIpcMemHandle_t h;
+    std::memcpy(&h, handle, sizeof(h));
+    void* base = nullptr;
+    A2A_CUDA(cudaIpcOpenMemHandle(&base, h, cudaIpcMemLazyEnablePeerAccess), "cudaIpcOpenMemHandle");
+    *dev_ptr = static_cast<char*>(base) + offset;
+    std::lock_guard<std::mutex> lock(g_ipc_mutex);
+    g_ipc_maps.emplace_back(*dev_ptr, base);
+    return A2A_SUCCESS;
+}
+
+a2a_status a2a_ipc_release(void* dev_ptr) {
+    void* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_ipc_mutex);
+        for (auto it = g_ipc_maps.begin(); it != g_ipc_maps.end(); ++it)
+            if (it->first == dev_ptr) {
+                base = it->second;
+                g_ipc_maps.erase(it);
+                break;
+            }
+    }
+    if (!base) return fail(A2A_ERROR_INVALID_VALUE, "dev_ptr was not imported with a2a_ipc_import");
+    A2A_CUDA(cudaIpcCloseMemHandle(base), "cudaIpcCloseMemHandle");
+    return A2A_SUCCESS;
 }
 
 const char* a2a_status_string(a2a_status s) {

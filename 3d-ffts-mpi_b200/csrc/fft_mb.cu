@@ -1,0 +1,81 @@
+// Instantiations of the multi-block pass kernel (one tile configuration per
+// length and precision, both access modes and directions) and their lookup.
+#include "fft_mb.cuh"
+#include "internal.h"
+
+namespace a2a {
+
+template <typename T, int N, int B, int TH, int MB, int MODE, bool INV> PassKernel make_mb_kernel() {
+    using P = typename PassPlan<T, N>::Plan;
+    PassKernel k;
+    k.fn = reinterpret_cast<const void*>(&fft_mb_kernel<T, P, B, TH, MODE, INV, MB>);
+    k.kind = KIND_DIRECT;
+    k.n = N;
+    k.threads = TH;
+    k.lines = B;
+    k.min_blocks = MB;
+    k.lpt = 1;
+    k.smem = mb_smem_bytes<T, P, B, MODE>();
+    k.nstages = P::S;
+    for (int s = 0; s < P::S; ++s) k.radix[s] = P::r[s];
+    k.twtotal = P::twtotal();
+    return k;
+}
+
+template <typename T, int N, int B, int TH, int MB> PassKernel mb_pick(int mode, bool inv) {
+    if (mode == MODE_LINE)
+        return inv ? make_mb_kernel<T, N, B, TH, MB, MODE_LINE, true>() : make_mb_kernel<T, N, B, TH, MB, MODE_LINE, false>();
+    return inv ? make_mb_kernel<T, N, B, TH, MB, MODE_BATCH, true>() : make_mb_kernel<T, N, B, TH, MB, MODE_BATCH, false>();
+}
+
+// (N, lines, threads, min blocks) per precision: the one-tile configurations
+// of the single-buffer registry (multi-stage plans only)
+#define A2A_MB_F32(X)                                                                                              \
+    X(12, 4, 32, 1) X(24, 8, 32, 1) X(32, 32, 128, 1) X(48, 16, 64, 1) X(64, 32, 128, 1) X(96, 32, 128, 1)       \
+    X(128, 32, 256, 1) X(192, 32, 256, 1) X(256, 16, 256, 2) X(384, 16, 256, 1) X(512, 8, 128, 4)                \
+    X(768, 8, 256, 1) X(1024, 8, 512, 1)
+#define A2A_MB_F64(X)                                                                                              \
+    X(12, 4, 32, 1) X(24, 8, 32, 1) X(32, 16, 128, 1) X(48, 8, 64, 1) X(64, 32, 128, 1) X(96, 16, 128, 1)        \
+    X(128, 16, 128, 1) X(192, 16, 256, 1) X(256, 16, 256, 1) X(384, 8, 256, 1) X(512, 8, 256, 1)                 \
+    X(768, 4, 192, 1) X(1024, 8, 512, 1)
+
+// 4-line tiles for passes whose line counts the configurations above do not divide
+#define A2A_MB_SMALL(X)                                                                                            \
+    X(12, 4, 64, 1) X(24, 4, 64, 1) X(32, 4, 64, 1) X(48, 4, 64, 1) X(64, 4, 64, 1) X(96, 4, 64, 1)              \
+    X(128, 4, 64, 1) X(192, 4, 64, 1) X(256, 4, 128, 1) X(384, 4, 128, 1) X(512, 4, 128, 1)                      \
+    X(768, 4, 128, 1) X(1024, 4, 128, 1)
+
+bool find_mb_kernel_small(a2a_precision prec, int n, int mode, bool inverse, PassKernel* out) {
+#define A2A_MB_CASE(N_, B_, TH_, MB_)                                                                       \
+    if (n == N_) {                                                                                          \
+        *out = prec == A2A_C128 ? mb_pick<double, N_, B_, TH_, MB_>(mode, inverse)                           \
+                                : mb_pick<float, N_, B_, TH_, MB_>(mode, inverse);                           \
+        return true;                                                                                        \
+    }
+    A2A_MB_SMALL(A2A_MB_CASE)
+#undef A2A_MB_CASE
+    return false;
+}
+
+bool find_mb_kernel(a2a_precision prec, int n, int mode, bool inverse, PassKernel* out) {
+    if (prec == A2A_C128) {
+#define A2A_MB_CASE(N_, B_, TH_, MB_) \
+    if (n == N_) {                    \
+        *out = mb_pick<double, N_, B_, TH_, MB_>(mode, inverse); \
+        return true;                  \
+    }
+        A2A_MB_F64(A2A_MB_CASE)
+#undef A2A_MB_CASE
+        return false;
+    }
+#define A2A_MB_CASE(N_, B_, TH_, MB_) \
+    if (n == N_) {                    \
+        *out = mb_pick<float, N_, B_, TH_, MB_>(mode, inverse); \
+        return true;                  \
+    }
+    A2A_MB_F32(A2A_MB_CASE)
+#undef A2A_MB_CASE
+    return false;
+}
+
+}  // namespace a2a

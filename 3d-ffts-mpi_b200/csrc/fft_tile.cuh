@@ -23,6 +23,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "remap.cuh"
+
 namespace a2a {
 
 // --------------------------------------------------------------------------
@@ -350,9 +352,27 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
 // Stages s >= 1 (and stage 0 of the pipelined kernel): shared -> registers,
 // twiddle, DFT_R, then shared (Stockham position) or, for the last stage,
 // global memory at base_s[b] + offA_s[n].  A thread moves LPT lines at once.
-template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV, int LPT, int s, int SWSH = -1>
+// A virtual rank-major buffer split into blocks of equal size that may live
+// in other GPUs' memory (the multi-block pass, fft_mb.cuh): element o is
+// element o mod L of block o div L.
+constexpr int kMbMaxBlocks = 8;
+template <typename T> struct MbArgs {
+    cx<T>* blk[kMbMaxBlocks];  // block base pointers (device or peer addresses)
+    FastDiv fbe;               // elements per block
+    int nblk;
+    int tile0;                 // first tile of this launch
+};
+template <typename T> __device__ __forceinline__ cx<T>* mb_addr(const MbArgs<T>& m, uint32_t o) {
+    uint32_t b, r;
+    m.fbe.divmod(o, b, r);
+    return m.blk[b] + r;
+}
+
+template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV, int LPT, int s, int SWSH = -1,
+          bool MB = false>
 __device__ __forceinline__ void run_stage(const PassArgs<T>& a, typename ElemOf<T, LPT>::type* tile,
-                                          const cx<T>* tw, const uint32_t* offA_s, const size_t* base_s, int tid) {
+                                          const cx<T>* tw, const uint32_t* offA_s, const size_t* base_s, int tid,
+                                          const MbArgs<T>* mb = nullptr) {
     using E = typename ElemOf<T, LPT>::type;
     constexpr int BV = B / LPT;
     using G = TileGeom<MODE, BV, PLAN::N, sizeof(E), SWSH>;
@@ -396,7 +416,13 @@ __device__ __forceinline__ void run_stage(const PassArgs<T>& a, typename ElemOf<
                 for (int r = 1; r < R; ++r) x[k][r] = cmulw<INV>(x[k][r], tw[TWO + (r - 1) * NS + m]);
             }
             Dft<R, INV, E>::run(x[k]);
-            if constexpr (LAST) {
+            if constexpr (LAST && MB) {
+                static_assert(LPT == 1, "the multi-block pass moves single lines");
+                const uint32_t line = (uint32_t)base_s[b];
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    st_stream(mb_addr(*mb, line + offA_s[j + r * NBL]), scl(x[k][r], a.scale));
+            } else if constexpr (LAST) {
                 cx<T>* line = a.dst + base_s[b];
                 if (a.split) {
                     cx<T>* p = line + offA_s[j];
@@ -417,7 +443,7 @@ __device__ __forceinline__ void run_stage(const PassArgs<T>& a, typename ElemOf<
     }
     if constexpr (!LAST) {
         __syncthreads();
-        run_stage<T, PLAN, B, THREADS, MODE, INV, LPT, s + 1, SWSH>(a, tile, tw, offA_s, base_s, tid);
+        run_stage<T, PLAN, B, THREADS, MODE, INV, LPT, s + 1, SWSH, MB>(a, tile, tw, offA_s, base_s, tid, mb);
     }
 }
 

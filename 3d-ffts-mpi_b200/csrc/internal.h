@@ -83,6 +83,11 @@ cudaError_t launch_scale(const Dist& d, const void* src, void* dst, double divis
 // api.cu: records "<what>: <detail>" for a2a_last_error and returns s
 a2a_status record_error(a2a_status s, const char* what, const char* detail);
 
+// fft_mb.cu: the multi-block pass kernel of length n (one configuration);
+// false for lengths with a single-stage plan (4 8 16) or none
+bool find_mb_kernel(a2a_precision prec, int n, int mode, bool inverse, PassKernel* out);
+bool find_mb_kernel_small(a2a_precision prec, int n, int mode, bool inverse, PassKernel* out);  // 4-line tiles
+
 // batch.cu: the batched persistent kernel per (precision, direction), its
 // dynamic shared memory, and the tile height of a length's variant (0: the
 // length has no batched tile code)

@@ -20,7 +20,8 @@ Every process takes the same collective steps in the same order.
 """
 from __future__ import annotations
 
-from . import a2aDistribution, decompose, fast_copy_fft, forward_1d_fft, inverse_1d_fft, scale_fft
+from . import (a2aDistribution, a2adfft, decompose, fast_copy_fft, forward_1d_fft, inverse_1d_fft, ipc_export,
+               ipc_import, ipc_release, scale_fft)
 
 
 class CudaLocal:
@@ -157,3 +158,77 @@ class DistributedDfft:
         self._run(d_data, True)
 
     backward = inverse
+
+
+class FusedDistributedDfft:
+    """The transform across processes (one per GPU) with the fused pass: no
+    alltoall.  Process g holds virtual ranks ``[g L, (g+1) L)`` (L = P / G) in
+    one device buffer; ``bind`` maps every other process's buffer into this
+    one (CUDA IPC), then each of the 3 passes of a transform is one kernel per
+    process over its share of the pass's tiles, reading and writing the
+    owners' bricks directly (peer loads and stores over NVLink), with a
+    group barrier between passes.  Same result as ``DistributedDfft``; each
+    element crosses the link once each way per pass, as in the reference's
+    get/return alltoall pair, without the separate pack/unpack passes."""
+
+    def __init__(self, world_size: int, Ng, precision: str = "c64", group=None):
+        import torch.distributed as tdist
+
+        self.group = group
+        self.G = tdist.get_world_size(group)
+        self.g = tdist.get_rank(group)
+        if world_size % self.G:
+            raise ValueError(f"world_size={world_size} virtual ranks do not split over {self.G} processes")
+        self.world_size = world_size
+        self.dist = a2aDistribution(world_size, Ng, 64, precision)
+        self.dfft = a2adfft(self.dist)
+        self.L = world_size // self.G
+        self.block_elems = self.L * self.dist.nlocal
+        self.blocks = None
+        self._imported = []
+
+    def bind(self, d_data) -> None:
+        """Exchange buffer handles with every process (collective)."""
+        import torch.distributed as tdist
+
+        if d_data.numel() < self.block_elems:
+            raise ValueError(f"this process's buffer needs {self.block_elems} elements")
+        mine = ipc_export(d_data)
+        allh = [None] * self.G
+        tdist.all_gather_object(allh, mine, group=self.group)
+        self.release()
+        blocks = []
+        for q, (h, off) in enumerate(allh):
+            if q == self.g:
+                blocks.append(d_data.data_ptr())
+            else:
+                p = ipc_import(h, off)
+                self._imported.append(p)
+                blocks.append(p)
+        self.blocks = blocks
+
+    def _run(self, inverse: bool) -> None:
+        import torch
+        import torch.distributed as tdist
+
+        if self.blocks is None:
+            raise RuntimeError("bind() first")
+        torch.cuda.synchronize()
+        tdist.barrier(group=self.group)  # every block holds its input
+        for p in range(3):
+            self.dfft.execute_pass_blocks(self.blocks, p, inverse, self.g, self.G)
+            torch.cuda.synchronize()
+            tdist.barrier(group=self.group)  # pass p complete everywhere
+
+    def forward(self) -> None:
+        self._run(False)
+
+    def inverse(self) -> None:
+        self._run(True)
+
+    def release(self) -> None:
+        for p in self._imported:
+            ipc_release(p)
+        self._imported = []
+        self.blocks = None
+

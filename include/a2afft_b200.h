@@ -251,6 +251,35 @@ a2a_status a2a_dfft_execute_pass_async(a2a_dfft* dfft, void** d_data, int pass, 
 /* Number of kernel launches one forward (or inverse) enqueues. */
 a2a_status a2a_dfft_launches_per_transform(const a2a_dfft* dfft, int* out);
 
+/* ---- several GPUs: the fused pass over peer memory ----------------------- */
+
+/* The reference exchanges each axis step between ranks with MPI_Alltoall plus
+ * pack/unpack kernels (distribution/a2adistribution.cpp:156-256).  Here one
+ * pass kernel does the whole step across devices: the virtual rank-major
+ * buffer is split into `nblocks` blocks of equal size (block g holds the
+ * contiguous virtual ranks [g L, (g+1) L), L = world_size / nblocks,
+ * world_size / nblocks * nlocal elements), blocks[g] its address on this
+ * device (this process's own block, or another GPU's block mapped with
+ * a2a_ipc_import); the kernel gathers each tile's lines from the owners,
+ * transforms them and scatters them back (peer loads and stores over
+ * NVLink).  A pass's tiles are split evenly into `nparts` parts and this
+ * call enqueues part `part` on `cuda_stream`.  The caller orders the passes:
+ * every part of pass p must be complete before any part of pass p + 1 starts
+ * (e.g. synchronise the stream, then a process-group barrier).  The inverse's
+ * pass 2 applies 1/(nx*ny*nz).  No kernel waits on another device. */
+a2a_status a2a_dfft_execute_pass_blocks(a2a_dfft* dfft, void** blocks, int nblocks, int pass, int inverse, int part,
+                                        int nparts, void* cuda_stream);
+
+/* Sharing a device buffer with another process (CUDA IPC): export writes an
+ * opaque handle of A2A_IPC_HANDLE_BYTES bytes and the buffer's offset inside
+ * its allocation; import maps it in this process (on its current device)
+ * and returns the buffer's address there; release unmaps it.  No reference
+ * counterpart. */
+#define A2A_IPC_HANDLE_BYTES 64
+a2a_status a2a_ipc_export(const void* dev_ptr, void* handle, uint64_t* offset);
+a2a_status a2a_ipc_import(const void* handle, uint64_t offset, void** dev_ptr);
+a2a_status a2a_ipc_release(void* dev_ptr);
+
 a2a_status a2a_dfft_destroy(a2a_dfft* dfft);
 
 /* ---- host-staged transforms -------------------------------------------- */
