@@ -1449,7 +1449,8 @@ struct a2a_batch {
     size_t queue_ints = 0;
     int var[2][a2a::kBatchNumLengths] = {};  // tile variant per (mode, length)
     bool used[2][a2a::kBatchNumLengths] = {};
-    float tuned_ms[2][a2a::kBatchNumLengths][2] = {};
+    float tuned_ms[2][a2a::kBatchNumLengths][a2a::kBatchVariants] = {};
+    bool pairs_ok[a2a::kBatchNumLengths] = {};  // batch-mode line pairs usable for every box of the length
     int fused = 1;   // 1: one launch per direction; 0: one launch per pass
     int claim = 16;
     int wait_extra = 0;
@@ -1751,6 +1752,28 @@ a2a_status a2a_batch_create(int nboxes, const int* shapes, int world_size, a2a_p
             }
             b->var[m][li] = pick;
         }
+    // batch-mode line pairs (16-byte accesses of two adjacent lines): complex
+    // float, and in every box using the length each tile's lines in aligned,
+    // contiguous pairs (checked on the offset tables, as for the single grid)
+    for (int li = 0; li < a2a::kBatchNumLengths; ++li) {
+        const int n = a2a::kBatchLengths[li];
+        bool ok = precision == A2A_C64 && b->used[a2a::MODE_BATCH][li];
+        for (int i = 0; i < nboxes && ok; ++i)
+            for (int p = 1; p < 3 && ok; ++p) {
+                int pn, NU, NV;
+                batch_pass_geom(b, i, p, pn, NU, NV);
+                if (pn != n) continue;
+                const Dist& d = b->dists[b->box_dist[i]]->d;
+                const std::vector<uint32_t>& hA = d.h_off[p == 1 ? 0 : 1];
+                const std::vector<uint32_t>& hU = d.h_off[p == 1 ? 1 : 0];
+                const std::vector<uint32_t>& hV = d.h_off[2];
+                for (int v = 0; v + 1 < NV && ok; v += 2) ok = hV[v + 1] == hV[v] + 1 && hV[v] % 2 == 0;
+                for (uint32_t o : hA) ok = ok && o % 2 == 0;
+                for (uint32_t o : hU) ok = ok && o % 2 == 0;
+                ok = ok && NV % 2 == 0;
+            }
+        b->pairs_ok[li] = ok;
+    }
     const size_t max_smem = a2a::batch_smem(precision);
     cudaError_t e = cudaSuccess;
     for (int inv = 0; inv < 2 && e == cudaSuccess; ++inv)
@@ -1796,9 +1819,12 @@ a2a_status a2a_batch_set_schedule(a2a_batch* b, int fused, int claim, int prefet
 a2a_status a2a_batch_select_variant(a2a_batch* b, int length, int batch_mode, int variant) {
     if (!b) return fail(A2A_ERROR_INVALID_VALUE, "batch is NULL");
     const int li = batch_len_index(length);
-    if (li < 0 || (batch_mode != 0 && batch_mode != 1) || (variant != 0 && variant != 1))
+    if (li < 0 || (batch_mode != 0 && batch_mode != 1) || variant < 0 || variant >= a2a::kBatchVariants)
         return fail(A2A_ERROR_INVALID_VALUE, "length %d / mode %d / variant %d out of range", length, batch_mode,
                     variant);
+    if (variant == 2 && !(batch_mode && b->pairs_ok[li]))
+        return fail(A2A_ERROR_UNSUPPORTED, "length %d: line pairs need batch mode, complex float and aligned pairs",
+                    length);
     const int m = batch_mode ? a2a::MODE_BATCH : a2a::MODE_LINE;
     const int old = b->var[m][li];
     b->var[m][li] = variant;
@@ -1862,20 +1888,24 @@ a2a_status a2a_batch_make_plans(a2a_batch* b, void** d_scratch) {
             if (!b->used[m][li]) continue;
             const int old = b->var[m][li];
             b->tuned_ms[m][li][old] = cur;
-            b->var[m][li] = 1 - old;
-            if (batch_layout(b) != A2A_SUCCESS) {  // the other tile does not divide
-                b->var[m][li] = old;
-                s = batch_layout(b);
-                continue;
-            }
-            float t = 0.f;
-            if ((s = timed(&t)) != A2A_SUCCESS) break;
-            b->tuned_ms[m][li][1 - old] = t;
-            if (t < cur) {
-                cur = t;
-            } else {
-                b->var[m][li] = old;
-                s = batch_layout(b);
+            int best = old;
+            for (int v = 0; v < a2a::kBatchVariants && s == A2A_SUCCESS; ++v) {
+                if (v == old || (v == 2 && !(m == a2a::MODE_BATCH && b->pairs_ok[li]))) continue;
+                b->var[m][li] = v;
+                if (batch_layout(b) != A2A_SUCCESS) {  // this tile does not divide every box
+                    b->var[m][li] = best;
+                    s = batch_layout(b);
+                    continue;
+                }
+                float t = 0.f;
+                if ((s = timed(&t)) != A2A_SUCCESS) break;
+                b->tuned_ms[m][li][v] = t;
+                if (t < cur) {
+                    cur = t;
+                    best = v;
+                }
+                b->var[m][li] = best;
+                if (s == A2A_SUCCESS) s = batch_layout(b);
             }
         }
     // the schedule: one launch or one per pass, items per queue access, L2
@@ -1914,8 +1944,10 @@ a2a_status a2a_batch_plan_report(const a2a_batch* b, char* buf, size_t len) {
         for (int li = 0; li < a2a::kBatchNumLengths; ++li) {
             if (!b->used[m][li]) continue;
             const int n = a2a::kBatchLengths[li];
-            snprintf(line, sizeof line, "  N=%d %s lines=%d (tuned ms: %.4f / %.4f)\n", n, m ? "batch" : "line",
-                     a2a::batch_tile_lines(b->prec, n, b->var[m][li]), b->tuned_ms[m][li][0], b->tuned_ms[m][li][1]);
+            snprintf(line, sizeof line, "  N=%d %s lines=%d%s (tuned ms: %.4f / %.4f / %.4f)\n", n,
+                     m ? "batch" : "line", a2a::batch_tile_lines(b->prec, n, b->var[m][li]),
+                     b->var[m][li] == 2 ? " as pairs" : "", b->tuned_ms[m][li][0], b->tuned_ms[m][li][1],
+                     b->tuned_ms[m][li][2]);
             r += line;
         }
     snprintf(buf, len, "%s", r.c_str());

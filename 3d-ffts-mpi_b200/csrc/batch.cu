@@ -18,6 +18,7 @@ size_t batch_smem(a2a_precision prec) {
 }
 
 int batch_tile_lines(a2a_precision prec, int n, int variant) {
+    if (variant < 0 || variant >= kBatchVariants) return 0;
     for (int i = 0; i < kBatchNumLengths; ++i)
         if (kBatchLengths[i] == n) return prec == A2A_C128 ? batch_lines<double>(n, variant) : batch_lines<float>(n, variant);
     return 0;
@@ -28,10 +29,13 @@ template <typename T> static size_t tile_smem(int n, int v, int mode) {
     if (n == N_) {                                                                                         \
         using P = typename PassPlan<T, N_>::Plan;                                                          \
         if (mode == MODE_LINE)                                                                             \
-            return v ? pass_smem_bytes<T, P, batch_lines<T>(N_, 1), MODE_LINE, KIND_DIRECT, 1>()           \
-                     : pass_smem_bytes<T, P, batch_lines<T>(N_, 0), MODE_LINE, KIND_DIRECT, 1>();          \
-        return v ? pass_smem_bytes<T, P, batch_lines<T>(N_, 1), MODE_BATCH, KIND_DIRECT, 1>()              \
-                 : pass_smem_bytes<T, P, batch_lines<T>(N_, 0), MODE_BATCH, KIND_DIRECT, 1>();             \
+            return v == 1 ? pass_smem_bytes<T, P, batch_lines<T>(N_, 1), MODE_LINE, KIND_DIRECT, 1>()      \
+                          : pass_smem_bytes<T, P, batch_lines<T>(N_, 0), MODE_LINE, KIND_DIRECT, 1>();     \
+        if (v == 2)                                                                                        \
+            return pass_smem_bytes<T, P, batch_lines<T>(N_, 2), MODE_BATCH, KIND_DIRECT,                   \
+                                   batch_lpt<T>(2, MODE_BATCH)>();                                         \
+        return v == 1 ? pass_smem_bytes<T, P, batch_lines<T>(N_, 1), MODE_BATCH, KIND_DIRECT, 1>()         \
+                      : pass_smem_bytes<T, P, batch_lines<T>(N_, 0), MODE_BATCH, KIND_DIRECT, 1>();        \
     }
     A2A_BATCH_FOR_EACH_N(A2A_TS)
 #undef A2A_TS

@@ -21,10 +21,17 @@ constexpr int kBatchThreads = 256;
 constexpr int kBatchMaxBoxes = 65536;
 
 // Tile height per (element type, length, variant) for kBatchThreads threads:
-// two choices per length for the plan's tuner; complex double uses half the
-// lines of complex float (same registers per thread).
+// three choices per length for the plan's tuner -- 0 and 1 two heights, 2 the
+// height of 0 with each thread moving two adjacent lines as one 16-byte access
+// (complex float, batch mode, lines in aligned pairs; elsewhere it is 0);
+// complex double uses half the lines of complex float (same registers per
+// thread).
+constexpr int kBatchVariants = 3;
 __host__ __device__ constexpr int batch_lines_f32(int n, int v) {
-    return (n == 48 || n == 256 || n == 512) ? (v ? 8 : 16) : (v ? 16 : 32);
+    return (n == 48 || n == 256 || n == 512) ? (v == 1 ? 8 : 16) : (v == 1 ? 16 : 32);
+}
+template <typename T> __host__ __device__ constexpr int batch_lpt(int v, int mode) {
+    return (v == 2 && sizeof(T) == 4 && mode == MODE_BATCH) ? 2 : 1;
 }
 template <typename T> __host__ __device__ constexpr int batch_lines(int n, int v) {
     return sizeof(T) == 4 ? batch_lines_f32(n, v) : batch_lines_f32(n, v) / 2;
@@ -73,20 +80,22 @@ struct BatchArgs {
 // loads of tile t+1, which stay in flight through stages 1..S-1 of tile t.
 // Loads read through L2 only (__ldcg): other CTAs of this launch wrote the
 // data (earlier passes).
-template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV>
+template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV, int LPT = 1>
 __device__ __forceinline__ void rpipe_run(const PassArgs<T>& a, int t0, int m, unsigned char* smem_raw, int tid) {
-    using E = cx<T>;
-    using G = TileGeom<MODE, B, PLAN::N, sizeof(E)>;
+    using E = typename ElemOf<T, LPT>::type;
+    constexpr int BV = B / LPT;
+    using G = TileGeom<MODE, BV, PLAN::N, sizeof(E)>;
     constexpr int N = PLAN::N;
     constexpr int R0 = PLAN::r[0];
     constexpr int NBL = N / R0;
-    constexpr int NBT = B * NBL;
+    constexpr int NBT = BV * NBL;
     constexpr int K = (NBT + THREADS - 1) / THREADS;
     constexpr bool EXACT = (NBT % THREADS) == 0;
     constexpr int TWN = PLAN::twtotal();
     constexpr bool BFAST0 = (MODE == MODE_BATCH);
     static_assert(PLAN::S >= 2, "the pipelined run needs at least two stages");
-    static_assert(MODE != MODE_BATCH || THREADS % B == 0, "batch mode needs THREADS % B == 0");
+    static_assert(MODE != MODE_BATCH || THREADS % BV == 0, "batch mode needs THREADS % (B/LPT) == 0");
+    static_assert(LPT == 1 || MODE == MODE_BATCH, "line pairs only in batch mode");
 
     E* tile = reinterpret_cast<E*>(smem_raw);
     cx<T>* tw = reinterpret_cast<cx<T>*>(tile + G::elems);
@@ -109,15 +118,16 @@ __device__ __forceinline__ void rpipe_run(const PassArgs<T>& a, int t0, int m, u
             const int q = tid + k * THREADS;
             if (EXACT || q < NBT) {
                 int b, j;
-                bf_map<BFAST0, B, NBL>(q, b, j);
-                const cx<T>* line = a.src + ubase + __ldg(a.offV + v0 + b);
+                bf_map<BFAST0, BV, NBL>(q, b, j);
+                const cx<T>* line = a.src + ubase + __ldg(a.offV + v0 + b * LPT);
                 if (a.split) {
                     const cx<T>* p = line + __ldg(a.offA + j);
 #pragma unroll
-                    for (int r = 0; r < R0; ++r) x[k][r] = __ldcg(p + d0[r]);
+                    for (int r = 0; r < R0; ++r) x[k][r] = __ldcg(reinterpret_cast<const E*>(p + d0[r]));
                 } else {
 #pragma unroll
-                    for (int r = 0; r < R0; ++r) x[k][r] = __ldcg(line + __ldg(a.offA + j + r * NBL));
+                    for (int r = 0; r < R0; ++r)
+                        x[k][r] = __ldcg(reinterpret_cast<const E*>(line + __ldg(a.offA + j + r * NBL)));
                 }
             }
         }
@@ -131,14 +141,14 @@ __device__ __forceinline__ void rpipe_run(const PassArgs<T>& a, int t0, int m, u
             const int u = t / tilesV;
             const int v0 = (t - u * tilesV) * B;
             const size_t ubase = __ldg(a.offU + u);
-            for (int i = tid; i < B; i += THREADS) base_s[i] = ubase + __ldg(a.offV + v0 + i);
+            for (int i = tid; i < BV; i += THREADS) base_s[i] = ubase + __ldg(a.offV + v0 + i * LPT);
         }
 #pragma unroll
         for (int k = 0; k < K; ++k) {
             const int q = tid + k * THREADS;
             if (EXACT || q < NBT) {
                 int b, j;
-                bf_map<BFAST0, B, NBL>(q, b, j);
+                bf_map<BFAST0, BV, NBL>(q, b, j);
                 Dft<R0, INV, E>::run(x[k]);
 #pragma unroll
                 for (int r = 0; r < R0; ++r) tile[G::idx(b, j * R0 + r)] = x[k][r];
@@ -146,7 +156,7 @@ __device__ __forceinline__ void rpipe_run(const PassArgs<T>& a, int t0, int m, u
         }
         if (t + 1 < t0 + m) load_tile(t + 1, x);  // in flight through the remaining stages
         __syncthreads();
-        run_stage<T, PLAN, B, THREADS, MODE, INV, 1, 1>(a, tile, tw, offA_s, base_s, tid);
+        run_stage<T, PLAN, B, THREADS, MODE, INV, LPT, 1>(a, tile, tw, offA_s, base_s, tid);
         __syncthreads();  // tile and line bases free for the next tile
     }
 }
@@ -172,7 +182,8 @@ __device__ __noinline__ void batch_tile(cx<T>* data, const uint32_t* offA, const
     pa.split = split;
     pa.err = nullptr;
     pa.tcb = nullptr;
-    rpipe_run<T, P, batch_lines<T>(N, V), kBatchThreads, MODE, INV>(pa, tile, count, smem, tid);
+    rpipe_run<T, P, batch_lines<T>(N, V), kBatchThreads, MODE, INV, batch_lpt<T>(V, MODE)>(pa, tile, count, smem,
+                                                                                           tid);
 }
 
 template <typename T, bool INV, int N>
@@ -182,9 +193,9 @@ __device__ __forceinline__ void batch_len(cx<T>* data, const uint32_t* offA, con
 #define A2A_BT(V_, M_) \
     batch_tile<T, INV, N, V_, M_>(data, offA, offU, offV, tw, NU, NV, scale, split, tile, count, smem, tid)
     if (mode == MODE_LINE) {
-        if (var == 0) A2A_BT(0, MODE_LINE); else A2A_BT(1, MODE_LINE);
+        if (var == 1) A2A_BT(1, MODE_LINE); else A2A_BT(0, MODE_LINE);
     } else {
-        if (var == 0) A2A_BT(0, MODE_BATCH); else A2A_BT(1, MODE_BATCH);
+        if (var == 0) A2A_BT(0, MODE_BATCH); else if (var == 1) A2A_BT(1, MODE_BATCH); else A2A_BT(2, MODE_BATCH);
     }
 #undef A2A_BT
 }
@@ -361,10 +372,12 @@ template <typename T> __host__ __device__ constexpr size_t batch_smem_bytes() {
 #define A2A_BATCH_SMEM(N_)                                                                                    \
     {                                                                                                         \
         using P = typename PassPlan<T, N_>::Plan;                                                             \
-        const size_t v[4] = {pass_smem_bytes<T, P, batch_lines<T>(N_, 0), MODE_LINE, KIND_DIRECT, 1>(),       \
-                             pass_smem_bytes<T, P, batch_lines<T>(N_, 0), MODE_BATCH, KIND_DIRECT, 1>(),      \
-                             pass_smem_bytes<T, P, batch_lines<T>(N_, 1), MODE_LINE, KIND_DIRECT, 1>(),       \
-                             pass_smem_bytes<T, P, batch_lines<T>(N_, 1), MODE_BATCH, KIND_DIRECT, 1>()};     \
+        const size_t v[5] = {                                                                                 \
+            pass_smem_bytes<T, P, batch_lines<T>(N_, 0), MODE_LINE, KIND_DIRECT, 1>(),                        \
+            pass_smem_bytes<T, P, batch_lines<T>(N_, 0), MODE_BATCH, KIND_DIRECT, 1>(),                       \
+            pass_smem_bytes<T, P, batch_lines<T>(N_, 1), MODE_LINE, KIND_DIRECT, 1>(),                        \
+            pass_smem_bytes<T, P, batch_lines<T>(N_, 1), MODE_BATCH, KIND_DIRECT, 1>(),                       \
+            pass_smem_bytes<T, P, batch_lines<T>(N_, 2), MODE_BATCH, KIND_DIRECT, batch_lpt<T>(2, MODE_BATCH)>()}; \
         for (size_t x : v) m = x > m ? x : m;                                                                 \
     }
     A2A_BATCH_FOR_EACH_N(A2A_BATCH_SMEM)

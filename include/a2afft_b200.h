@@ -343,8 +343,10 @@ a2a_status a2a_batch_make_plans(a2a_batch* batch, void** d_scratch);
  * items a CTA takes per queue access (1..64; fewer as the queue drains).  prefetch = 1: each CTA asks L2 for
  * its next tile while it transforms the current one. */
 a2a_status a2a_batch_set_schedule(a2a_batch* batch, int fused, int claim, int prefetch);
-/* Tile height choice (0 or 1) for one length in line (batch_mode = 0, the Z
- * pass) or batch mode (the X and Y passes). */
+/* Tile choice for one length in line (batch_mode = 0, the Z pass) or batch
+ * mode (the X and Y passes): 0 and 1 are two tile heights; 2 (batch mode,
+ * A2A_C64, boxes whose lines pair into aligned 16-byte accesses) is height 0
+ * with each thread moving two adjacent lines at once. */
 a2a_status a2a_batch_select_variant(a2a_batch* batch, int length, int batch_mode, int variant);
 /* 1 (default): replay a captured CUDA graph; 0: plain launches. */
 a2a_status a2a_batch_set_graph(a2a_batch* batch, int enable);

@@ -98,6 +98,35 @@ def test_batch_schedules_agree_bitwise(pkg, oracle, cuda, fused, claim, prefetch
     assert torch.equal(flat, flat2)
 
 
+def test_batch_line_pairs_bit_identical(pkg, oracle, cuda):
+    """Variant 2 (batch mode, each thread moving two adjacent lines as one
+    16-byte access) computes every line exactly as variant 0 does."""
+    import torch
+
+    P, prec = 4, "c64"
+    ref_b = pkg.a2aBatch(SMALL, P, prec)
+    flat, views, _ = fill(pkg, oracle, cuda, ref_b, prec, seed=23)
+    flat2 = flat.clone()
+    views2 = [flat2[o:o + n] for o, n in zip(ref_b.offsets()[:-1], ref_b.elements)]
+    ref_b.forward(views)
+    ref_b.inverse(views)
+    b = pkg.a2aBatch(SMALL, P, prec)
+    paired = 0
+    for n in (32, 48, 64, 96, 128, 192, 256, 512):
+        try:
+            b.select_variant(n, True, 2)
+            paired += 1
+        except pkg.A2AError:
+            pass  # unused length, or a box whose lines do not pair
+    assert paired >= 4, b.plan_report()
+    assert "as pairs" in b.plan_report()
+    with pytest.raises(pkg.A2AError):
+        b.select_variant(64, False, 2)  # line mode has no pairs
+    b.forward(views2)
+    b.inverse(views2)
+    assert torch.equal(flat, flat2)
+
+
 def test_batch_variants_and_autotune(pkg, oracle, cuda):
     P, prec = 4, "c64"
     b = pkg.a2aBatch(SMALL, P, prec)
