@@ -157,6 +157,7 @@ template <typename T, int N> struct PlanOf<T, N, KIND_TMAT2W> { using Plan = typ
     X(float,  512, KIND_TMAT2,   4, 128, 4, 1)      \
     X(float,  512, KIND_TMAT3,   4, 128, 3, 1)      \
     X(float,  512, KIND_TMAT2,   8, 128, 3, 1)      \
+    X(float,  512, KIND_RPIPE,   8, 128, 4, 1)      \
     X(float,  512, KIND_TMAT2W,  8, 128, 2, 1)      \
     X(float,  512, KIND_TMAT2W,  8, 256, 2, 1)      \
     X(float,  512, KIND_TMAT2W, 16, 256, 1, 2)      \
@@ -166,6 +167,7 @@ template <typename T, int N> struct PlanOf<T, N, KIND_TMAT2W> { using Plan = typ
     X(float, 1024, KIND_TMAT2,   8, 512, 1, 1)      \
     X(float, 1024, KIND_TMAT2,   2, 128, 4, 1)      \
     X(float, 1024, KIND_TMAT3,   4, 256, 1, 2)      \
+    X(float, 1024, KIND_RPIPE,   4, 256, 2, 1)      \
     X(float, 1024, KIND_TMAT2W,  8, 256, 1, 1)      \
     X(float, 1024, KIND_TMAT2W,  4, 128, 2, 1)      \
     X(float,  768, KIND_TMAT2,   4, 128, 3, 1)

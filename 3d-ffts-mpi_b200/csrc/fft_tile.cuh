@@ -872,7 +872,13 @@ __global__ void __launch_bounds__(THREADS, MINB) fft_tma_kernel(const PassArgs<T
         const int slot = it % NBUF;
         const bool ok = mbar_wait_bounded(bar + slot, (uint32_t)((it / NBUF) & 1));
         if (__syncthreads_or(!ok)) {
-            if (tid == 0) atomicExch(a.err, 1);
+            if (tid == 0) {
+                atomicExch(a.err, 1);
+                // wait (bounded) for this CTA's copies still in flight before leaving
+                for (int j = it; j < it + NBUF; ++j)
+                    if (blockIdx.x + j * gridDim.x < (unsigned)ntiles)
+                        mbar_wait_bounded(bar + j % NBUF, (uint32_t)((j / NBUF) & 1));
+            }
             return;
         }
         run_stage<T, PLAN, B, THREADS, MODE_BATCH, INV, LPT, 0>(a, buf + slot * G::elems, tw, offA_s,
