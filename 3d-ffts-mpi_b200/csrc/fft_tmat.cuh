@@ -19,7 +19,7 @@
 // each completing on its own mbarrier; stage 0 reads its slot into
 // registers and writes the Stockham tile (BATCH rows narrower than a bank
 // row are swizzled, see TileGeom), which frees the slot for the tile NSTG
-// ahead while stages 1..S-1 run.  No copy here uses cluster multicast.
+// ahead while stages 1..S-1 run.  Every copy is a plain single-CTA tensor copy.
 #pragma once
 
 #include <cuda.h>
