@@ -151,6 +151,7 @@ template <typename T, int N> struct PlanOf<T, N, KIND_TMAT2W> { using Plan = typ
     X(float,  128, KIND_TMAT2,  32, 256, 2, 1)      \
     X(float,  256, KIND_TMAT2,  16, 256, 2, 1)      \
     X(float,  256, KIND_TMAT3,  16, 256, 1, 1)      \
+    X(float,  256, KIND_TMATI,  16, 256, 2, 1)      \
     X(float,  512, KIND_TMAT2,   8, 256, 2, 1)      \
     X(float,  512, KIND_TMAT3,   8, 256, 1, 1)      \
     X(float,  512, KIND_TMAT2,  16, 512, 1, 2)      \
@@ -158,6 +159,8 @@ template <typename T, int N> struct PlanOf<T, N, KIND_TMAT2W> { using Plan = typ
     X(float,  512, KIND_TMAT3,   4, 128, 3, 1)      \
     X(float,  512, KIND_TMAT2,   8, 128, 3, 1)      \
     X(float,  512, KIND_RPIPE,   8, 128, 4, 1)      \
+    X(float,  512, KIND_TMATI,   8, 128, 3, 1)      \
+    X(float,  512, KIND_TMATI,   8, 256, 2, 1)      \
     X(float,  512, KIND_TMAT2W,  8, 128, 2, 1)      \
     X(float,  512, KIND_TMAT2W,  8, 256, 2, 1)      \
     X(float,  512, KIND_TMAT2W, 16, 256, 1, 2)      \
@@ -168,9 +171,12 @@ template <typename T, int N> struct PlanOf<T, N, KIND_TMAT2W> { using Plan = typ
     X(float, 1024, KIND_TMAT2,   2, 128, 4, 1)      \
     X(float, 1024, KIND_TMAT3,   4, 256, 1, 2)      \
     X(float, 1024, KIND_RPIPE,   4, 256, 2, 1)      \
+    X(float, 1024, KIND_TMATI,   8, 256, 1, 1)      \
+    X(float, 1024, KIND_TMATI,   8, 512, 1, 1)      \
     X(float, 1024, KIND_TMAT2W,  8, 256, 1, 1)      \
     X(float, 1024, KIND_TMAT2W,  4, 128, 2, 1)      \
-    X(float,  768, KIND_TMAT2,   4, 128, 3, 1)
+    X(float,  768, KIND_TMAT2,   4, 128, 3, 1)      \
+    X(float,  768, KIND_TMATI,   8, 256, 2, 1)
 
 #define A2A_VARIANTS_F64(X)                         \
     X(double,    4, KIND_DIRECT,  4,  32, 1, 1)     \
@@ -216,8 +222,10 @@ template <typename T, int N> struct PlanOf<T, N, KIND_TMAT2W> { using Plan = typ
     X(double, 1024, KIND_DIRECT,  4, 256, 1, 1)     \
     X(double,  256, KIND_TMAT2,   8, 256, 2, 1)     \
     X(double,  512, KIND_TMAT2,   4, 256, 2, 1)     \
+    X(double,  512, KIND_TMATI,   4, 128, 3, 1)     \
     X(double,  512, KIND_TMAT2,   8, 512, 1, 1)     \
     X(double,  768, KIND_TMAT2,   4, 192, 1, 1)     \
+    X(double,  768, KIND_TMATI,   4, 192, 2, 1)     \
     X(double,  768, KIND_TMAT2,   2, 128, 3, 1)     \
     X(double,  768, KIND_TMAT3,   2, 128, 2, 1)     \
     X(double,  512, KIND_TMAT2,   2, 128, 4, 1)     \
@@ -230,9 +238,9 @@ template <typename T, int N, int KIND, int B, int TH, int MB, int LPT, int MODE,
 PassKernel make_pass_kernel() {
     using P = typename PlanOf<T, N, KIND>::Plan;
     PassKernel k;
-    if constexpr (KIND == KIND_TMAT2 || KIND == KIND_TMAT3 || KIND == KIND_TMAT2W)
+    if constexpr (KIND == KIND_TMAT2 || KIND == KIND_TMAT3 || KIND == KIND_TMAT2W || KIND == KIND_TMATI)
         k.fn = reinterpret_cast<const void*>(
-            &fft_tmat_kernel<T, P, B, TH, MODE, INV, MB, LPT, (KIND == KIND_TMAT3 ? 3 : 2)>);
+            &fft_tmat_kernel<T, P, B, TH, MODE, INV, MB, LPT, (KIND == KIND_TMAT3 ? 3 : 2), KIND == KIND_TMATI>);
     else if constexpr (KIND == KIND_PIPE)
         k.fn = reinterpret_cast<const void*>(&fft_pipe_kernel<T, P, B, TH, MODE, INV, MB, LPT>);
     else if constexpr (KIND == KIND_TMA)
@@ -247,8 +255,8 @@ PassKernel make_pass_kernel() {
     k.lines = B;
     k.min_blocks = MB;
     k.lpt = LPT;
-    if constexpr (KIND == KIND_TMAT2 || KIND == KIND_TMAT3 || KIND == KIND_TMAT2W)
-        k.smem = tmat_smem_bytes<T, P, B, MODE, LPT, (KIND == KIND_TMAT3 ? 3 : 2)>();
+    if constexpr (KIND == KIND_TMAT2 || KIND == KIND_TMAT3 || KIND == KIND_TMAT2W || KIND == KIND_TMATI)
+        k.smem = tmat_smem_bytes<T, P, B, MODE, LPT, (KIND == KIND_TMAT3 ? 3 : 2), KIND == KIND_TMATI>();
     else
         k.smem = pass_smem_bytes<T, P, B, MODE, KIND, LPT>();
     k.nstages = P::S;
@@ -280,7 +288,7 @@ bool make_variant(int mode, bool inv, PassKernel* out) {
 int find_pass_kernels_f32(int n, int mode, bool inverse, PassKernel* out, int max);
 int find_pass_kernels_f64(int n, int mode, bool inverse, PassKernel* out, int max);
 
-constexpr int kMaxVariants = 24;
+constexpr int kMaxVariants = 32;
 
 // fft_tc.cu: the split-precision tensor-core kernel of length n (fmt 0 =
 // fp16, 1 = bf16); false when n has none.

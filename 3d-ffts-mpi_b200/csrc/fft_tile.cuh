@@ -455,7 +455,8 @@ enum PassKind : int {
     KIND_RPIPE = 4,   // persistent CTAs, next tile's stage-0 loads in flight in registers
     KIND_TMAT2 = 5,   // persistent CTAs, whole tiles fetched by TMA tensor copies into a 2-slot ring
     KIND_TMAT3 = 6,   // the same with a 3-slot ring
-    KIND_TMAT2W = 7   // the 2-slot ring with the length's two-stage wide-radix plan (radix 16/32)
+    KIND_TMAT2W = 7,  // the 2-slot ring with the length's two-stage wide-radix plan (radix 16/32)
+    KIND_TMATI = 8    // the 2-slot ring with each slot transformed in place (no separate tile)
 };
 
 constexpr int kTmaBuffers = 2;

@@ -47,14 +47,25 @@ template <typename T, int B, int N> __host__ __device__ constexpr uint32_t tmat_
     return (uint32_t)((B * N * sizeof(cx<T>) + kTmatAlign - 1) / kTmatAlign * kTmatAlign);
 }
 
-template <typename T, class PLAN, int B, int MODE, int LPT, int NSTG>
+// In-place rings (INPLACE): each slot also serves as its tile's Stockham tile,
+// so a slot holds the larger of the copy and the (padded) tile.
+template <typename T, class PLAN, int B, int MODE, int LPT, bool INPLACE>
+__host__ __device__ constexpr uint32_t tmat_slot_bytes_for() {
+    using E = typename ElemOf<T, LPT>::type;
+    constexpr size_t tile = sizeof(E) * (size_t)TileGeom<MODE, B / LPT, PLAN::N, sizeof(E)>::elems;
+    constexpr uint32_t copy = tmat_slot_bytes<T, B, PLAN::N>();
+    constexpr uint32_t t = (uint32_t)((tile + kTmatAlign - 1) / kTmatAlign * kTmatAlign);
+    return INPLACE && t > copy ? t : copy;
+}
+
+template <typename T, class PLAN, int B, int MODE, int LPT, int NSTG, bool INPLACE = false>
 __host__ __device__ constexpr size_t tmat_smem_bytes() {
     using E = typename ElemOf<T, LPT>::type;
     constexpr int N = PLAN::N;
     constexpr int BV = B / LPT;
     size_t bytes = kTmatAlign;  // room to align the ring
-    bytes += (size_t)NSTG * tmat_slot_bytes<T, B, N>();
-    bytes += sizeof(E) * (size_t)TileGeom<MODE, BV, N, sizeof(E)>::elems;
+    bytes += (size_t)NSTG * tmat_slot_bytes_for<T, PLAN, B, MODE, LPT, INPLACE>();
+    if (!INPLACE) bytes += sizeof(E) * (size_t)TileGeom<MODE, BV, N, sizeof(E)>::elems;
     bytes += sizeof(cx<T>) * (size_t)PLAN::twtotal();
     bytes += sizeof(uint32_t) * (size_t)N;
     bytes = (bytes + 15) & ~size_t(15);
@@ -98,7 +109,11 @@ __device__ __forceinline__ void tmat_issue(const TmatMaps& m, int t, int tilesV,
     }
 }
 
-template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV, int MINB, int LPT, int NSTG>
+// INPLACE: every slot is its tile's Stockham tile; a slot is refilled (with
+// the tile NSTG ahead) once its tile is done -- less shared memory per CTA
+// (more CTAs per SM) for a shorter prefetch distance.
+template <typename T, class PLAN, int B, int THREADS, int MODE, bool INV, int MINB, int LPT, int NSTG,
+          bool INPLACE = false>
 __global__ void __launch_bounds__(THREADS, MINB) fft_tmat_kernel(const PassArgs<T> a, const __grid_constant__ TmatMaps m) {
     using E = typename ElemOf<T, LPT>::type;
     constexpr int BV = B / LPT;
@@ -112,7 +127,7 @@ __global__ void __launch_bounds__(THREADS, MINB) fft_tmat_kernel(const PassArgs<
     constexpr bool EXACT = (NBT % THREADS) == 0;
     constexpr int TWN = PLAN::twtotal();
     constexpr bool BFAST0 = (MODE == MODE_BATCH);
-    constexpr uint32_t SLOT = tmat_slot_bytes<T, B, N>();
+    constexpr uint32_t SLOT = tmat_slot_bytes_for<T, PLAN, B, MODE, LPT, INPLACE>();
     static_assert(PLAN::S >= 2, "the ring kernel needs at least two stages");
     static_assert(MODE != MODE_BATCH || THREADS % BV == 0, "batch mode needs THREADS % (B/LPT) == 0");
     static_assert(LPT == 1 || MODE == MODE_BATCH, "line pairs only in batch mode");
@@ -121,12 +136,11 @@ __global__ void __launch_bounds__(THREADS, MINB) fft_tmat_kernel(const PassArgs<
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const uint32_t s0 = smem_u32(smem_raw);
     unsigned char* ring = smem_raw + (((s0 + kTmatAlign - 1) & ~(kTmatAlign - 1)) - s0);
-    E* tile = reinterpret_cast<E*>(ring + NSTG * SLOT);
-    cx<T>* tw = reinterpret_cast<cx<T>*>(tile + G::elems);
+    E* const xtile = reinterpret_cast<E*>(ring + NSTG * SLOT);  // separate tile (not INPLACE)
+    cx<T>* tw = reinterpret_cast<cx<T>*>(INPLACE ? ring + NSTG * SLOT : reinterpret_cast<unsigned char*>(xtile + G::elems));
     uint32_t* offA_s = reinterpret_cast<uint32_t*>(tw + TWN);
     size_t* base_s = reinterpret_cast<size_t*>(
-        reinterpret_cast<unsigned char*>(tile) +
-        ((sizeof(E) * (size_t)G::elems + sizeof(cx<T>) * TWN + sizeof(uint32_t) * N + 15) & ~size_t(15)));
+        reinterpret_cast<unsigned char*>(tw) + ((sizeof(cx<T>) * TWN + sizeof(uint32_t) * N + 15) & ~size_t(15)));
     unsigned long long* bar = reinterpret_cast<unsigned long long*>(base_s + BV);
 
     const int tid = threadIdx.x;
@@ -165,6 +179,7 @@ __global__ void __launch_bounds__(THREADS, MINB) fft_tmat_kernel(const PassArgs<
         }
         // stage 0 from the ring slot
         const E* src = reinterpret_cast<const E*>(ring + s * SLOT);
+        E* tile = INPLACE ? reinterpret_cast<E*>(ring + s * SLOT) : xtile;
         E x[K][R0];
 #pragma unroll
         for (int k = 0; k < K; ++k) {
@@ -189,19 +204,33 @@ __global__ void __launch_bounds__(THREADS, MINB) fft_tmat_kernel(const PassArgs<
                         x[k][r] = src[(q2 * B + b) * m.chunk + zl];
                     }
                 }
+            }
+        }
+        if constexpr (INPLACE) __syncthreads();  // every read of the slot before it is rewritten
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int q = tid + k * THREADS;
+            if (EXACT || q < NBT) {
+                int b, j;
+                bf_map<BFAST0, BV, NBL>(q, b, j);
                 Dft<R0, INV, E>::run(x[k]);
 #pragma unroll
                 for (int r = 0; r < R0; ++r) tile[G::idx(b, j * R0 + r)] = x[k][r];
             }
         }
         __syncthreads();  // slot s read out; the tile and its line bases are ready
-        if (tid == 0 && issued < mine) {
+        if (!INPLACE && tid == 0 && issued < mine) {
             fence_proxy_async_smem();  // the generic reads of slot s come before the async writes
             tmat_issue<T, B, N>(m, blockIdx.x + issued * gridDim.x, tilesV, ring + s * SLOT, bar + s);
             ++issued;
         }
         run_stage<T, PLAN, B, THREADS, MODE, INV, LPT, 1, SWSH>(a, tile, tw, offA_s, base_s, tid);
         __syncthreads();  // tile and line bases free for the next tile
+        if (INPLACE && tid == 0 && issued < mine) {  // the slot's tile is done: refill it
+            fence_proxy_async_smem();
+            tmat_issue<T, B, N>(m, blockIdx.x + issued * gridDim.x, tilesV, ring + s * SLOT, bar + s);
+            ++issued;
+        }
     }
 }
 
