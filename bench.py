@@ -65,6 +65,7 @@ def parse_args():
     ap.add_argument("--ranks", type=int, default=RANKS)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg")
+    ap.add_argument("--no-vendor", action="store_true", help="skip the cuFFT context leg")
     ap.add_argument("--no-check", action="store_true", help="skip the accuracy check (profiling runs)")
     ap.add_argument("--workload", choices=["cube", "batch"], default="cube")
     ap.add_argument("--layout", choices=["replicas", "fused"], default="replicas",
@@ -184,9 +185,10 @@ class ClockSampler:
 def pipelined_e2e(torch, hin, houts, bufs, run, ke, dev):
     """End-to-end steps through the public API with pinned host buffers: each
     step copies its input host -> device, runs `run(buf, stream)` and copies
-    the result device -> host.  Two device buffers and three streams let step
-    i+1's upload overlap step i's download (the link is full duplex) and
-    compute; returns ms per step over `ke` steps after two untimed ones."""
+    the result device -> host.  Two or more device buffers (used in turn) and
+    three streams let step i+1's upload overlap step i's download (the link is
+    full duplex) and compute; returns ms per step over `ke` steps after two
+    untimed ones."""
     s_in, s_run, s_out = (torch.cuda.Stream(device=dev) for _ in range(3))
     freed = [torch.cuda.Event() for _ in bufs]  # the buffer's last download is done
     for f in freed:
@@ -218,6 +220,29 @@ def pipelined_e2e(torch, hin, houts, bufs, run, ke, dev):
     e1.record(s_out)
     torch.cuda.synchronize()
     return e0.elapsed_time(e1) / ke
+
+
+def vendor_fft_ms(torch, buf, ng, steps, warmup):
+    """cuFFT -- the library behind the reference's 1D transforms -- as a plain
+    single-GPU 3D transform of a cube of the same size through torch.fft
+    (fftn then ifftn, natural order, out of place, no virtual-rank bricks):
+    context for the pass kernels' speed, not a run of the reference's pipeline.
+    Returns ms per forward+inverse on the current stream."""
+    cube = buf.view(ng, ng, ng)
+    out, back = torch.empty_like(cube), torch.empty_like(cube)
+    for _ in range(warmup):
+        torch.fft.fftn(cube, out=out)
+        torch.fft.ifftn(out, out=back)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        torch.fft.fftn(cube, out=out)
+        torch.fft.ifftn(out, out=back)
+    e1.record()
+    torch.cuda.synchronize()
+    del out, back
+    return e0.elapsed_time(e1) / steps
 
 
 def measured_peak():
@@ -643,6 +668,17 @@ def run_ours(args, rank, world, local_rank):
                "d2h_bytes_per_step": nbytes_buf, "steps": ke,
                "pipelined": "2 device buffers: step i+1's upload overlaps step i's download"}
         del hin, houts
+        torch.cuda.empty_cache()
+
+    vendor = None
+    if world == 1 and not args.no_vendor:
+        vendor = {"library": "cuFFT via torch.fft.fftn + ifftn", "ms_per_step": None,
+                  "layout": "one natural-order cube, out of place (no virtual-rank bricks)"}
+        try:
+            vendor["ms_per_step"] = round(vendor_fft_ms(torch, x, ng, min(args.steps, 20), max(args.warmup, 3)), 4)
+        except RuntimeError as e:  # e.g. out of memory for the out-of-place buffers
+            vendor["error"] = str(e).splitlines()[0]
+        torch.cuda.empty_cache()
 
     if rank != 0:
         return
@@ -679,6 +715,7 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clk.summary(),
         "gpu_launches": 6 * args.steps,
         "e2e": e2e,
+        "vendor_fft": vendor,
     }
     if world == 1 and not args.no_cpu:
         ms, cores, sample, _ = cpu_pipeline_ms(CPU_SAMPLE_NG, ranks, ng, precision=prec, seed=seed, tones=tones)
