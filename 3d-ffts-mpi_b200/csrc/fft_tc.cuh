@@ -10,12 +10,15 @@
 // x = xh + xl after scaling each row by a power of two into [-1, 1),
 // R = Rh + Rl (generated in FP64 on the host), and the product keeps the
 // three significant terms  xh Rh + xh Rl + xl Rh  (xl Rl is below FP32
-// rounding).  The A operand of a 128-row block is [xh | xl] (K = 64, K-major,
-// no swizzle); six K = 16 MMAs accumulate xh Rh into 32 FP32 columns of
-// tensor memory and the corrections xh Rl + xl Rh into 32 more, which each
-// warp reads back for its 32 rows with tcgen05.ld and adds in FP32.  A row is
-// one butterfly: the thread that built row m reads row m back, undoes its
-// scale and stores the 16 outputs.
+// rounding).  The A operand of a 128-row block, [xh | xl] (K = 64), lives in
+// tensor memory: each thread writes its row into its own lane with one
+// tcgen05.st (two 16-bit values per 32-bit column), so A never passes through
+// shared memory; B = [Rh | Rl] is in shared memory (K-major, no swizzle).  Six
+// K = 16 MMAs accumulate xh Rh into 32 FP32 columns of tensor memory and the
+// corrections xh Rl + xl Rh into 32 more, which each warp reads back for its
+// 32 rows with tcgen05.ld and adds in FP32.  A row is one butterfly: the
+// thread that built row m reads row m back, undoes its scale and stores the
+// 16 outputs.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -27,12 +30,10 @@ namespace a2a {
 
 enum TcFormat : int { TC_FP16 = 0, TC_BF16 = 1 };
 
-// Shared-memory operand layout (UMMA canonical K-major, SWIZZLE_NONE): an
-// 8-row x 16-byte core matrix is 128 contiguous bytes; core matrices step by
-// SBO = 128 bytes along M (or N) and by LBO bytes along K.
+// Shared-memory layout of the B operand (UMMA canonical K-major,
+// SWIZZLE_NONE): an 8-row x 16-byte core matrix is 128 contiguous bytes; core
+// matrices step by SBO = 128 bytes along N and by LBO bytes along K.
 constexpr int kTcRows = 128;                     // M of one MMA block
-constexpr int kTcChunkA = kTcRows / 8 * 128;     // bytes of one 8-wide K chunk of A (2048)
-constexpr int kTcBlockA = 8 * kTcChunkA;         // bytes of one A block: K = 64 halves (16 KB)
 constexpr int kTcChunkB = 32 / 8 * 128;          // bytes of one K chunk of B (N = 32): 512
 constexpr int kTcMatB = 4 * kTcChunkB;           // one 32 x 32 matrix: 2 KB
 constexpr int kTcBBytes = 2 * kTcMatB;           // Rh and Rl
@@ -60,8 +61,7 @@ template <int FMT> __device__ __forceinline__ void split16(float v, uint16_t& hi
 }
 
 struct TcCtx {
-    unsigned char* abuf;       // A blocks (kTcBlockA bytes each)
-    uint32_t a_addr, b_addr;   // shared addresses of A and of [Rh | Rl]
+    uint32_t b_addr;           // shared address of [Rh | Rl]
     uint32_t tmem;             // accumulator base (lane 0, column 0)
     unsigned long long* bar;   // MMA completion
     uint32_t phase;
@@ -70,13 +70,6 @@ struct TcCtx {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
 
-__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
-    asm volatile(
-        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
-        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)
-        : "memory");
-}
 __device__ __forceinline__ void tc_commit(unsigned long long* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
                      smem_u32(bar))
@@ -96,6 +89,31 @@ __device__ __forceinline__ void tc_ld32(uint32_t taddr, float* v) {
 #pragma unroll
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
+
+// A operand rows written into tensor memory: 32 columns of this warp's 32
+// lanes from 32 registers each.
+__device__ __forceinline__ void tc_st32(uint32_t taddr, const uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};\n" ::"r"(taddr),
+        "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]), "r"(r[16]), "r"(r[17]), "r"(r[18]), "r"(r[19]), "r"(r[20]), "r"(r[21]), "r"(r[22]), "r"(r[23]), "r"(r[24]), "r"(r[25]), "r"(r[26]), "r"(r[27]), "r"(r[28]), "r"(r[29]), "r"(r[30]), "r"(r[31])
+        : "memory");
+}
+__device__ __forceinline__ void tc_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory"); }
+// D = A B (+ D) with A in tensor memory (K-major, 16-bit values two to a
+// 32-bit column) and B in shared memory; no output lanes disabled.
+__device__ __forceinline__ void tc_mma_ts(uint32_t dtmem, uint32_t atmem, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t acc) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(dtmem),
+        "r"(atmem), "l"(bdesc), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+        : "memory");
+}
+
+// Tensor-memory columns of one 128-row block: the A operand (32 columns: hi
+// re, hi im, lo re, lo im, 8 each), then the two 32-column accumulators.
+constexpr int kTcBlockCols = 96;
+constexpr int kTcAccCol = 32;
 
 // One radix-16 stage on the tensor cores.  THREADS == butterflies per stage;
 // thread q owns butterfly q, i.e. A row q % 128 of block q / 128.
@@ -141,34 +159,29 @@ __device__ __forceinline__ void tc_stage(const PassArgs<float>& a, float2* tile,
     e = mx > 0.f ? min(max(e, -125), 126) : 0;
     const float down = __int_as_float((127 - e) << 23);  // 2^-e
     const float up = __int_as_float((127 + e) << 23);    // 2^e
-    // A row: chunks 0,1 = hi re; 2,3 = hi im; 4,5 = lo re; 6,7 = lo im
     {
-        const int row = tid % kTcRows;
-        unsigned char* rowp = ctx.abuf + (tid / kTcRows) * kTcBlockA + (row / 8) * 128 + (row % 8) * 16;
+        // the row into this warp's lanes of its block's A columns: 0-7 hi re,
+        // 8-15 hi im, 16-23 lo re, 24-31 lo im, values k and k+1 in the low
+        // and high half of column k/2
+        uint32_t w[32];
 #pragma unroll
-        for (int part = 0; part < 4; ++part) {  // re 0..7, re 8..15, im 0..7, im 8..15
-            uint16_t h[8], l[8];
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const int r = (part & 1) * 8 + i;
-                const float v = ((part < 2) ? x[r].x : x[r].y) * down;
-                split16<FMT>(v, h[i], l[i]);
-            }
-            uint4 hv, lv;
-            hv.x = h[0] | (uint32_t(h[1]) << 16);
-            hv.y = h[2] | (uint32_t(h[3]) << 16);
-            hv.z = h[4] | (uint32_t(h[5]) << 16);
-            hv.w = h[6] | (uint32_t(h[7]) << 16);
-            lv.x = l[0] | (uint32_t(l[1]) << 16);
-            lv.y = l[2] | (uint32_t(l[3]) << 16);
-            lv.z = l[4] | (uint32_t(l[5]) << 16);
-            lv.w = l[6] | (uint32_t(l[7]) << 16);
-            *reinterpret_cast<uint4*>(rowp + part * kTcChunkA) = hv;
-            *reinterpret_cast<uint4*>(rowp + (4 + part) * kTcChunkA) = lv;
+        for (int i = 0; i < 8; ++i) {
+            uint16_t h0, l0, h1, l1;
+            split16<FMT>(x[2 * i].x * down, h0, l0);
+            split16<FMT>(x[2 * i + 1].x * down, h1, l1);
+            w[i] = h0 | (uint32_t(h1) << 16);
+            w[16 + i] = l0 | (uint32_t(l1) << 16);
+            split16<FMT>(x[2 * i].y * down, h0, l0);
+            split16<FMT>(x[2 * i + 1].y * down, h1, l1);
+            w[8 + i] = h0 | (uint32_t(h1) << 16);
+            w[24 + i] = l0 | (uint32_t(l1) << 16);
         }
+        const int warp = tid / 32;
+        tc_st32(ctx.tmem + ((uint32_t)((warp % 4) * 32) << 16) + (uint32_t)((warp / 4) * kTcBlockCols), w);
+        tc_wait_st();
+        tc_fence_before();
+        __syncthreads();  // all A rows stored; all tile reads of this stage done
     }
-    fence_proxy_async_smem();  // the tensor cores read A through the async proxy
-    __syncthreads();           // all A rows written; all tile reads of this stage done
     if (tid == 0) {
         tc_fence_after();
         const uint32_t idesc = umma_idesc_f16(FMT);
@@ -178,23 +191,19 @@ __device__ __forceinline__ void tc_stage(const PassArgs<float>& a, float2* tile,
             // corrections xh Rl + xl Rh (2^-11 smaller), added in FP32 after
             // the read-back so the corrections do not share the main term's
             // accumulator rounding
-            const uint32_t dmain = ctx.tmem + blk * 64;
+            const uint32_t ab = ctx.tmem + blk * kTcBlockCols;  // lane 0 of the block's A columns
+            const uint32_t dmain = ab + kTcAccCol;
             const uint32_t dcorr = dmain + 32;
-            const uint32_t ab = ctx.a_addr + blk * kTcBlockA;
-            const uint64_t ah_re = umma_smem_desc(ab + 0 * kTcChunkA, kTcChunkA, 128);
-            const uint64_t ah_im = umma_smem_desc(ab + 2 * kTcChunkA, kTcChunkA, 128);
-            const uint64_t al_re = umma_smem_desc(ab + 4 * kTcChunkA, kTcChunkA, 128);
-            const uint64_t al_im = umma_smem_desc(ab + 6 * kTcChunkA, kTcChunkA, 128);
             const uint64_t rh_re = umma_smem_desc(ctx.b_addr + 0 * kTcChunkB, kTcChunkB, 128);
             const uint64_t rh_im = umma_smem_desc(ctx.b_addr + 2 * kTcChunkB, kTcChunkB, 128);
             const uint64_t rl_re = umma_smem_desc(ctx.b_addr + kTcMatB + 0 * kTcChunkB, kTcChunkB, 128);
             const uint64_t rl_im = umma_smem_desc(ctx.b_addr + kTcMatB + 2 * kTcChunkB, kTcChunkB, 128);
-            tc_mma(dmain, ah_re, rh_re, idesc, 0);
-            tc_mma(dmain, ah_im, rh_im, idesc, 1);
-            tc_mma(dcorr, ah_re, rl_re, idesc, 0);
-            tc_mma(dcorr, ah_im, rl_im, idesc, 1);
-            tc_mma(dcorr, al_re, rh_re, idesc, 1);
-            tc_mma(dcorr, al_im, rh_im, idesc, 1);
+            tc_mma_ts(dmain, ab + 0, rh_re, idesc, 0);
+            tc_mma_ts(dmain, ab + 8, rh_im, idesc, 1);
+            tc_mma_ts(dcorr, ab + 0, rl_re, idesc, 0);
+            tc_mma_ts(dcorr, ab + 8, rl_im, idesc, 1);
+            tc_mma_ts(dcorr, ab + 16, rh_re, idesc, 1);
+            tc_mma_ts(dcorr, ab + 24, rh_im, idesc, 1);
         }
         tc_commit(ctx.bar);
     }
@@ -204,7 +213,8 @@ __device__ __forceinline__ void tc_stage(const PassArgs<float>& a, float2* tile,
     float y[32], yc[32];
     {
         const int warp = tid / 32;
-        const uint32_t taddr = ctx.tmem + ((uint32_t)((warp % 4) * 32) << 16) + (warp / 4) * 64;
+        const uint32_t taddr = ctx.tmem + ((uint32_t)((warp % 4) * 32) << 16) +
+                               (uint32_t)((warp / 4) * kTcBlockCols + kTcAccCol);
         tc_ld32(taddr, y);
         tc_ld32(taddr + 32, yc);
     }
@@ -229,10 +239,9 @@ __device__ __forceinline__ void tc_stage(const PassArgs<float>& a, float2* tile,
 template <class PLAN, int B, int MODE>
 __host__ __device__ constexpr size_t tc_smem_bytes() {
     constexpr int N = PLAN::N;
-    constexpr int THREADS = B * N / 16;
     size_t bytes = sizeof(float2) * (size_t)TileGeom<MODE, B, N, sizeof(float2)>::elems;
     bytes = (bytes + 127) & ~size_t(127);
-    bytes += (size_t)(THREADS / kTcRows) * kTcBlockA + kTcBBytes;
+    bytes += kTcBBytes;
     bytes += sizeof(float2) * (size_t)PLAN::twtotal();
     bytes += sizeof(uint32_t) * (size_t)N;
     bytes = (bytes + 15) & ~size_t(15);
@@ -241,13 +250,16 @@ __host__ __device__ constexpr size_t tc_smem_bytes() {
 }
 
 // One CTA = one tile of B lines, THREADS = B N / 16.  Tensor memory:
-// 32 columns per 128-row block, allocated and freed by warp 0.
+// kTcBlockCols columns per 128-row block (rounded up to a power of two),
+// allocated and freed by warp 0.
 template <class PLAN, int B, int MODE, bool INV, int FMT>
 __global__ void __launch_bounds__(B * PLAN::N / 16, 1) fft_tc_kernel(const PassArgs<float> a) {
     constexpr int N = PLAN::N;
     constexpr int THREADS = B * N / 16;
     constexpr int NBLK = THREADS / kTcRows;
-    constexpr uint32_t TCOLS = NBLK <= 1 ? 64 : NBLK <= 2 ? 128 : NBLK <= 4 ? 256 : 512;  // 64 per block
+    constexpr int NEED = NBLK * kTcBlockCols;
+    static_assert(NEED <= 512, "tensor memory holds 512 columns");
+    constexpr uint32_t TCOLS = NEED <= 32 ? 32 : NEED <= 64 ? 64 : NEED <= 128 ? 128 : NEED <= 256 ? 256 : 512;
     using G = TileGeom<MODE, B, N, sizeof(float2)>;
     constexpr int TWN = PLAN::twtotal();
     constexpr int R0 = PLAN::r[0];
@@ -255,8 +267,6 @@ __global__ void __launch_bounds__(B * PLAN::N / 16, 1) fft_tc_kernel(const PassA
     extern __shared__ __align__(128) unsigned char smem_raw[];
     float2* tile = reinterpret_cast<float2*>(smem_raw);
     size_t off = (sizeof(float2) * (size_t)G::elems + 127) & ~size_t(127);
-    unsigned char* abuf = smem_raw + off;
-    off += (size_t)NBLK * kTcBlockA;
     unsigned char* bmat = smem_raw + off;
     off += kTcBBytes;
     float2* tw = reinterpret_cast<float2*>(smem_raw + off);
@@ -298,8 +308,6 @@ __global__ void __launch_bounds__(B * PLAN::N / 16, 1) fft_tc_kernel(const PassA
     tc_fence_after();
 
     TcCtx ctx;
-    ctx.abuf = abuf;
-    ctx.a_addr = smem_u32(abuf);
     ctx.b_addr = smem_u32(bmat);
     ctx.tmem = *tmem_slot;
     ctx.bar = bar;
