@@ -14,11 +14,13 @@
 // tensor memory: each thread writes its row into its own lane with one
 // tcgen05.st (two 16-bit values per 32-bit column), so A never passes through
 // shared memory; B = [Rh | Rl] is in shared memory (K-major, no swizzle).  Six
-// K = 16 MMAs accumulate xh Rh into 32 FP32 columns of tensor memory and the
-// corrections xh Rl + xl Rh into 32 more, which each warp reads back for its
-// 32 rows with tcgen05.ld and adds in FP32.  A row is one butterfly: the
-// thread that built row m reads row m back, undoes its scale and stores the
-// 16 outputs.
+// K = 16 MMAs accumulate, into one block of 32 FP32 columns of tensor memory,
+// first the corrections xh Rl + xl Rh (2^-11 smaller) and then the main term
+// xh Rh; each warp reads its 32 rows back with tcgen05.ld.  (Two accumulators
+// added in FP32 afterwards were 1.2e-7 more accurate but take 96 instead of
+// 64 columns per block, which halves the CTAs an SM's tensor memory holds.)
+// A row is one butterfly: the thread that built row m reads row m back,
+// undoes its scale and stores the 16 outputs.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -111,8 +113,8 @@ __device__ __forceinline__ void tc_mma_ts(uint32_t dtmem, uint32_t atmem, uint64
 }
 
 // Tensor-memory columns of one 128-row block: the A operand (32 columns: hi
-// re, hi im, lo re, lo im, 8 each), then the two 32-column accumulators.
-constexpr int kTcBlockCols = 96;
+// re, hi im, lo re, lo im, 8 each), then the 32-column accumulator.
+constexpr int kTcBlockCols = 64;
 constexpr int kTcAccCol = 32;
 
 // One radix-16 stage on the tensor cores.  THREADS == butterflies per stage;
@@ -187,40 +189,36 @@ __device__ __forceinline__ void tc_stage(const PassArgs<float>& a, float2* tile,
         const uint32_t idesc = umma_idesc_f16(FMT);
 #pragma unroll
         for (int blk = 0; blk < NBLK; ++blk) {
-            // two accumulators per block: the main term xh Rh, and the
-            // corrections xh Rl + xl Rh (2^-11 smaller), added in FP32 after
-            // the read-back so the corrections do not share the main term's
-            // accumulator rounding
+            // one accumulator per block: the corrections xh Rl + xl Rh
+            // (2^-11 smaller) first, then the main term xh Rh
             const uint32_t ab = ctx.tmem + blk * kTcBlockCols;  // lane 0 of the block's A columns
-            const uint32_t dmain = ab + kTcAccCol;
-            const uint32_t dcorr = dmain + 32;
+            const uint32_t dacc = ab + kTcAccCol;
             const uint64_t rh_re = umma_smem_desc(ctx.b_addr + 0 * kTcChunkB, kTcChunkB, 128);
             const uint64_t rh_im = umma_smem_desc(ctx.b_addr + 2 * kTcChunkB, kTcChunkB, 128);
             const uint64_t rl_re = umma_smem_desc(ctx.b_addr + kTcMatB + 0 * kTcChunkB, kTcChunkB, 128);
             const uint64_t rl_im = umma_smem_desc(ctx.b_addr + kTcMatB + 2 * kTcChunkB, kTcChunkB, 128);
-            tc_mma_ts(dmain, ab + 0, rh_re, idesc, 0);
-            tc_mma_ts(dmain, ab + 8, rh_im, idesc, 1);
-            tc_mma_ts(dcorr, ab + 0, rl_re, idesc, 0);
-            tc_mma_ts(dcorr, ab + 8, rl_im, idesc, 1);
-            tc_mma_ts(dcorr, ab + 16, rh_re, idesc, 1);
-            tc_mma_ts(dcorr, ab + 24, rh_im, idesc, 1);
+            tc_mma_ts(dacc, ab + 0, rl_re, idesc, 0);
+            tc_mma_ts(dacc, ab + 8, rl_im, idesc, 1);
+            tc_mma_ts(dacc, ab + 16, rh_re, idesc, 1);
+            tc_mma_ts(dacc, ab + 24, rh_im, idesc, 1);
+            tc_mma_ts(dacc, ab + 0, rh_re, idesc, 1);
+            tc_mma_ts(dacc, ab + 8, rh_im, idesc, 1);
         }
         tc_commit(ctx.bar);
     }
     const bool ok = mbar_wait_bounded(ctx.bar, ctx.phase);
     ctx.phase ^= 1u;
     tc_fence_after();
-    float y[32], yc[32];
+    float y[32];
     {
         const int warp = tid / 32;
         const uint32_t taddr = ctx.tmem + ((uint32_t)((warp % 4) * 32) << 16) +
                                (uint32_t)((warp / 4) * kTcBlockCols + kTcAccCol);
         tc_ld32(taddr, y);
-        tc_ld32(taddr + 32, yc);
     }
     if (!ok && (tid % 32) == 0) atomicExch(a.err, 1);
 #pragma unroll
-    for (int k = 0; k < 16; ++k) x[k] = make_float2((y[k] + yc[k]) * up, (y[16 + k] + yc[16 + k]) * up);
+    for (int k = 0; k < 16; ++k) x[k] = make_float2(y[k] * up, y[16 + k] * up);
     if constexpr (LAST) {
         float2* line = a.dst + base_s[b];
 #pragma unroll
