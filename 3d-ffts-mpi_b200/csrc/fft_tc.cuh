@@ -251,7 +251,7 @@ __host__ __device__ constexpr size_t tc_smem_bytes() {
 // kTcBlockCols columns per 128-row block (rounded up to a power of two),
 // allocated and freed by warp 0.
 template <class PLAN, int B, int MODE, bool INV, int FMT>
-__global__ void __launch_bounds__(B * PLAN::N / 16, 1) fft_tc_kernel(const PassArgs<float> a) {
+__global__ void __launch_bounds__(B * PLAN::N / 16, 4) fft_tc_kernel(const PassArgs<float> a) {
     constexpr int N = PLAN::N;
     constexpr int THREADS = B * N / 16;
     constexpr int NBLK = THREADS / kTcRows;
