@@ -117,13 +117,20 @@ __device__ __forceinline__ void tc_mma_ts(uint32_t dtmem, uint32_t atmem, uint64
 constexpr int kTcBlockCols = 64;
 constexpr int kTcAccCol = 32;
 
+// Row swizzle of a batch-mode tile (the pass kernels' rule): the first
+// stage's stride-R0 row writes of 8-line rows would otherwise meet 2-4-way
+// bank conflicts.
+template <class PLAN, int B, int MODE> __host__ __device__ constexpr int tc_tile_swizzle() {
+    return MODE == MODE_BATCH ? tile_swizzle_shift<PLAN, B, (int)sizeof(float2)>() : -1;
+}
+
 // One radix-16 stage on the tensor cores.  THREADS == butterflies per stage;
 // thread q owns butterfly q, i.e. A row q % 128 of block q / 128.
 template <class PLAN, int B, int THREADS, int MODE, bool INV, int FMT, int s, bool SRC_GLOBAL>
 __device__ __forceinline__ void tc_stage(const PassArgs<float>& a, float2* tile, const float2* tw,
                                          const uint32_t* offA_s, const size_t* base_s, TcCtx& ctx, int tid,
                                          size_t ubase, int v0) {
-    using G = TileGeom<MODE, B, PLAN::N, sizeof(float2)>;
+    using G = TileGeom<MODE, B, PLAN::N, sizeof(float2), tc_tile_swizzle<PLAN, B, MODE>()>;
     constexpr int N = PLAN::N;
     constexpr int R = PLAN::r[s];
     static_assert(R == 16, "tensor-core stages are radix 16");
@@ -258,7 +265,7 @@ __global__ void __launch_bounds__(B * PLAN::N / 16, 4) fft_tc_kernel(const PassA
     constexpr int NEED = NBLK * kTcBlockCols;
     static_assert(NEED <= 512, "tensor memory holds 512 columns");
     constexpr uint32_t TCOLS = NEED <= 32 ? 32 : NEED <= 64 ? 64 : NEED <= 128 ? 128 : NEED <= 256 ? 256 : 512;
-    using G = TileGeom<MODE, B, N, sizeof(float2)>;
+    using G = TileGeom<MODE, B, N, sizeof(float2), tc_tile_swizzle<PLAN, B, MODE>()>;
     constexpr int TWN = PLAN::twtotal();
     constexpr int R0 = PLAN::r[0];
 
