@@ -17,8 +17,9 @@
 // K = 16 MMAs accumulate, into one block of 32 FP32 columns of tensor memory,
 // first the corrections xh Rl + xl Rh (2^-11 smaller) and then the main term
 // xh Rh; each warp reads its 32 rows back with tcgen05.ld.  (Two accumulators
-// added in FP32 afterwards were 1.2e-7 more accurate but take 96 instead of
-// 64 columns per block, which halves the CTAs an SM's tensor memory holds.)
+// added in FP32 afterwards give a slightly smaller error -- 3.8e-7 instead of
+// 4.4e-7 relative L2 for a 512^3 transform -- but take 96 instead of 64
+// columns per block, which halves the CTAs an SM's tensor memory holds.)
 // A row is one butterfly: the thread that built row m reads row m back,
 // undoes its scale and stores the 16 outputs.
 #pragma once
