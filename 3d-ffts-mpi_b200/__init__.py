@@ -109,7 +109,7 @@ def _torch_dtype(prec: int):
 
 class a2aDistribution:
     """``a2aDistribution(MPI_Comm, int Ng, int blockSize)``
-    (``a2adistribution.cpp:85-154``) over ``world_size`` virtual ranks.
+    (``a2adistribution.cpp:44-113``) over ``world_size`` virtual ranks.
 
     ``Ng`` may be a 3-tuple ``(nx, ny, nz)`` for a box (an extension the
     reference does not have; only ``a2adfft`` accepts boxes)."""
@@ -195,7 +195,7 @@ class a2aDistribution:
             raise ValueError(f"buffer must be contiguous with local_ranks*nlocal = {n} elements")
         return bufptr(t.data_ptr())
 
-    # -- the six steps (a2adistribution.cpp:156-256) -------------------------
+    # -- the six steps (a2adistribution.cpp:115-215) -------------------------
     def getZPencils(self, d_Buff1, d_Buff2):
         call("a2a_get_z_pencils", self._h, self._buf(d_Buff1), self._buf(d_Buff2))
 
@@ -228,11 +228,11 @@ class a2aDistribution:
         call("a2a_" + kernel, self._h, self._buf(source), self._buf(dest))
 
     def write_dims(self, path: str) -> None:
-        """The reference's ``dims`` file (``a2adistribution.cpp:142-151``)."""
+        """The reference's ``dims`` file (``a2adistribution.cpp:101-111``)."""
         write_dims(self.Ng, self.world_size, path)
 
     def finalize(self) -> None:
-        """``a2aDistribution::finalize`` (``a2adistribution.cpp:258-265``)."""
+        """``a2aDistribution::finalize`` (``a2adistribution.cpp:217-224``)."""
         if self._h:
             call("a2a_distribution_finalize", self._h)
             self._h = None

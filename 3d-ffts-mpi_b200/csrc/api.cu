@@ -376,7 +376,7 @@ a2a_status setup_distribution(Dist& d, int nx, int ny, int nz, int P, int block_
     d.elem_bytes = prec == A2A_C128 ? 16 : 8;
     d.cube = (nx == ny && ny == nz);
     dims_create(P, d.dims);
-    for (int a = 0; a < 3; ++a)  // a2adistribution.cpp:102-104
+    for (int a = 0; a < 3; ++a)  // a2adistribution.cpp:61-63
         if (d.ng[a] % d.dims[a])
             return fail(A2A_ERROR_DECOMPOSITION, "N[%d]=%d is not divisible by dims[%d]=%d", a, d.ng[a], a, d.dims[a]);
     for (int a = 0; a < 3; ++a) d.local[a] = d.ng[a] / d.dims[a];
@@ -687,12 +687,15 @@ namespace {
 
 // Byte image of the split radix-16 operand for one direction: the real
 // 32 x 32 DFT matrix R (K x N: rows 0-15 take x_re, 16-31 x_im; columns 0-15
-// give y_re, 16-31 y_im), split as R = Rh + Rl in fp16 or bf16, stored as the
-// K-major N x K operand of the UMMA canonical no-swizzle layout: element
-// (n, k) at (k/8)*512 + (n/8)*128 + (n%8)*16 + (k%8)*2; Rh then Rl.
+// give y_re, 16-31 y_im), split from its FP64 values as R = Rh + Rl (fp16) or
+// Rh + Rm + Rl (bf16), each part the rounding of what the previous ones
+// leave, stored as the K-major N x K operand of the UMMA canonical
+// no-swizzle layout: element (n, k) at (k/8)*512 + (n/8)*128 + (n%8)*16 +
+// (k%8)*2; the parts one after the other.
 void tc_operand_image(bool inverse, int fmt, std::vector<uint16_t>& img) {
     const long double pi = acosl(-1.0L);
-    img.assign(a2a::kTcBBytes / 2, 0);
+    const int parts = a2a::tc_parts(fmt);
+    img.assign(a2a::tc_b_bytes(fmt) / 2, 0);
     for (int k = 0; k < 32; ++k)
         for (int n = 0; n < 32; ++n) {
             const int r = k % 16, c = n % 16;
@@ -702,19 +705,20 @@ void tc_operand_image(bool inverse, int fmt, std::vector<uint16_t>& img) {
             double v;
             if (k < 16) v = n < 16 ? C : S;
             else v = n < 16 ? -S : C;
-            uint16_t hi, lo;
-            if (fmt == a2a::TC_FP16) {
-                const __half h = __float2half_rn((float)v);
-                hi = __half_as_ushort(h);
-                lo = __half_as_ushort(__float2half_rn((float)(v - (double)__half2float(h))));
-            } else {
-                const __nv_bfloat16 h = __float2bfloat16_rn((float)v);
-                hi = __bfloat16_as_ushort(h);
-                lo = __bfloat16_as_ushort(__float2bfloat16_rn((float)(v - (double)__bfloat162float(h))));
-            }
             const size_t off = (size_t)(k / 8) * a2a::kTcChunkB + (n / 8) * 128 + (n % 8) * 16 + (k % 8) * 2;
-            img[off / 2] = hi;
-            img[(a2a::kTcMatB + off) / 2] = lo;
+            for (int q = 0; q < parts; ++q) {
+                uint16_t h;
+                if (fmt == a2a::TC_FP16) {
+                    const __half hh = __float2half_rn((float)v);
+                    h = __half_as_ushort(hh);
+                    v -= (double)__half2float(hh);
+                } else {
+                    const __nv_bfloat16 hh = __float2bfloat16_rn((float)v);
+                    h = __bfloat16_as_ushort(hh);
+                    v -= (double)__bfloat162float(hh);
+                }
+                img[(q * a2a::kTcMatB + off) / 2] = h;
+            }
         }
 }
 
@@ -757,16 +761,16 @@ a2a_status setup_tc(a2a_dfft* f, a2a_method m) {
     tc_operand_image(true, fmt, b1);
     if (f->d_tc) cudaFree(f->d_tc);
     f->d_tc = nullptr;
-    A2A_CUDA(cudaMalloc(&f->d_tc, tw_bytes + 2 * a2a::kTcBBytes), "cudaMalloc(tensor-core tables)");
+    const size_t bb = (size_t)a2a::tc_b_bytes(fmt);
+    A2A_CUDA(cudaMalloc(&f->d_tc, tw_bytes + 2 * bb), "cudaMalloc(tensor-core tables)");
     char* base = static_cast<char*>(f->d_tc);
     if (!tw.empty())
         A2A_CUDA(cudaMemcpy(base, tw.data(), tw.size() * sizeof(float), cudaMemcpyHostToDevice), "cudaMemcpy");
-    A2A_CUDA(cudaMemcpy(base + tw_bytes, b0.data(), a2a::kTcBBytes, cudaMemcpyHostToDevice), "cudaMemcpy");
-    A2A_CUDA(cudaMemcpy(base + tw_bytes + a2a::kTcBBytes, b1.data(), a2a::kTcBBytes, cudaMemcpyHostToDevice),
-             "cudaMemcpy");
+    A2A_CUDA(cudaMemcpy(base + tw_bytes, b0.data(), bb, cudaMemcpyHostToDevice), "cudaMemcpy");
+    A2A_CUDA(cudaMemcpy(base + tw_bytes + bb, b1.data(), bb, cudaMemcpyHostToDevice), "cudaMemcpy");
     for (int axis = 0; axis < 3; ++axis) f->tc_tw[axis] = base + twpos[axis] * sizeof(float2);
     f->tc_b[0] = base + tw_bytes;
-    f->tc_b[1] = base + tw_bytes + a2a::kTcBBytes;
+    f->tc_b[1] = base + tw_bytes + bb;
     return A2A_SUCCESS;
 }
 
@@ -1244,7 +1248,7 @@ a2a_status a2a_dfft_destroy(a2a_dfft* f) {
     return A2A_SUCCESS;
 }
 
-// ---- dump files (a2adistribution.cpp:142-151, tests/test.cpp:69-125) ----
+// ---- dump files (a2adistribution.cpp:101-111, tests/test.cpp:69-125) ----
 
 static a2a_status host_decomp(int ng, int P, int dims[3], int local[3], long long* nlocal) {
     if (ng < 1 || P < 1) return fail(A2A_ERROR_INVALID_VALUE, "ng and world_size must be >= 1");

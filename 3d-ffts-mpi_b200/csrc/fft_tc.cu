@@ -24,7 +24,7 @@ template <int N, int MODE, bool INV, int FMT> PassKernel make_tc_kernel() {
     k.lines = B;
     k.min_blocks = 1;
     k.lpt = 1;
-    k.smem = tc_smem_bytes<P, B, MODE>();
+    k.smem = tc_smem_bytes<P, B, MODE, FMT>();
     k.nstages = P::S;
     for (int s = 0; s < P::S; ++s) k.radix[s] = P::r[s];
     k.twtotal = P::twtotal();

@@ -6,22 +6,24 @@
 // One radix-16 butterfly is y = F16 x with F16 the 16-point DFT matrix.  As a
 // real GEMM row: [y_re | y_im] = [x_re | x_im] R with the 32 x 32 matrix
 //   R = [[C, S], [-S, C]],  C = cos(2 pi r k / 16),  S = -+ sin(2 pi r k / 16).
-// Operands are split into a high and a low 16-bit part (fp16 or bf16):
-// x = xh + xl after scaling each row by a power of two into [-1, 1),
-// R = Rh + Rl (generated in FP64 on the host), and the product keeps the
-// three significant terms  xh Rh + xh Rl + xl Rh  (xl Rl is below FP32
-// rounding).  The A operand of a 128-row block, [xh | xl] (K = 64), lives in
-// tensor memory: each thread writes its row into its own lane with one
-// tcgen05.st (two 16-bit values per 32-bit column), so A never passes through
-// shared memory; B = [Rh | Rl] is in shared memory (K-major, no swizzle).  Six
-// K = 16 MMAs accumulate, into one block of 32 FP32 columns of tensor memory,
-// first the corrections xh Rl + xl Rh (2^-11 smaller) and then the main term
-// xh Rh; each warp reads its 32 rows back with tcgen05.ld.  (Two accumulators
-// added in FP32 afterwards give a slightly smaller error -- 3.8e-7 instead of
-// 4.4e-7 relative L2 for a 512^3 transform -- but take 96 instead of 64
-// columns per block, which halves the CTAs an SM's tensor memory holds.)
-// A row is one butterfly: the thread that built row m reads row m back,
-// undoes its scale and stores the 16 outputs.
+// Both operands are split into 16-bit parts after scaling each row by a power
+// of two into [-1, 1); R is split on the host from FP64 values.
+//   fp16 (11-bit significands): x = xh + xl, R = Rh + Rl, and the product
+//     keeps xh Rh + xh Rl + xl Rh (xl Rl is below FP32 rounding): 22 bits.
+//   bf16 (8-bit significands): two parts carry only 16 bits, which leaves a
+//     relative error near 7e-6 on a 512^3 transform, so bf16 uses three parts
+//     x = xh + xm + xl, R = Rh + Rm + Rl and keeps every product down to
+//     2^-16 of the main term -- xh Rh, xh Rm + xm Rh, xh Rl + xm Rm + xl Rh
+//     (the dropped xm Rl, xl Rm, xl Rl are at or below FP32 rounding): 24 bits.
+// The A operand of a 128-row block (16 columns per part: the row's 16 real
+// then 16 imaginary values, two 16-bit values per 32-bit column) lives in
+// tensor memory: each thread writes its row into its own lane with
+// tcgen05.st, so A never passes through shared memory; B = [Rh | (Rm) | Rl]
+// is in shared memory (K-major, no swizzle).  The K = 16 MMAs (2 per kept
+// term: real and imaginary halves of K) accumulate into one block of 32 FP32
+// columns, smallest terms first; each warp reads its 32 rows back with
+// tcgen05.ld.  A row is one butterfly: the thread that built row m reads row
+// m back, undoes its scale and stores the 16 outputs.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -33,13 +35,17 @@ namespace a2a {
 
 enum TcFormat : int { TC_FP16 = 0, TC_BF16 = 1 };
 
+// 16-bit parts each operand is split into.
+__host__ __device__ constexpr int tc_parts(int fmt) { return fmt == TC_BF16 ? 3 : 2; }
+
 // Shared-memory layout of the B operand (UMMA canonical K-major,
 // SWIZZLE_NONE): an 8-row x 16-byte core matrix is 128 contiguous bytes; core
 // matrices step by SBO = 128 bytes along N and by LBO bytes along K.
 constexpr int kTcRows = 128;                     // M of one MMA block
 constexpr int kTcChunkB = 32 / 8 * 128;          // bytes of one K chunk of B (N = 32): 512
 constexpr int kTcMatB = 4 * kTcChunkB;           // one 32 x 32 matrix: 2 KB
-constexpr int kTcBBytes = 2 * kTcMatB;           // Rh and Rl
+__host__ __device__ constexpr int tc_b_bytes(int fmt) { return tc_parts(fmt) * kTcMatB; }
+constexpr int kTcBBytesMax = 3 * kTcMatB;        // room for the largest split
 
 __host__ __device__ constexpr uint64_t umma_smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
     return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
@@ -51,23 +57,29 @@ __host__ __device__ constexpr uint32_t umma_idesc_f16(int fmt) {
     return (1u << 4) | ((uint32_t)fmt << 7) | ((uint32_t)fmt << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
 }
 
-template <int FMT> __device__ __forceinline__ void split16(float v, uint16_t& hi, uint16_t& lo) {
-    if constexpr (FMT == TC_FP16) {
-        const __half h = __float2half_rn(v);
-        hi = __half_as_ushort(h);
-        lo = __half_as_ushort(__float2half_rn(v - __half2float(h)));
-    } else {
-        const __nv_bfloat16 h = __float2bfloat16_rn(v);
-        hi = __bfloat16_as_ushort(h);
-        lo = __bfloat16_as_ushort(__float2bfloat16_rn(v - __bfloat162float(h)));
+// v = p[0] + p[1] (+ p[2]) in 16-bit parts, each the rounding of what the
+// previous parts leave.
+template <int FMT> __device__ __forceinline__ void split16(float v, uint16_t (&p)[tc_parts(FMT)]) {
+#pragma unroll
+    for (int i = 0; i < tc_parts(FMT); ++i) {
+        if constexpr (FMT == TC_FP16) {
+            const __half h = __float2half_rn(v);
+            p[i] = __half_as_ushort(h);
+            v -= __half2float(h);
+        } else {
+            const __nv_bfloat16 h = __float2bfloat16_rn(v);
+            p[i] = __bfloat16_as_ushort(h);
+            v -= __bfloat162float(h);
+        }
     }
 }
 
 struct TcCtx {
-    uint32_t b_addr;           // shared address of [Rh | Rl]
-    uint32_t tmem;             // accumulator base (lane 0, column 0)
+    uint32_t b_addr;           // shared address of [Rh | (Rm) | Rl]
+    uint32_t tmem;             // tensor-memory base (lane 0, column 0)
     unsigned long long* bar;   // MMA completion
     uint32_t phase;
+    bool drained;              // after an abandoned stage: its MMAs did finish
 };
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
@@ -101,6 +113,12 @@ __device__ __forceinline__ void tc_st32(uint32_t taddr, const uint32_t (&r)[32])
         "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]), "r"(r[16]), "r"(r[17]), "r"(r[18]), "r"(r[19]), "r"(r[20]), "r"(r[21]), "r"(r[22]), "r"(r[23]), "r"(r[24]), "r"(r[25]), "r"(r[26]), "r"(r[27]), "r"(r[28]), "r"(r[29]), "r"(r[30]), "r"(r[31])
         : "memory");
 }
+__device__ __forceinline__ void tc_st16(uint32_t taddr, const uint32_t* r) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};\n" ::"r"(taddr),
+        "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+        : "memory");
+}
 __device__ __forceinline__ void tc_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory"); }
 // D = A B (+ D) with A in tensor memory (K-major, 16-bit values two to a
 // 32-bit column) and B in shared memory; no output lanes disabled.
@@ -113,10 +131,11 @@ __device__ __forceinline__ void tc_mma_ts(uint32_t dtmem, uint32_t atmem, uint64
         : "memory");
 }
 
-// Tensor-memory columns of one 128-row block: the A operand (32 columns: hi
-// re, hi im, lo re, lo im, 8 each), then the 32-column accumulator.
-constexpr int kTcBlockCols = 64;
-constexpr int kTcAccCol = 32;
+// Tensor-memory columns of one 128-row block: the A operand (16 columns per
+// part: real values in 0-7, imaginary in 8-15), then the 32-column
+// accumulator.  fp16: 64 columns; bf16: 80.
+__host__ __device__ constexpr int tc_acc_col(int fmt) { return 16 * tc_parts(fmt); }
+__host__ __device__ constexpr int tc_block_cols(int fmt) { return tc_acc_col(fmt) + 32; }
 
 // Row swizzle of a batch-mode tile (the pass kernels' rule): the first
 // stage's stride-R0 row writes of 8-line rows would otherwise meet 2-4-way
@@ -126,9 +145,13 @@ template <class PLAN, int B, int MODE> __host__ __device__ constexpr int tc_tile
 }
 
 // One radix-16 stage on the tensor cores.  THREADS == butterflies per stage;
-// thread q owns butterfly q, i.e. A row q % 128 of block q / 128.
+// thread q owns butterfly q, i.e. A row q % 128 of block q / 128.  Returns
+// false when the MMA completion wait gave up (the device error flag is then
+// set, the rest of the pass is skipped, and ctx.drained says whether the
+// stage's MMAs were seen to finish by a second bounded wait, i.e. whether the
+// tensor memory may be freed).
 template <class PLAN, int B, int THREADS, int MODE, bool INV, int FMT, int s, bool SRC_GLOBAL>
-__device__ __forceinline__ void tc_stage(const PassArgs<float>& a, float2* tile, const float2* tw,
+__device__ __forceinline__ bool tc_stage(const PassArgs<float>& a, float2* tile, const float2* tw,
                                          const uint32_t* offA_s, const size_t* base_s, TcCtx& ctx, int tid,
                                          size_t ubase, int v0) {
     using G = TileGeom<MODE, B, PLAN::N, sizeof(float2), tc_tile_swizzle<PLAN, B, MODE>()>;
@@ -143,6 +166,9 @@ __device__ __forceinline__ void tc_stage(const PassArgs<float>& a, float2* tile,
     constexpr bool LAST = (s == PLAN::S - 1);
     constexpr bool BFAST = (MODE == MODE_BATCH) || !(LAST || SRC_GLOBAL);
     constexpr int TWO = PLAN::twoff(s);
+    constexpr int NP = tc_parts(FMT);
+    constexpr int BCOLS = tc_block_cols(FMT);
+    constexpr int ACC = tc_acc_col(FMT);
 
     int b, j;
     bf_map<BFAST, B, NBL>(tid, b, j);
@@ -169,25 +195,32 @@ __device__ __forceinline__ void tc_stage(const PassArgs<float>& a, float2* tile,
     e = mx > 0.f ? min(max(e, -125), 126) : 0;
     const float down = __int_as_float((127 - e) << 23);  // 2^-e
     const float up = __int_as_float((127 + e) << 23);    // 2^e
+    const int warp = tid / 32;
+    const uint32_t lane_row = ((uint32_t)((warp % 4) * 32) << 16) + (uint32_t)((warp / 4) * BCOLS);
     {
-        // the row into this warp's lanes of its block's A columns: 0-7 hi re,
-        // 8-15 hi im, 16-23 lo re, 24-31 lo im, values k and k+1 in the low
-        // and high half of column k/2
-        uint32_t w[32];
+        // the row into this warp's lanes of its block's A columns: part q at
+        // columns 16q..16q+15 (real values k, k+1 in the low and high half of
+        // column 16q + k/2, imaginary ones in 16q + 8 + k/2)
+        uint32_t w[16 * NP];
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
-            uint16_t h0, l0, h1, l1;
-            split16<FMT>(x[2 * i].x * down, h0, l0);
-            split16<FMT>(x[2 * i + 1].x * down, h1, l1);
-            w[i] = h0 | (uint32_t(h1) << 16);
-            w[16 + i] = l0 | (uint32_t(l1) << 16);
-            split16<FMT>(x[2 * i].y * down, h0, l0);
-            split16<FMT>(x[2 * i + 1].y * down, h1, l1);
-            w[8 + i] = h0 | (uint32_t(h1) << 16);
-            w[24 + i] = l0 | (uint32_t(l1) << 16);
+            uint16_t r0[NP], r1[NP], i0[NP], i1[NP];
+            split16<FMT>(x[2 * i].x * down, r0);
+            split16<FMT>(x[2 * i + 1].x * down, r1);
+            split16<FMT>(x[2 * i].y * down, i0);
+            split16<FMT>(x[2 * i + 1].y * down, i1);
+#pragma unroll
+            for (int q = 0; q < NP; ++q) {
+                w[16 * q + i] = r0[q] | (uint32_t(r1[q]) << 16);
+                w[16 * q + 8 + i] = i0[q] | (uint32_t(i1[q]) << 16);
+            }
         }
-        const int warp = tid / 32;
-        tc_st32(ctx.tmem + ((uint32_t)((warp % 4) * 32) << 16) + (uint32_t)((warp / 4) * kTcBlockCols), w);
+        if constexpr (NP == 2) {
+            tc_st32(ctx.tmem + lane_row, reinterpret_cast<const uint32_t(&)[32]>(w));
+        } else {
+            tc_st32(ctx.tmem + lane_row, reinterpret_cast<const uint32_t(&)[32]>(w));
+            tc_st16(ctx.tmem + lane_row + 32, w + 32);
+        }
         tc_wait_st();
         tc_fence_before();
         __syncthreads();  // all A rows stored; all tile reads of this stage done
@@ -195,36 +228,48 @@ __device__ __forceinline__ void tc_stage(const PassArgs<float>& a, float2* tile,
     if (tid == 0) {
         tc_fence_after();
         const uint32_t idesc = umma_idesc_f16(FMT);
+        // B parts: R part q at b_addr + q kTcMatB; the real half of K first
+        auto bre = [&](int q) { return umma_smem_desc(ctx.b_addr + q * kTcMatB, kTcChunkB, 128); };
+        auto bim = [&](int q) { return umma_smem_desc(ctx.b_addr + q * kTcMatB + 2 * kTcChunkB, kTcChunkB, 128); };
 #pragma unroll
         for (int blk = 0; blk < NBLK; ++blk) {
-            // one accumulator per block: the corrections xh Rl + xl Rh
-            // (2^-11 smaller) first, then the main term xh Rh
-            const uint32_t ab = ctx.tmem + blk * kTcBlockCols;  // lane 0 of the block's A columns
-            const uint32_t dacc = ab + kTcAccCol;
-            const uint64_t rh_re = umma_smem_desc(ctx.b_addr + 0 * kTcChunkB, kTcChunkB, 128);
-            const uint64_t rh_im = umma_smem_desc(ctx.b_addr + 2 * kTcChunkB, kTcChunkB, 128);
-            const uint64_t rl_re = umma_smem_desc(ctx.b_addr + kTcMatB + 0 * kTcChunkB, kTcChunkB, 128);
-            const uint64_t rl_im = umma_smem_desc(ctx.b_addr + kTcMatB + 2 * kTcChunkB, kTcChunkB, 128);
-            tc_mma_ts(dacc, ab + 0, rl_re, idesc, 0);
-            tc_mma_ts(dacc, ab + 8, rl_im, idesc, 1);
-            tc_mma_ts(dacc, ab + 16, rh_re, idesc, 1);
-            tc_mma_ts(dacc, ab + 24, rh_im, idesc, 1);
-            tc_mma_ts(dacc, ab + 0, rh_re, idesc, 1);
-            tc_mma_ts(dacc, ab + 8, rh_im, idesc, 1);
+            const uint32_t ab = ctx.tmem + blk * BCOLS;  // lane 0 of the block's A columns
+            const uint32_t dacc = ab + ACC;
+            // one term x_p R_q: the real and the imaginary half of K
+            auto term = [&](int pa, int qb, uint32_t acc) {
+                tc_mma_ts(dacc, ab + 16 * pa, bre(qb), idesc, acc);
+                tc_mma_ts(dacc, ab + 16 * pa + 8, bim(qb), idesc, 1);
+            };
+            if constexpr (NP == 2) {
+                // corrections xh Rl + xl Rh (2^-11 smaller), then xh Rh
+                term(0, 1, 0);
+                term(1, 0, 1);
+                term(0, 0, 1);
+            } else {
+                // 2^-16 terms, 2^-8 terms, then xh Rh
+                term(0, 2, 0);
+                term(1, 1, 1);
+                term(2, 0, 1);
+                term(0, 1, 1);
+                term(1, 0, 1);
+                term(0, 0, 1);
+            }
         }
         tc_commit(ctx.bar);
     }
     const bool ok = mbar_wait_bounded(ctx.bar, ctx.phase);
+    if (__syncthreads_or(!ok)) {
+        // the MMAs did not complete in time: flag it, skip the rest of the
+        // pass, and look once more (bounded) for their completion before the
+        // caller may free the tensor memory they write
+        if ((tid % 32) == 0) atomicExch(a.err, 1);
+        ctx.drained = __syncthreads_and(mbar_wait_bounded(ctx.bar, ctx.phase)) != 0;
+        return false;
+    }
     ctx.phase ^= 1u;
     tc_fence_after();
     float y[32];
-    {
-        const int warp = tid / 32;
-        const uint32_t taddr = ctx.tmem + ((uint32_t)((warp % 4) * 32) << 16) +
-                               (uint32_t)((warp / 4) * kTcBlockCols + kTcAccCol);
-        tc_ld32(taddr, y);
-    }
-    if (!ok && (tid % 32) == 0) atomicExch(a.err, 1);
+    tc_ld32(ctx.tmem + lane_row + ACC, y);
 #pragma unroll
     for (int k = 0; k < 16; ++k) x[k] = make_float2(y[k] * up, y[16 + k] * up);
     if constexpr (LAST) {
@@ -239,15 +284,17 @@ __device__ __forceinline__ void tc_stage(const PassArgs<float>& a, float2* tile,
     tc_fence_before();
     __syncthreads();  // tile written; accumulators read before the next stage's MMAs
     if constexpr (!LAST)
-        tc_stage<PLAN, B, THREADS, MODE, INV, FMT, s + 1, false>(a, tile, tw, offA_s, base_s, ctx, tid, ubase, v0);
+        return tc_stage<PLAN, B, THREADS, MODE, INV, FMT, s + 1, false>(a, tile, tw, offA_s, base_s, ctx, tid, ubase,
+                                                                        v0);
+    return true;
 }
 
-template <class PLAN, int B, int MODE>
+template <class PLAN, int B, int MODE, int FMT>
 __host__ __device__ constexpr size_t tc_smem_bytes() {
     constexpr int N = PLAN::N;
     size_t bytes = sizeof(float2) * (size_t)TileGeom<MODE, B, N, sizeof(float2)>::elems;
     bytes = (bytes + 127) & ~size_t(127);
-    bytes += kTcBBytes;
+    bytes += tc_b_bytes(FMT);
     bytes += sizeof(float2) * (size_t)PLAN::twtotal();
     bytes += sizeof(uint32_t) * (size_t)N;
     bytes = (bytes + 15) & ~size_t(15);
@@ -256,16 +303,25 @@ __host__ __device__ constexpr size_t tc_smem_bytes() {
 }
 
 // One CTA = one tile of B lines, THREADS = B N / 16.  Tensor memory:
-// kTcBlockCols columns per 128-row block (rounded up to a power of two),
-// allocated and freed by warp 0.
+// tc_block_cols(FMT) columns per 128-row block (the total rounded up to a
+// power of two), allocated and freed by warp 0.
+// Tensor-memory columns one CTA allocates (a power of two >= 32), and the
+// CTAs per SM that many columns allow (at most 4).
+template <class PLAN, int B, int FMT> __host__ __device__ constexpr int tc_tcols() {
+    constexpr int NEED = (B * PLAN::N / 16 / kTcRows) * tc_block_cols(FMT);
+    return NEED <= 32 ? 32 : NEED <= 64 ? 64 : NEED <= 128 ? 128 : NEED <= 256 ? 256 : 512;
+}
+template <class PLAN, int B, int FMT> __host__ __device__ constexpr int tc_min_blocks() {
+    return 512 / tc_tcols<PLAN, B, FMT>() < 4 ? 512 / tc_tcols<PLAN, B, FMT>() : 4;
+}
+
 template <class PLAN, int B, int MODE, bool INV, int FMT>
-__global__ void __launch_bounds__(B * PLAN::N / 16, 4) fft_tc_kernel(const PassArgs<float> a) {
+__global__ void __launch_bounds__(B * PLAN::N / 16, (tc_min_blocks<PLAN, B, FMT>())) fft_tc_kernel(const PassArgs<float> a) {
     constexpr int N = PLAN::N;
     constexpr int THREADS = B * N / 16;
     constexpr int NBLK = THREADS / kTcRows;
-    constexpr int NEED = NBLK * kTcBlockCols;
-    static_assert(NEED <= 512, "tensor memory holds 512 columns");
-    constexpr uint32_t TCOLS = NEED <= 32 ? 32 : NEED <= 64 ? 64 : NEED <= 128 ? 128 : NEED <= 256 ? 256 : 512;
+    static_assert(NBLK * tc_block_cols(FMT) <= 512, "tensor memory holds 512 columns");
+    constexpr uint32_t TCOLS = tc_tcols<PLAN, B, FMT>();
     using G = TileGeom<MODE, B, N, sizeof(float2), tc_tile_swizzle<PLAN, B, MODE>()>;
     constexpr int TWN = PLAN::twtotal();
     constexpr int R0 = PLAN::r[0];
@@ -274,7 +330,7 @@ __global__ void __launch_bounds__(B * PLAN::N / 16, 4) fft_tc_kernel(const PassA
     float2* tile = reinterpret_cast<float2*>(smem_raw);
     size_t off = (sizeof(float2) * (size_t)G::elems + 127) & ~size_t(127);
     unsigned char* bmat = smem_raw + off;
-    off += kTcBBytes;
+    off += tc_b_bytes(FMT);
     float2* tw = reinterpret_cast<float2*>(smem_raw + off);
     off += sizeof(float2) * (size_t)TWN;
     uint32_t* offA_s = reinterpret_cast<uint32_t*>(smem_raw + off);
@@ -303,7 +359,7 @@ __global__ void __launch_bounds__(B * PLAN::N / 16, 4) fft_tc_kernel(const PassA
     {
         const uint4* src = reinterpret_cast<const uint4*>(a.tcb);
         uint4* dst = reinterpret_cast<uint4*>(bmat);
-        for (int i = tid; i < kTcBBytes / 16; i += THREADS) dst[i] = src[i];
+        for (int i = tid; i < tc_b_bytes(FMT) / 16; i += THREADS) dst[i] = src[i];
     }
     for (int i = tid; i < TWN; i += THREADS) tw[i] = a.tw[i];
     for (int i = tid; i < N; i += THREADS) offA_s[i] = a.offA[i];
@@ -318,9 +374,11 @@ __global__ void __launch_bounds__(B * PLAN::N / 16, 4) fft_tc_kernel(const PassA
     ctx.tmem = *tmem_slot;
     ctx.bar = bar;
     ctx.phase = 0;
+    ctx.drained = true;
 
+    bool ok;
     if constexpr (R0 == 16) {
-        tc_stage<PLAN, B, THREADS, MODE, INV, FMT, 0, true>(a, tile, tw, offA_s, base_s, ctx, tid, ubase, v0);
+        ok = tc_stage<PLAN, B, THREADS, MODE, INV, FMT, 0, true>(a, tile, tw, offA_s, base_s, ctx, tid, ubase, v0);
     } else {
         // stage 0 on the CUDA cores: global -> registers -> shared
         constexpr int NBL = N / R0;
@@ -352,9 +410,13 @@ __global__ void __launch_bounds__(B * PLAN::N / 16, 4) fft_tc_kernel(const PassA
             }
         }
         __syncthreads();
-        tc_stage<PLAN, B, THREADS, MODE, INV, FMT, 1, false>(a, tile, tw, offA_s, base_s, ctx, tid, ubase, v0);
+        ok = tc_stage<PLAN, B, THREADS, MODE, INV, FMT, 1, false>(a, tile, tw, offA_s, base_s, ctx, tid, ubase, v0);
     }
-    // every stage ends with tcgen05.wait::ld and a block barrier
+    // every stage ends with tcgen05.wait::ld and a block barrier.  After an
+    // abandoned stage whose MMAs were never seen to finish, the columns stay
+    // allocated (freeing them under running MMAs would hand them to another
+    // CTA while they are written); the error flag is already set.
+    if (!ok && !ctx.drained) return;
     tc_fence_after();
     if (tid < 32)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(ctx.tmem), "r"(TCOLS)

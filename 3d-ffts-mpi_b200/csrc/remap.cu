@@ -6,7 +6,7 @@ namespace a2a {
 
 // ---------------------------------------------------------------------------
 // alltoall over virtual ranks: dst[q][r][i] = src[r][q][i], i < chunk
-// (MPI_Alltoall with nsends = nlocal / P, a2adistribution.cpp:158-165).
+// (MPI_Alltoall with nsends = nlocal / P, a2adistribution.cpp:117-125).
 // U is the copy unit (16-byte vectors whenever the chunk allows).
 // ---------------------------------------------------------------------------
 template <typename U>

@@ -2,7 +2,7 @@
 // rank-major chunk permutation, the pack/unpack pencil remaps and the
 // fast-axis changes.  They reproduce, element for element, what the reference
 // leaves in both buffers after each of its six steps
-// (src/a2afft/distribution/a2adistribution.cpp:156-256).
+// (src/a2afft/distribution/a2adistribution.cpp:115-215).
 #pragma once
 
 #include <cstdint>

@@ -4,7 +4,7 @@ group, one process per GPU, each holding a contiguous block of
 ``L = P / G`` ranks (``[g L, (g+1) L)``).
 
 The reference runs one MPI rank per GPU and exchanges with ``MPI_Alltoall``
-(``src/a2afft/distribution/a2adistribution.cpp:156-256``), either staged
+(``src/a2afft/distribution/a2adistribution.cpp:115-215``), either staged
 through host memory (its default, ``:160-163``) or on device buffers with
 CUDA-aware MPI (``-Dcudampi``, ``:164-166``).  Here the alltoall over the P
 virtual ranks is one ``all_to_all_single`` between the G processes (NCCL over
@@ -92,7 +92,7 @@ class DistributedDistribution:
             tdist.all_to_all_single(back, out, group=self.group)
         recv.view(L, G, L, C).copy_(back.permute(2, 0, 1, 3))  # [dest rank][source proc][sender][chunk]
 
-    # -- the six steps (a2adistribution.cpp:156-256) -------------------------
+    # -- the six steps (a2adistribution.cpp:115-215) -------------------------
     def getZPencils(self, b1, b2):
         self.alltoall(b1, b2)
         self.local.launch("d_z_a2a_to_z_pencils", b2, b1)
@@ -148,7 +148,7 @@ class DistributedDfft:
         if inverse:
             loc.scale(s, d_data)  # a2adfft.cpp:147
         else:
-            loc.copy(s, d_data)  # a2adfft.cpp:108
+            loc.copy(s, d_data)  # a2adfft.cpp:79
         d.returnYPencils(d_data, s)
 
     def forward(self, d_data) -> None:
@@ -187,18 +187,41 @@ class FusedDistributedDfft:
         self.blocks = None
         self._imported = []
 
+    def _check_block(self, d_data):
+        """Why ``d_data`` cannot serve as this process's block ('' if it can):
+        the fused kernels of every process index it as ``block_elems``
+        elements of the distribution's own element type, so a buffer of the
+        wrong type, shape or length would let peer loads and stores run past
+        its allocation."""
+        import torch
+
+        want = self.dist.dtype
+        if not isinstance(d_data, torch.Tensor) or not d_data.is_cuda:
+            return "the block must be a CUDA tensor"
+        if d_data.dtype != want:
+            return f"the block must be {want} for this distribution, not {d_data.dtype}"
+        if not d_data.is_contiguous():
+            return "the block must be contiguous"
+        if d_data.numel() * d_data.element_size() < self.block_elems * self.dist.element_bytes:
+            return f"the block needs {self.block_elems} elements, it has {d_data.numel()}"
+        return ""
+
     def bind(self, d_data) -> None:
-        """Exchange buffer handles with every process (collective)."""
+        """Exchange buffer handles with every process (collective).  Every
+        process checks its own block first and all of them raise if any
+        block is unusable, so no process maps a bad buffer or waits alone."""
         import torch.distributed as tdist
 
-        if d_data.numel() < self.block_elems:
-            raise ValueError(f"this process's buffer needs {self.block_elems} elements")
-        mine = ipc_export(d_data)
+        why = self._check_block(d_data)
+        mine = (why, None if why else ipc_export(d_data))
         allh = [None] * self.G
         tdist.all_gather_object(allh, mine, group=self.group)
+        bad = [(q, w) for q, (w, _) in enumerate(allh) if w]
+        if bad:
+            raise ValueError("; ".join(f"process {q}: {w}" for q, w in bad))
         self.release()
         blocks = []
-        for q, (h, off) in enumerate(allh):
+        for q, (_, (h, off)) in enumerate(allh):
             if q == self.g:
                 blocks.append(d_data.data_ptr())
             else:

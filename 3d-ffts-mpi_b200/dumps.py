@@ -2,7 +2,7 @@
 runs against this library's output.
 
 The reference writes a ``dims`` file (nine int32: world_size, Ng, nlocal,
-dims[3], local_grid_size[3]; ``src/a2afft/distribution/a2adistribution.cpp:142-151``)
+dims[3], local_grid_size[3]; ``src/a2afft/distribution/a2adistribution.cpp:101-111``)
 and one ``proc<r>`` file per rank holding that rank's brick of the input, the
 forward result and the inverse result (``src/a2afft/tests/test.cpp:69-125``).
 Its checker reassembles the bricks with ``rank2coords`` and asserts

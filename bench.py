@@ -9,21 +9,27 @@ place.  The 1 GiB buffer is larger than the 126 MB L2, so no flush is needed
 between steps.
 
 Printed (rank 0, one JSON line):
-  value         ms per forward+inverse, device-resident data, CUDA events on the
-                launching stream (max over ranks; with N ranks, N independent
-                replicas run and value = max time / N)
-  e2e           the same through the public API with pinned HOST buffers: the
-                H2D copy of the input and the D2H copy of the result are inside
-                every timed step
+  value         ms per forward+inverse of the plain FP32 method, device-resident
+                data, CUDA events on the launching stream (max over ranks; with
+                N ranks, N independent replicas run and value = max time / N)
+  methods       the same timing, per-pass times, roofline and accuracy for each
+                method on the same input: plain, split_fp16 and split_bf16 (the
+                split-precision tensor-core form), so the metric's comparison
+                is in one line
+  rel_l2_vs_fp64  per method: relative L2 error of the forward result against
+                the oracle's complex128 transform of the same input (the
+                reference's own check, np.fft.fftn, in FP64)
+  e2e           the plain method through the public API with pinned HOST
+                buffers: the H2D copy of the input and the D2H copy of the
+                result are inside every timed step
   roofline      the dominant pass kernel: algorithmic bytes (2 x Ng^3 x 8 B per
                 launch) / its mean CUDA-event duration, against the measured HBM
                 copy bandwidth
-  cpu_baseline  the reference's step sequence on the host cores (oracle port:
-                numpy remaps + scipy pocketfft), on a 256^3 sample scaled to
-                512^3 by N log N
+  cpu_baseline  the reference's host step sequence (the oracle port's
+                HostPipeline) on the full cube, on all host threads
 
-``--impl reference`` times only that CPU pipeline (rank 0) on the same
-workload and prints its line with "impl": "reference".
+``--impl reference`` times only that host pipeline (rank 0) on the full
+workload, every step, and prints its line with "impl": "reference".
 
 ``--workload batch`` measures the batched form instead: 96 complex64 cubes with
 edges drawn from 32 48 64 96 128 192 (seed 3) plus two 128x256x512 boxes, each
@@ -51,7 +57,8 @@ NG = 512
 RANKS = 64
 SEED = 2
 FALLBACK_HBM_GBS = 6650.0
-CPU_SAMPLE_NG = 256
+CPU_BASELINE_STEPS = 2  # full-size host pipeline pairs timed for cpu_baseline
+REF_BUDGET_S = 300.0  # timed seconds the reference arm may spend
 
 
 def parse_args():
@@ -60,7 +67,8 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--method", choices=["plain", "split_bf16", "split_fp16"], default="plain")
+    ap.add_argument("--method", choices=["all", "plain", "split_bf16", "split_fp16"], default="all",
+                    help="cube workload: all = plain, split_fp16, split_bf16 where the split form exists")
     ap.add_argument("--ng", type=int, default=NG)
     ap.add_argument("--ranks", type=int, default=RANKS)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
@@ -88,32 +96,40 @@ def workload_name(ng, ranks, dims, precision="c64", seed=SEED, tones=3):
     return f"{ng}^3 {cname} C2C forward+inverse, {ranks} virtual ranks (dims {dims}), {inp} seed {seed}"
 
 
-def cpu_pipeline_ms(ng_sample, ranks, ng_target, reps=1, precision="c64", seed=SEED, tones=3):
-    """The reference's host step sequence (oracle port) on one cube of
-    ng_sample^3, best of `reps`, scaled to ng_target^3 by N log N."""
-    import numpy as np
+def host_pipeline_ms(ng, ranks, steps, warmup, precision="c64", seed=SEED, tones=3, budget_s=None):
+    """The reference's host step sequence (the oracle port's HostPipeline:
+    19 passes per direction, every remap a multi-threaded strided copy, 1D
+    transforms torch.fft on the host) on the full ng^3 cube, all host
+    threads.  Times `steps` forward+inverse pairs after `warmup` untimed ones
+    (fewer if `budget_s` of timed work would be exceeded); returns
+    (mean ms, steps timed, threads, sample text)."""
+    import torch
 
     import __graft_entry__ as entry
 
     O = entry.load_oracle()
-    cores = os.cpu_count() or 1
-    cdt = np.complex128 if precision == "c128" else np.complex64
-    d = O.Decomp(ng_sample, ranks)
-    g = O.make_input("uniform", (ng_sample,) * 3, seed=seed, dtype=cdt, tones=tones)
-    b = O.global_to_bricks(g, d)
-    lines = O.scipy_lines(cores)
-    best = float("inf")
-    for _ in range(reps):
+    d = O.Decomp(ng, ranks)
+    hp = O.HostPipeline(d, precision)
+    real = torch.float64 if precision == "c128" else torch.float32
+    hp.b1.copy_(synth_bricks(torch, ng, d.dims, seed, "cpu", real, tones))
+    for _ in range(warmup):
+        hp.run(False)
+        hp.run(True)
+    times = []
+    t_start = time.perf_counter()
+    for i in range(steps):
         t0 = time.perf_counter()
-        f = O.forward(b, d, lines, cdt)
-        O.inverse(f, d, lines, cdt)
-        best = min(best, time.perf_counter() - t0)
-    n_s, n_t = float(ng_sample) ** 3, float(ng_target) ** 3
-    scale = (n_t * math.log2(n_t)) / (n_s * math.log2(n_s))
+        hp.run(False)
+        hp.run(True)
+        times.append((time.perf_counter() - t0) * 1e3)
+        if budget_s is not None and time.perf_counter() - t_start > budget_s:
+            break
     cname = "complex128" if precision == "c128" else "complex64"
-    sample = (f"one forward+inverse of a {ng_sample}^3 {cname} cube on {ranks} virtual ranks "
-              f"(dims {d.dims}), best of {reps}, x{scale:.3f} (N log N) to {ng_target}^3")
-    return best * 1e3 * scale, cores, sample, best
+    sample = (f"the full {ng}^3 {cname} cube on {ranks} virtual ranks (dims {d.dims}), {len(times)} timed "
+              f"forward+inverse pairs after {warmup} untimed; the reference's 19 passes per direction (alltoall, "
+              f"pack/unpack, fast-axis changes, 1D transforms, copy/scale), remaps as multi-threaded strided "
+              f"copies, 1D transforms torch.fft (pocketfft) on {hp.threads} threads")
+    return statistics.mean(times), len(times), hp.threads, sample
 
 
 class ClockSampler:
@@ -268,14 +284,20 @@ def profiled_traffic(kernel_key):
     return None
 
 
-def synth_bricks(torch, ng, dims, seed, device, real=None, tones=3):
-    """Seeded U[-1,1) re/im + `tones` pure tones of amplitude 100, generated
-    on the GPU, returned in the rank-major brick layout."""
+def synth_bricks(torch, ng, dims, seed, device, real=None, tones=3, kind="uniform"):
+    """Seeded synthetic cube in the rank-major brick layout, generated on
+    `device`: real and imaginary parts i.i.d. U[-1,1) (kind "uniform") or
+    N(0,1) (kind "normal"), plus `tones` pure tones of amplitude 100 at random
+    wave vectors."""
     real = real or torch.float32
     gen = torch.Generator(device=device).manual_seed(seed)
     shape = (ng, ng, ng)
-    re = torch.rand(shape, generator=gen, device=device, dtype=real) * 2 - 1
-    im = torch.rand(shape, generator=gen, device=device, dtype=real) * 2 - 1
+    if kind == "normal":
+        re = torch.randn(shape, generator=gen, device=device, dtype=real)
+        im = torch.randn(shape, generator=gen, device=device, dtype=real)
+    else:
+        re = torch.rand(shape, generator=gen, device=device, dtype=real) * 2 - 1
+        im = torch.rand(shape, generator=gen, device=device, dtype=real) * 2 - 1
     g = torch.complex(re, im)
     del re, im
     ks = torch.randint(0, ng, (tones, 3), generator=gen, device=device)
@@ -532,95 +554,67 @@ def run_reference(args, rank, world):
     if args.workload == "batch":
         run_batch_reference(args, rank, world)
         return
-    ng_target = args.ng
-    prec = args.precision
+    ng, prec = args.ng, args.precision
     seed, tones = cube_input(args)
-    # calibrate the sample size so the whole run stays within a few minutes
-    est_ms, cores, _, wall = cpu_pipeline_ms(128, args.ranks, ng_target, precision=prec, seed=seed, tones=tones)
-    sample_ng = CPU_SAMPLE_NG if wall * 8.5 * (args.steps + args.warmup) < 240 else 128
-    times = []
-    for i in range(args.warmup + args.steps):
-        ms, cores, sample, _ = cpu_pipeline_ms(sample_ng, args.ranks, ng_target, precision=prec, seed=seed,
-                                               tones=tones)
-        if i >= args.warmup:
-            times.append(ms)
-    value = statistics.mean(times)
+    # the full workload every step; a timed budget keeps an oversized
+    # --steps request within a few minutes (the line reports what was timed)
+    value, steps, cores, sample = host_pipeline_ms(ng, args.ranks, args.steps, args.warmup, precision=prec,
+                                                   seed=seed, tones=tones, budget_s=REF_BUDGET_S)
     import __graft_entry__ as entry
 
     dims = entry.load_oracle().dims_create(args.ranks, 3)
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "ms", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(value, 3), "higher_is_better": False,
+        "steps": steps, "warmup": args.warmup, "ms_per_step": round(value, 3), "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == "c128" else "f32", "data": "synthetic",
-        "config": {"workload": workload_name(ng_target, args.ranks, dims, prec, seed, tones), "ng": ng_target,
-                   "world_size": args.ranks, "precision": prec, "sample_ng": sample_ng},
-        "cpu_baseline": {"value": round(value, 3), "unit": "ms", "cores": cores, "kind": "port",
-                         "sample": sample + "; remaps single-threaded numpy, 1D transforms scipy.fft workers=cores"},
+        "config": {"workload": workload_name(ng, args.ranks, dims, prec, seed, tones), "ng": ng,
+                   "world_size": args.ranks, "dims": dims, "precision": prec, "method": "host pipeline"},
+        "cpu_baseline": {"value": round(value, 3), "unit": "ms", "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": round(value, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
-def run_ours(args, rank, world, local_rank):
-    import torch
+TC_LENGTHS = (64, 128, 256, 512, 1024)
 
-    import __graft_entry__ as entry
 
-    pkg = entry.load_package()
-    torch.cuda.set_device(local_rank)
-    dev = torch.device("cuda", local_rank)
-    ng, ranks = args.ng, args.ranks
-    prec = args.precision
-    seed, tones = cube_input(args)
-    esz = 16 if prec == "c128" else 8
-    dist = pkg.a2aDistribution(ranks, ng, 64, precision=prec)
-    dfft = pkg.a2adfft(dist, method=args.method)
+def cube_methods(args):
+    """Methods timed on the cube workload: all three where the split
+    tensor-core form exists (complex64, radix-16 lengths), else plain."""
+    if args.method != "all":
+        return [args.method]
+    if args.precision == "c64" and args.ng in TC_LENGTHS:
+        return ["plain", "split_fp16", "split_bf16"]
+    return ["plain"]
+
+
+PASS_NAMES = ["Z_fwd", "X_fwd", "Y_fwd", "Z_inv", "X_inv", "Y_inv"]
+
+
+def time_method(pkg, torch, dist, method, x, stream, args, local_rank, world):
+    """Plans (make_plans timing every launch variant on a scratch buffer, or
+    the --variants choice), warms up, then times K forward+inverse steps on
+    `x` with an event between every pass launch.  Returns the plan object,
+    the step time (max over ranks), the per-pass means and the clocks."""
+    dfft = pkg.a2adfft(dist, method=method)
     if args.variants:
         dfft.make_plans()
         for p, v in enumerate(int(t) for t in args.variants.split(",")):
             dfft.select_variant(p, v)
     else:
-        scratch = dist.empty(dev)  # make_plans times the pass variants on it
+        scratch = dist.empty(x.device)  # make_plans times the pass variants on it
         dfft.make_plans(scratch)
         del scratch
-    plan_report = dfft.plan_report()
-    x = synth_bricks(torch, ng, dist.dims, seed, dev, torch.float64 if prec == "c128" else torch.float32, tones)
-    x0 = x.clone()
-    stream = torch.cuda.Stream(device=dev)
-    nbytes_buf = x.numel() * x.element_size()
-
-    def step():
-        for inv in (0, 1):
-            for p in range(3):
-                dfft.execute_pass(x, p, inv, stream)
+        torch.cuda.empty_cache()
 
     torch.cuda.synchronize()
     with torch.cuda.stream(stream):
         for _ in range(max(args.warmup, 3)):
-            step()
+            for inv in (0, 1):
+                for p in range(3):
+                    dfft.execute_pass(x, p, inv, stream)
     torch.cuda.synchronize()
 
-    # accuracy (outside the timed region): forward vs our FP64 path, round trip
-    rel_err = None
-    rt_err = None
-    if (world == 1 or rank == 0) and not args.no_check:
-        x.copy_(x0)
-        dfft.forward(x)
-        if prec == "c64":  # against our complex128 transform of the same input
-            d64 = pkg.a2aDistribution(ranks, ng, 64, precision="c128")
-            f64 = pkg.a2adfft(d64)
-            f64.make_plans()
-            y = x0.to(torch.complex128)
-            f64.forward(y)
-            rel_err = float(torch.linalg.vector_norm(x.to(torch.complex128) - y) / torch.linalg.vector_norm(y))
-            del y, f64, d64
-        dfft.inverse(x)
-        rt_err = float(torch.linalg.vector_norm((x - x0).to(torch.complex128)) /
-                       torch.linalg.vector_norm(x0.to(torch.complex128)))
-        torch.cuda.empty_cache()
-    x.copy_(x0)
-
-    # timed region: K steps, an event between every pass launch
     evs = [torch.cuda.Event(enable_timing=True) for _ in range(6 * args.steps + 1)]
     if world > 1:
         torch.distributed.barrier()
@@ -638,19 +632,60 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
-    total_ms = evs[0].elapsed_time(evs[-1])
+    dfft.check_device()
     per_pass = [[] for _ in range(6)]
     for i in range(6 * args.steps):
         per_pass[i % 6].append(evs[i].elapsed_time(evs[i + 1]))
-    step_ms = total_ms / args.steps
+    step_ms = evs[0].elapsed_time(evs[-1]) / args.steps
     if world > 1:
-        t = torch.tensor([step_ms], device=dev)
+        t = torch.tensor([step_ms], device=x.device)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         step_ms = float(t.item())
+    return dfft, step_ms, [statistics.mean(v) for v in per_pass], clk.summary()
 
-    # e2e through the public API with pinned host buffers
+
+def method_roofline(means, ng, esz, prec, peak, peak_kind, method):
+    dom = max(range(6), key=lambda i: means[i])
+    alg_bytes = 2.0 * float(ng) ** 3 * esz  # one read + one write of the cube per pass
+    achieved = alg_bytes / (means[dom] * 1e-3) / 1e9
+    traffic = profiled_traffic(["line", "batch", "batch"][dom % 3] + f"_{ng}_{prec}") if method == "plain" else \
+        profiled_traffic(f"tc_{['line', 'batch', 'batch'][dom % 3]}_{ng}_{prec}")
+    return {"bound": "hbm", "kernel": PASS_NAMES[dom], "achieved": round(achieved, 1), "peak": peak,
+            "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+            "traffic_source": "profiles/dram_traffic.txt (ncu capture of that kernel)" if traffic else None,
+            "algorithmic_bytes": alg_bytes}
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    import __graft_entry__ as entry
+
+    pkg = entry.load_package()
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    ng, ranks = args.ng, args.ranks
+    prec = args.precision
+    seed, tones = cube_input(args)
+    esz = 16 if prec == "c128" else 8
+    dist = pkg.a2aDistribution(ranks, ng, 64, precision=prec)
+    x = synth_bricks(torch, ng, dist.dims, seed, dev, torch.float64 if prec == "c128" else torch.float32, tones)
+    x0 = x.clone()
+    stream = torch.cuda.Stream(device=dev)
+    nbytes_buf = x.numel() * x.element_size()
+    peak, peak_kind = measured_peak()
+
+    methods = cube_methods(args)
+    results = {}
+    for method in methods:  # the same input, each method timed on its own
+        x.copy_(x0)
+        results[method] = time_method(pkg, torch, dist, method, x, stream, args, local_rank, world)
+    dfft, step_ms, means, clocks = results[methods[0]]
+
+    # e2e through the public API with pinned host buffers (the first method)
     e2e = None
     if not args.no_e2e:
+        x.copy_(x0)
         hin = x0.cpu().pin_memory()
         houts = [torch.empty_like(hin).pin_memory() for _ in range(2)]
         ke = max(1, min(args.steps, 10))
@@ -682,46 +717,69 @@ def run_ours(args, rank, world, local_rank):
 
     if rank != 0:
         return
-    peak, peak_kind = measured_peak()
-    names = ["Z_fwd", "X_fwd", "Y_fwd", "Z_inv", "X_inv", "Y_inv"]
-    means = [statistics.mean(v) for v in per_pass]
-    dom = max(range(6), key=lambda i: means[i])
-    alg_bytes = 2.0 * float(ng) ** 3 * esz  # one read + one write of the cube per pass
-    achieved = alg_bytes / (means[dom] * 1e-3) / 1e9
-    key = ["line", "batch", "batch"][dom % 3] + f"_{ng}_{prec}"
-    traffic = profiled_traffic(key)
-    alg_total = 6 * alg_bytes
+
+    # accuracy of every method, outside the timed regions: the forward result
+    # against the oracle's complex128 transform of the same input (the
+    # reference's own check, np.fft.fftn, in FP64), and the round trip
+    acc = {m: {"rel_l2_vs_fp64": None, "roundtrip_rel_l2": None} for m in methods}
+    if not args.no_check:
+        O = entry.load_oracle()
+        d = O.Decomp(ng, ranks)
+        h0 = x0.cpu().numpy().reshape(ranks, -1)
+        ref = O.global_to_bricks(O.fft3_fp64(O.bricks_to_global(h0, d)), d)
+        for m in methods:
+            f = results[m][0]
+            x.copy_(x0)
+            f.forward(x)
+            acc[m]["rel_l2_vs_fp64"] = O.rel_l2_chunked(x.cpu().numpy(), ref)
+            f.inverse(x)
+            acc[m]["roundtrip_rel_l2"] = O.rel_l2_chunked(x.cpu().numpy(), h0)
+        del ref, h0
+
+    alg_total = 6 * 2.0 * float(ng) ** 3 * esz
     value = step_ms / world
+    per_method = {}
+    for m in methods:
+        f, ms, mm, ck = results[m]
+        per_method[m] = {
+            "ms_per_step": round(ms / world, 4),
+            "hbm_frac": round(alg_total / (ms * 1e-3) / 1e9 / peak, 4),
+            "per_pass_ms": {n: round(v, 4) for n, v in zip(PASS_NAMES, mm)},
+            "roofline": method_roofline(mm, ng, esz, prec, peak, peak_kind, m),
+            "rel_l2_vs_fp64": acc[m]["rel_l2_vs_fp64"], "roundtrip_rel_l2": acc[m]["roundtrip_rel_l2"],
+            "plan": [ln for ln in f.plan_report().splitlines() if "chosen" in ln],
+            "clocks": ck, "gpu_launches": 6 * args.steps,
+        }
     line = {
         "metric": METRIC, "value": round(value, 4), "unit": "ms", "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": round(step_ms, 4), "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == "c128" else "f32", "data": "synthetic",
         "impl": "a2afft_b200",
         "config": {"workload": workload_name(ng, ranks, dist.dims, prec, seed, tones), "ng": ng, "world_size": ranks,
-                   "dims": dist.dims, "precision": prec, "method": args.method,
+                   "dims": dist.dims, "precision": prec, "method": methods[0], "methods": methods,
                    "l2": f"inputs {nbytes_buf / 2**30:.2f} GiB > 126 MB L2 (no flush)",
                    "replicas": world},
-        "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": round(achieved, 1), "peak": peak,
-                     "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                     "traffic": traffic, "algorithmic_bytes": alg_bytes},
-        "per_pass_ms": {n: round(m, 4) for n, m in zip(names, means)},
-        "plan": [ln for ln in plan_report.splitlines() if "chosen" in ln],
+        "roofline": per_method[methods[0]]["roofline"],
+        "per_pass_ms": per_method[methods[0]]["per_pass_ms"],
+        "plan": per_method[methods[0]]["plan"],
         "effective_gbs": round(alg_total / (step_ms * 1e-3) / 1e9, 1),
         "hbm_frac": round(alg_total / (step_ms * 1e-3) / 1e9 / peak, 4),
-        "transforms_per_s": round(2 * 1e3 / step_ms, 2),
+        "fwd_inv_pairs_per_s": round(1e3 / step_ms * world, 2),
         "gflops": round(2 * 5 * float(ng) ** 3 * math.log2(float(ng) ** 3) / (step_ms * 1e-3) / 1e9, 1),
-        "rel_l2_reference": "our complex128 transform" if prec == "c64" else None,
-        "rel_l2_vs_fp64": rel_err, "roundtrip_rel_l2": rt_err,
-        "clocks": clk.summary(),
+        "rel_l2_reference": "the oracle's complex128 transform (scipy pocketfft fftn) of the same input",
+        "rel_l2_vs_fp64": acc[methods[0]]["rel_l2_vs_fp64"],
+        "roundtrip_rel_l2": acc[methods[0]]["roundtrip_rel_l2"],
+        "methods": per_method,
+        "clocks": clocks,
         "gpu_launches": 6 * args.steps,
         "e2e": e2e,
         "vendor_fft": vendor,
     }
     if world == 1 and not args.no_cpu:
-        ms, cores, sample, _ = cpu_pipeline_ms(CPU_SAMPLE_NG, ranks, ng, precision=prec, seed=seed, tones=tones)
+        ms, n, cores, sample = host_pipeline_ms(ng, ranks, CPU_BASELINE_STEPS, 1, precision=prec, seed=seed,
+                                                tones=tones, budget_s=30)
         line["cpu_baseline"] = {"value": round(ms, 1), "unit": "ms", "cores": cores, "kind": "port",
-                                "sample": sample + "; remaps single-threaded numpy, 1D transforms scipy.fft "
-                                "workers=cores"}
+                                "sample": sample}
     print(json.dumps(line), flush=True)
 
 

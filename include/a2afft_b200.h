@@ -35,7 +35,7 @@ typedef enum a2a_status {
     A2A_SUCCESS = 0,
     A2A_ERROR_INVALID_VALUE = 1,   /* null pointer, bad enum, non-positive size */
     A2A_ERROR_DECOMPOSITION = 2,   /* a grid the reference asserts on
-                                      (distribution/a2adistribution.cpp:102-121) */
+                                      (distribution/a2adistribution.cpp:61-80) */
     A2A_ERROR_UNSUPPORTED = 3,     /* a transform length with no compiled kernel */
     A2A_ERROR_NO_PLANS = 4,        /* forward/inverse before make_plans */
     A2A_ERROR_MISALIGNED = 5,      /* a device buffer not 16-byte aligned */
@@ -84,7 +84,7 @@ typedef struct a2a_dfft a2a_dfft;                 /* a2adfft */
 /* ---- a2aDistribution ---------------------------------------------------- */
 
 /* a2aDistribution(MPI_Comm, int Ng, int blockSize)
- * (distribution/a2adistribution.cpp:85-154).  The communicator is replaced by
+ * (distribution/a2adistribution.cpp:44-113).  The communicator is replaced by
  * the number of virtual ranks.  Returns A2A_ERROR_DECOMPOSITION where the
  * reference asserts.  Allocates only small device tables on the current
  * device. */
@@ -99,7 +99,7 @@ a2a_status a2a_distribution_create_box(int nx, int ny, int nz, int world_size, i
 
 a2a_status a2a_distribution_describe(const a2a_distribution* dist, a2a_distribution_desc* out);
 
-/* rank2coords + get_local_grid_start (a2adistribution.cpp:55-83). */
+/* rank2coords + get_local_grid_start (a2adistribution.cpp:14-42). */
 a2a_status a2a_rank_coords(const a2a_distribution* dist, int rank, int coords[3], int local_start[3]);
 
 /* Narrows the buffers this process passes to the per-rank kernels (the
@@ -116,7 +116,7 @@ a2a_status a2a_distribution_set_rank_range(a2a_distribution* dist, int first, in
 /* Stream used by the calls below that take no stream (NULL = default). */
 a2a_status a2a_distribution_set_stream(a2a_distribution* dist, void* cuda_stream);
 
-/* The six transpose steps of a2aDistribution (a2adistribution.cpp:156-256),
+/* The six transpose steps of a2aDistribution (a2adistribution.cpp:115-215),
  * over all virtual ranks at once.  On return BOTH buffers hold what the
  * reference leaves in them (the alltoall becomes a rank-major chunk
  * permutation in device memory).  One deliberate difference: the Y return
@@ -124,18 +124,18 @@ a2a_status a2a_distribution_set_stream(a2a_distribution* dist, void* cuda_stream
  * d_y_pencils_to_y_a2a (distribution/kernels/a2apencils.cu:189-208) is not a
  * permutation unless dims[1]==2 or dims[0]==1, and the two agree wherever it
  * is. */
-a2a_status a2a_get_z_pencils(a2a_distribution* dist, void** d_buff1, void** d_buff2);    /* :156-170 */
-a2a_status a2a_return_z_pencils(a2a_distribution* dist, void** d_buff1, void** d_buff2); /* :172-186 */
-a2a_status a2a_get_x_pencils(a2a_distribution* dist, void** d_buff1, void** d_buff2);    /* :188-204 */
-a2a_status a2a_return_x_pencils(a2a_distribution* dist, void** d_buff1, void** d_buff2); /* :206-220 */
-a2a_status a2a_get_y_pencils(a2a_distribution* dist, void** d_buff1, void** d_buff2);    /* :222-238 */
-a2a_status a2a_return_y_pencils(a2a_distribution* dist, void** d_buff1, void** d_buff2); /* :240-256 */
+a2a_status a2a_get_z_pencils(a2a_distribution* dist, void** d_buff1, void** d_buff2);    /* :115-129 */
+a2a_status a2a_return_z_pencils(a2a_distribution* dist, void** d_buff1, void** d_buff2); /* :131-145 */
+a2a_status a2a_get_x_pencils(a2a_distribution* dist, void** d_buff1, void** d_buff2);    /* :147-163 */
+a2a_status a2a_return_x_pencils(a2a_distribution* dist, void** d_buff1, void** d_buff2); /* :165-179 */
+a2a_status a2a_get_y_pencils(a2a_distribution* dist, void** d_buff1, void** d_buff2);    /* :181-197 */
+a2a_status a2a_return_y_pencils(a2a_distribution* dist, void** d_buff1, void** d_buff2); /* :199-215 */
 
 /* The individual kernels the steps are made of, as the reference exposes
  * them in distribution/kernels/kernels.h:3-17 (each synchronous; source and
  * dest are distinct buffers of world_size * nlocal elements):
  * MPI_Alltoall with nsends = nlocal / world_size over the virtual ranks
- * (a2adistribution.cpp:158-165); the pack/unpack remaps
+ * (a2adistribution.cpp:117-125); the pack/unpack remaps
  * (distribution/kernels/a2apencils.cu:5-226; the Y pack is the true inverse
  * of the Y unpack, see above); the fast-axis changes
  * (distribution/kernels/a2achangefastaxis.cu:4-93). */
@@ -150,7 +150,7 @@ a2a_status a2a_d_fast_z_to_x(a2a_distribution* dist, void** source, void** dest)
 a2a_status a2a_d_fast_x_to_y(a2a_distribution* dist, void** source, void** dest);
 a2a_status a2a_d_fast_y_to_z(a2a_distribution* dist, void** source, void** dest);
 
-/* a2aDistribution::finalize (a2adistribution.cpp:258-265); also frees the
+/* a2aDistribution::finalize (a2adistribution.cpp:217-224); also frees the
  * object.  NULL is accepted. */
 a2a_status a2a_distribution_finalize(a2a_distribution* dist);
 
@@ -254,7 +254,7 @@ a2a_status a2a_dfft_launches_per_transform(const a2a_dfft* dfft, int* out);
 /* ---- several GPUs: the fused pass over peer memory ----------------------- */
 
 /* The reference exchanges each axis step between ranks with MPI_Alltoall plus
- * pack/unpack kernels (distribution/a2adistribution.cpp:156-256).  Here one
+ * pack/unpack kernels (distribution/a2adistribution.cpp:115-215).  Here one
  * pass kernel does the whole step across devices: the virtual rank-major
  * buffer is split into `nblocks` blocks of equal size (block g holds the
  * contiguous virtual ranks [g L, (g+1) L), L = world_size / nblocks,
@@ -300,7 +300,7 @@ a2a_status a2a_decompose(int ng, int world_size, int dims[3], int local_grid_siz
 
 /* ---- dump files ---------------------------------------------------------- */
 
-/* The reference's `dims` file (distribution/a2adistribution.cpp:142-151):
+/* The reference's `dims` file (distribution/a2adistribution.cpp:101-111):
  * nine int32 -- world_size, Ng, nlocal, dims[3], local_grid_size[3].  Host
  * only; needs no device. */
 a2a_status a2a_write_dims(int ng, int world_size, const char* path);

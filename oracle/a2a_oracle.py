@@ -11,12 +11,12 @@ What is restated, and from where:
 
 * decomposition -- ``MPI_Dims_create(P, 3)`` (balanced, non-increasing; the
   MPI standard's rule, which the reference calls at
-  ``src/a2afft/distribution/a2adistribution.cpp:100``), ``rank2coords``
-  (``a2adistribution.cpp:55-61``), ``topology2localgrid`` (``:66-72``),
-  ``get_local_grid_start`` (``:77-83``) and the divisibility asserts
-  (``:102-121``);
+  ``src/a2afft/distribution/a2adistribution.cpp:59``), ``rank2coords``
+  (``a2adistribution.cpp:14-20``), ``topology2localgrid`` (``:25-31``),
+  ``get_local_grid_start`` (``:36-42``) and the divisibility asserts
+  (``:61-80``);
 * the alltoall -- ``MPI_Alltoall`` with ``nsends = nlocal / P`` complexes per
-  peer (``a2adistribution.cpp:158-165`` and the five other call sites);
+  peer (``a2adistribution.cpp:117-125`` and the five other call sites);
 * the six pack/unpack remaps of ``distribution/kernels/a2apencils.cu`` and the
   three fast-axis changes of ``distribution/kernels/a2achangefastaxis.cu``,
   written here from the pencil geometry they implement (sender groups,
@@ -46,6 +46,7 @@ What is restated, and from where:
 from __future__ import annotations
 
 import math
+import os
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -70,7 +71,7 @@ def _prime_factors(n: int) -> list[int]:
 def dims_create(nnodes: int, ndims: int = 3) -> list[int]:
     """Balanced non-increasing factorisation of ``nnodes`` into ``ndims``
     factors: the MPI standard's ``MPI_Dims_create`` rule for all-zero input
-    dims, as the reference calls it (``a2adistribution.cpp:100``).
+    dims, as the reference calls it (``a2adistribution.cpp:59``).
 
     Prime factors are handed out largest first, each to the dimension with
     the smallest running product; the result is sorted non-increasing.  This
@@ -87,7 +88,7 @@ def dims_create(nnodes: int, ndims: int = 3) -> list[int]:
 
 
 def rank2coords(rank: int, dims) -> tuple[int, int, int]:
-    """Row-major rank -> brick coordinates (``a2adistribution.cpp:55-61``)."""
+    """Row-major rank -> brick coordinates (``a2adistribution.cpp:14-20``)."""
     d1, d2 = dims[1], dims[2]
     return rank // (d1 * d2), (rank // d2) % d1, rank % d2
 
@@ -99,7 +100,7 @@ class DecompositionError(ValueError):
 @dataclass
 class Decomp:
     """Per-rank brick geometry of ``a2aDistribution``
-    (``a2adistribution.cpp:85-121``), generalised to an ``nx x ny x nz`` box
+    (``a2adistribution.cpp:44-80``), generalised to an ``nx x ny x nz`` box
     (the reference itself only takes one ``Ng``)."""
 
     ng: tuple  # (nx, ny, nz)
@@ -118,16 +119,16 @@ class Decomp:
         if not self.dims:
             self.dims = dims_create(P, 3)
         d = self.dims
-        for a in range(3):  # a2adistribution.cpp:102-104
+        for a in range(3):  # a2adistribution.cpp:61-63
             if self.ng[a] % d[a]:
                 raise DecompositionError(f"N[{a}]={self.ng[a]} not divisible by dims[{a}]={d[a]}")
         self.local = tuple(self.ng[a] // d[a] for a in range(3))
         lx, ly, lz = self.local
         self.nlocal = lx * ly * lz
-        for a in range(3):  # a2adistribution.cpp:115-117
+        for a in range(3):  # a2adistribution.cpp:74-76
             if P % d[a]:
                 raise DecompositionError(f"world_size={P} not divisible by dims[{a}]={d[a]}")
-        for pa, pb in ((lx, ly), (lx, lz), (ly, lz)):  # a2adistribution.cpp:119-121
+        for pa, pb in ((lx, ly), (lx, lz), (ly, lz)):  # a2adistribution.cpp:78-80
             if (pa * pb) % P:
                 raise DecompositionError("a face of the local brick is not divisible by world_size")
 
@@ -297,7 +298,7 @@ def fast_y_to_z(b: np.ndarray, d: Decomp) -> np.ndarray:
 
 
 # --------------------------------------------------------------------------
-# The six distribution steps (a2adistribution.cpp:156-256), all ranks at once.
+# The six distribution steps (a2adistribution.cpp:115-215), all ranks at once.
 # Each takes and returns (buff1, buff2) with the contents the reference leaves.
 # --------------------------------------------------------------------------
 
@@ -335,7 +336,7 @@ def get_y_pencils(b1, b2, d):
 
 
 def return_y_pencils(b1, b2, d):
-    # the Y return packs from Buff2 (a2adistribution.cpp:244): a2adfft puts
+    # the Y return packs from Buff2 (a2adistribution.cpp:203): a2adfft puts
     # the transformed pencils there with its parity copy or its scale kernel
     b1 = scatter(b2, pack_map("y", d))  # corrected inverse (see module doc)
     b2 = alltoall(b1, d)
@@ -409,7 +410,7 @@ def forward(data: np.ndarray, d: Decomp, lines=dft_lines, dtype=np.complex128):
     b1, b2 = return_x_pencils(b1, b2, d)
     b1, b2 = get_y_pencils(b1, b2, d)
     b1 = lines(b1, ng)
-    b2 = b1.copy()  # launch_fast_copy_fft(d_scratch, d_data) (a2adfft.cpp:108)
+    b2 = b1.copy()  # launch_fast_copy_fft(d_scratch, d_data) (a2adfft.cpp:79)
     b1, b2 = return_y_pencils(b1, b2, d)
     return b1
 
@@ -457,19 +458,56 @@ def rel_l2(a: np.ndarray, b: np.ndarray) -> float:
     return float(np.linalg.norm((a - b).ravel())) / (den if den else 1.0)
 
 
-def dft_points(g: np.ndarray, points, inverse: bool = False) -> np.ndarray:
+def rel_l2_chunked(a: np.ndarray, b: np.ndarray, rows: int = 1 << 22) -> float:
+    """``rel_l2`` over flat views in slices of ``rows`` elements, so that
+    multi-GiB arrays need no full-size FP64 temporaries."""
+    a, b = a.reshape(-1), b.reshape(-1)
+    if a.size != b.size:
+        raise ValueError("size mismatch")
+    num = den = 0.0
+    for i in range(0, a.size, rows):
+        bb = b[i:i + rows].astype(np.complex128)
+        dd = a[i:i + rows].astype(np.complex128) - bb
+        num += float(np.vdot(dd, dd).real)
+        den += float(np.vdot(bb, bb).real)
+    return math.sqrt(num / den) if den else math.sqrt(num)
+
+
+def fft3_fp64(g: np.ndarray, inverse: bool = False, workers: int | None = None) -> np.ndarray:
+    """The reference's own acceptance transform, ``np.fft.fftn(inp)``
+    (``src/a2afft/tests/stitch.py:89``), evaluated in complex128 for any box
+    through scipy's pocketfft (the same FFT library numpy uses) on
+    ``workers`` threads, in place on one complex128 copy of ``g``.  Forward
+    unnormalised; the inverse scaled by ``1/(nx ny nz)``.  Used for the
+    full-cube checks at sizes where the matrix DFT (``fft3_global``) is too
+    slow; ``fft3_global`` and ``dft_points`` cross-check it."""
+    import scipy.fft as sfft
+
+    x = np.array(g, dtype=np.complex128)  # always a private copy
+    workers = workers or (os.cpu_count() or 1)
+    if inverse:
+        return sfft.ifftn(x, workers=workers, overwrite_x=True)
+    return sfft.fftn(x, workers=workers, overwrite_x=True)
+
+
+def dft_points(g: np.ndarray, points, inverse: bool = False, slab: int = 32) -> np.ndarray:
     """Exact FP64 3D DFT at a few output points ``[(kx, ky, kz), ...]`` by
-    direct summation (for spot checks of sizes too big for ``fft3_global``)."""
+    direct summation (spot checks independent of any FFT), accumulated over
+    slabs of ``slab`` x planes so that large cubes need no full-size FP64
+    copy."""
     nx, ny, nz = g.shape
-    out = []
     sgn = 1.0 if inverse else -1.0
-    gx = np.asarray(g, dtype=np.complex128)
+    ws = []
     for kx, ky, kz in points:
-        wx = np.exp(sgn * 2j * np.pi * ((np.arange(nx) * kx) % nx) / nx)
-        wy = np.exp(sgn * 2j * np.pi * ((np.arange(ny) * ky) % ny) / ny)
-        wz = np.exp(sgn * 2j * np.pi * ((np.arange(nz) * kz) % nz) / nz)
-        out.append(np.einsum("xyz,x,y,z->", gx, wx, wy, wz))
-    return np.array(out)
+        ws.append((np.exp(sgn * 2j * np.pi * ((np.arange(nx) * kx) % nx) / nx),
+                   np.exp(sgn * 2j * np.pi * ((np.arange(ny) * ky) % ny) / ny),
+                   np.exp(sgn * 2j * np.pi * ((np.arange(nz) * kz) % nz) / nz)))
+    out = np.zeros(len(ws), dtype=np.complex128)
+    for x0 in range(0, nx, slab):
+        blk = np.asarray(g[x0:x0 + slab], dtype=np.complex128)
+        for i, (wx, wy, wz) in enumerate(ws):
+            out[i] += wx[x0:x0 + slab] @ ((blk @ wz) @ wy)
+    return out
 
 
 # --------------------------------------------------------------------------
@@ -511,3 +549,140 @@ def make_input(kind: str, shape, seed: int, dtype=np.complex64, tones: int = 0, 
             ph = 2 * np.pi * (kx * x + ky * y + kz * z)
             out += (amp * np.exp(1j * ph)).astype(dtype)
     return out
+
+
+# --------------------------------------------------------------------------
+# The reference's host step sequence on all host cores (timed CPU baseline)
+# --------------------------------------------------------------------------
+
+
+class HostPipeline:
+    """``a2adfft::forward`` / ``inverse`` (``dfft/a2adfft.cpp:26-158``) over
+    all P virtual ranks on the host cores, step for step and pass for pass as
+    the reference runs it: every alltoall, pack/unpack remap, fast-axis
+    change, batched 1D transform, parity copy and scale is its own pass over
+    the rank-major buffer (19 per direction).  Each remap is the permutation
+    ``unpack_map`` / ``pack_map`` / ``fast_*`` define, written here as the
+    strided copy it is (the sender group and the chunk line are separate
+    tensor axes), so torch's CPU copy kernels run it on every thread; the 1D
+    transforms are torch.fft on the host (pocketfft), in the buffer's own
+    precision, standing in for the reference's batched cuFFT calls.  This is
+    the reference arm and CPU baseline of the benchmark, not a checker: it is
+    itself pinned against the step functions above (tests/test_oracle.py).
+    The Y return uses the true inverse of the Y unpack (see
+    ``y_pencils_to_y_a2a_ref_map``)."""
+
+    def __init__(self, d: Decomp, dtype: str = "c64", threads: int | None = None):
+        import torch
+
+        if d.ng[0] != d.ng[1] or d.ng[1] != d.ng[2]:
+            raise ValueError("the reference pipeline is defined for cubes")
+        self.t = torch
+        self.d = d
+        self.threads = threads or (os.cpu_count() or 1)
+        torch.set_num_threads(self.threads)
+        self.cdt = torch.complex128 if dtype == "c128" else torch.complex64
+        n = d.world_size * d.nlocal
+        self.b1 = torch.empty(n, dtype=self.cdt)
+        self.b2 = torch.empty(n, dtype=self.cdt)
+        self.tmp = torch.empty(n, dtype=self.cdt)  # out-of-place FFT target, swapped in
+
+    # -- passes ---------------------------------------------------------------
+    def _alltoall(self, src, dst):
+        P, c = self.d.world_size, self.d.chunk
+        dst.view(P, P, c).copy_(src.view(P, P, c).transpose(0, 1))
+
+    def _split(self, axis):
+        d0, d1, d2 = self.d.dims
+        la = self.d.local[_AXIS[axis]]
+        return d0, d1, d2, self.d.chunk // la, la
+
+    def _unpack(self, axis, src, dst):
+        P = self.d.world_size
+        d0, d1, d2, m, la = self._split(axis)
+        s = src.view(P, d0, d1, d2, m, la)  # [q][c0][c1][c2][j][e]
+        if axis == "z":  # pencil (c0, c1, j, c2, e)
+            dst.view(P, d0, d1, m, d2, la).copy_(s.permute(0, 1, 2, 4, 3, 5))
+        elif axis == "x":  # pencil (c1, c2, j, c0, e)
+            dst.view(P, d1, d2, m, d0, la).copy_(s.permute(0, 2, 3, 4, 1, 5))
+        else:  # pencil (c0, c2, j, c1, e)
+            dst.view(P, d0, d2, m, d1, la).copy_(s.permute(0, 1, 3, 4, 2, 5))
+
+    def _pack(self, axis, src, dst):
+        P = self.d.world_size
+        d0, d1, d2, m, la = self._split(axis)
+        o = dst.view(P, d0, d1, d2, m, la)
+        if axis == "z":
+            o.copy_(src.view(P, d0, d1, m, d2, la).permute(0, 1, 2, 4, 3, 5))
+        elif axis == "x":
+            o.copy_(src.view(P, d1, d2, m, d0, la).permute(0, 4, 1, 2, 3, 5))
+        else:
+            o.copy_(src.view(P, d0, d2, m, d1, la).permute(0, 1, 4, 2, 3, 5))
+
+    def _fast(self, which, src, dst):
+        P = self.d.world_size
+        lx, ly, lz = self.d.local
+        if which == "z_to_x":  # [x][y][z] -> [z][y][x]
+            dst.view(P, lz, ly, lx).copy_(src.view(P, lx, ly, lz).permute(0, 3, 2, 1))
+        elif which == "x_to_y":  # [z][y][x] -> [x][z][y]
+            dst.view(P, lx, lz, ly).copy_(src.view(P, lz, ly, lx).permute(0, 3, 1, 2))
+        else:  # [x][z][y] -> [x][y][z]
+            dst.view(P, lx, ly, lz).copy_(src.view(P, lx, lz, ly).permute(0, 1, 3, 2))
+
+    def _lines(self, name, inverse):
+        """In-place (by buffer swap) unnormalised 1D transforms of every
+        length-Ng line of buffer ``name``."""
+        t, ng = self.t, self.d.ng[0]
+        src = getattr(self, name)
+        if inverse:
+            t.fft.ifft(src.view(-1, ng), dim=1, norm="forward", out=self.tmp.view(-1, ng))
+        else:
+            t.fft.fft(src.view(-1, ng), dim=1, out=self.tmp.view(-1, ng))
+        setattr(self, name, self.tmp)
+        self.tmp = src
+
+    # -- the six steps (a2adistribution.cpp:115-215) ---------------------------
+    def get_z_pencils(self):
+        self._alltoall(self.b1, self.b2)
+        self._unpack("z", self.b2, self.b1)
+
+    def return_z_pencils(self):
+        self._pack("z", self.b1, self.b2)
+        self._alltoall(self.b2, self.b1)
+
+    def get_x_pencils(self):
+        self._fast("z_to_x", self.b1, self.b2)
+        self._alltoall(self.b2, self.b1)
+        self._unpack("x", self.b1, self.b2)
+
+    def return_x_pencils(self):
+        self._pack("x", self.b2, self.b1)
+        self._alltoall(self.b1, self.b2)
+
+    def get_y_pencils(self):
+        self._fast("x_to_y", self.b2, self.b1)
+        self._alltoall(self.b1, self.b2)
+        self._unpack("y", self.b2, self.b1)
+
+    def return_y_pencils(self):
+        self._pack("y", self.b2, self.b1)
+        self._alltoall(self.b1, self.b2)
+        self._fast("y_to_z", self.b2, self.b1)
+
+    # -- a2adfft::forward / inverse --------------------------------------------
+    def run(self, inverse: bool = False):
+        """One transform of ``self.b1`` in place (``b2`` is the scratch)."""
+        ng = self.d.ng[0]
+        self.get_z_pencils()
+        self._lines("b1", inverse)
+        self.return_z_pencils()
+        self.get_x_pencils()
+        self._lines("b2", inverse)
+        self.return_x_pencils()
+        self.get_y_pencils()
+        self._lines("b1", inverse)
+        if inverse:  # launch_scale_fft(d_scratch, d_data) (a2adfft.cpp:147)
+            self.t.div(self.b1, float(ng) ** 3, out=self.b2)
+        else:  # launch_fast_copy_fft(d_scratch, d_data) (a2adfft.cpp:79)
+            self.b2.copy_(self.b1)
+        self.return_y_pencils()

@@ -48,7 +48,7 @@ def test_status_strings(pkg):
 
 @pytest.mark.parametrize("ng,P", [(8, 6), (10, 4), (64, 256), (12, 8)])
 def test_decomposition_errors_without_gpu(pkg, ng, P):
-    """Grids the reference rejects with assert (a2adistribution.cpp:102-121)
+    """Grids the reference rejects with assert (a2adistribution.cpp:61-80)
     return A2A_ERROR_DECOMPOSITION."""
     with pytest.raises(pkg.A2AError) as e:
         pkg.a2aDistribution(P, ng, 64, precision="c64")

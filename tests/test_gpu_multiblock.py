@@ -110,6 +110,16 @@ def _worker(rank, world, port, P, ng, prec, q):
         bricks = O.global_to_bricks(g, d)
         mine = torch.from_numpy(bricks[rank * L:(rank + 1) * L].ravel().copy()).cuda()
         f = dd.FusedDistributedDfft(P, ng, prec)
+        # a block of the wrong element type on one process: every process
+        # refuses to bind (nothing is mapped, no process waits alone)
+        wrong = torch.zeros(mine.numel(), dtype=torch.complex128 if prec == "c64" else torch.complex64,
+                            device="cuda")
+        try:
+            f.bind(wrong if rank == 0 else mine)
+            raise AssertionError("a block of the wrong element type was bound")
+        except ValueError as e:
+            assert "process 0" in str(e), e
+        del wrong
         f.bind(mine)
         f.forward()
         ref = O.global_to_bricks(O.fft3_global(g, lines=O.fft_lines), d)[rank * L:(rank + 1) * L]

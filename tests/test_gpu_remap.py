@@ -2,17 +2,21 @@
 reference sequence through the C ABI, against the oracle.
 
 Permutations are checked bit-exactly per virtual rank: the input is a
-global-id tracer (cell (x,y,z) holds its linear id in the real part, the rank
-in the imaginary part of the scratch), so any misplaced element changes a
-value.  Both buffers are compared after every step, as the reference leaves
-data in both (``src/a2afft/distribution/a2adistribution.cpp:156-256``)."""
+global-id tracer (every element of both buffers holds a distinct pair of
+exactly representable values derived from its index), so any misplaced element
+changes a value.  Both buffers are compared after every step, as the reference leaves
+data in both (``src/a2afft/distribution/a2adistribution.cpp:115-215``)."""
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
+# the reference's four test grids, then others; (16, 256) is the 256^3 workload's
+# grid at full size, (64, 128) / (256, 128) / (256, 256) the [4,4,4] and
+# [8,8,4] grids of the 512^3 and 1024^3 workloads, where the reference's Y
+# pack is not a permutation
 GRIDS = [(8, 8), (8, 32), (6, 12), (4, 4), (4, 64), (16, 32), (64, 32), (2, 16), (1, 8), (3, 12), (12, 24),
-         (32, 32), (24, 48), (16, 64)]
+         (32, 32), (24, 48), (16, 64), (16, 256), (64, 128), (256, 128), (256, 256)]
 
 STEPS = ["getZPencils", "returnZPencils", "getXPencils", "returnXPencils", "getYPencils", "returnYPencils"]
 ORACLE_STEPS = ["get_z_pencils", "return_z_pencils", "get_x_pencils", "return_x_pencils", "get_y_pencils",
@@ -20,11 +24,14 @@ ORACLE_STEPS = ["get_z_pencils", "return_z_pencils", "get_x_pencils", "return_x_
 
 
 def tracer(O, d, prec, salt):
+    """Distinct exact values: element i of the buffer with salt s (0 or 1)
+    holds v = 2 i + s split as (v // 4096, -(v % 4096)), exact in float32 for
+    every grid here."""
     n = d.world_size * d.nlocal
-    v = np.arange(n, dtype=np.float64) + salt
+    v = 2 * np.arange(n, dtype=np.int64) + int(salt)
     out = np.empty(n, dtype=np.complex128 if prec == "c128" else np.complex64)
-    out.real = v
-    out.imag = -v
+    out.real = v // 4096
+    out.imag = -(v % 4096)
     return out.reshape(d.world_size, d.nlocal)
 
 
@@ -35,14 +42,14 @@ def test_steps_bit_exact(pkg, oracle, cuda, P, ng, prec):
 
     dist = pkg.a2aDistribution(P, ng, 64, precision=prec)
     d = oracle.Decomp(ng, P)
-    b1 = tracer(oracle, d, prec, 0.0)
-    b2 = tracer(oracle, d, prec, 0.5)
+    b1 = tracer(oracle, d, prec, 0)
+    b2 = tracer(oracle, d, prec, 1)
     t1 = torch.from_numpy(b1.ravel().copy()).to(cuda)
     t2 = torch.from_numpy(b2.ravel().copy()).to(cuda)
     for name, oname in zip(STEPS, ORACLE_STEPS):
         if name == "returnYPencils":
             # the Y return packs from Buff2: a2adfft fills it with its parity
-            # copy first (dfft/a2adfft.cpp:108)
+            # copy first (dfft/a2adfft.cpp:79)
             pkg.fast_copy_fft(dist, t2, t1)
             b2 = b1.copy()
         getattr(dist, name)(t1, t2)
@@ -52,7 +59,7 @@ def test_steps_bit_exact(pkg, oracle, cuda, P, ng, prec):
         assert np.array_equal(g1, b1.astype(g1.dtype)), f"{name}: buff1 differs"
         assert np.array_equal(g2, b2.astype(g2.dtype)), f"{name}: buff2 differs"
     # the six steps compose to the identity on the data buffer
-    assert np.array_equal(t1.cpu().numpy().reshape(P, -1), tracer(oracle, d, prec, 0.0))
+    assert np.array_equal(t1.cpu().numpy().reshape(P, -1), tracer(oracle, d, prec, 0))
 
 
 @pytest.mark.parametrize("prec", ["c64", "c128"])

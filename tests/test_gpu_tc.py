@@ -1,14 +1,16 @@
 """Split-precision tensor-core form (tcgen05, kind::f16, FP32 accumulate):
-every radix-16 stage of the pass kernels runs as a GEMM with hi/lo-split
-operands.  Accuracy is stated against the FP64 oracle: split fp16 (22
-significant bits) is held to the 1e-6 relative-L2 bar; split bf16 (16 bits)
-cannot reach it and is held to 5e-5."""
+every radix-16 stage of the pass kernels runs as a GEMM with split 16-bit
+operands.  Accuracy is stated against the FP64 oracle, and both forms are held
+to the 1e-6 relative-L2 bar: split fp16 with two parts (hi + lo, 22
+significant bits), split bf16 with three (hi + mid + lo, 24 bits; two bf16
+parts carry only 16 bits).  The full-size 512^3 and 1024^3 checks are in
+test_gpu_configs.py."""
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
-TOL = {"split_fp16": 1e-6, "split_bf16": 5e-5}
+TOL = {"split_fp16": 1e-6, "split_bf16": 1e-6}
 
 
 def run(pkg, O, cuda, P, shape, method, kind="uniform", tones=0, seed=0):
@@ -48,31 +50,6 @@ def test_split_with_tones(pkg, oracle, cuda, method):
     ref = oracle.fft3_global(g)
     assert oracle.rel_l2(fwd, ref) <= TOL[method]
     assert oracle.rel_l2(inv, g) <= 2 * TOL[method]
-
-
-def test_split_fp16_512_against_fp64_path(pkg, oracle, cuda):
-    """The 512^3 workload (64 virtual ranks): split fp16 against this
-    library's FP64 transform of the same input."""
-    import torch
-
-    dist = pkg.a2aDistribution(64, 512, 64, precision="c64")
-    d64 = pkg.a2aDistribution(64, 512, 64, precision="c128")
-    gen = torch.Generator(device=cuda).manual_seed(5)
-    x = torch.complex(torch.rand(dist.world_size * dist.nlocal, generator=gen, device=cuda) * 2 - 1,
-                      torch.rand(dist.world_size * dist.nlocal, generator=gen, device=cuda) * 2 - 1)
-    y = x.to(torch.complex128)
-    f = pkg.a2adfft(dist, method="split_fp16")
-    f.make_plans()
-    f64 = pkg.a2adfft(d64)
-    f64.make_plans()
-    x0 = x.clone()
-    f.forward(x)
-    f64.forward(y)
-    err = float(torch.linalg.vector_norm(x.to(torch.complex128) - y) / torch.linalg.vector_norm(y))
-    assert err <= 1e-6, err
-    f.inverse(x)
-    rt = float(torch.linalg.vector_norm((x - x0).to(torch.complex128)) / torch.linalg.vector_norm(x0.to(torch.complex128)))
-    assert rt <= 2e-6, rt
 
 
 def test_split_rejects_double_and_unsupported_lengths(pkg, cuda):

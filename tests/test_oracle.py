@@ -166,3 +166,33 @@ def test_dft_points_and_tones(oracle):
     pts = [(0, 0, 0), (3, 5, 7), (15, 7, 11)]
     full = np.fft.fftn(g)
     assert np.allclose(oracle.dft_points(g, pts), [full[p] for p in pts])
+
+
+@pytest.mark.parametrize("P,ng", [(4, 16), (8, 8), (6, 12), (64, 32), (16, 32), (256, 128), (1, 8)])
+def test_host_pipeline_matches_the_step_functions(oracle, P, ng):
+    """The threaded host pipeline (the benchmark's reference arm) takes every
+    step to the same buffers, bit for bit, as the oracle's step functions, and
+    its transform equals the oracle's."""
+    import torch
+
+    d = oracle.Decomp(ng, P)
+    hp = oracle.HostPipeline(d, "c128", threads=2)
+    g = oracle.make_input("normal", (ng,) * 3, seed=5, dtype=np.complex128)
+    b = oracle.global_to_bricks(g, d)
+    b1, b2 = b.copy(), np.zeros_like(b)
+    hp.b1.copy_(torch.from_numpy(b.ravel()))
+    for name in ("get_z_pencils", "return_z_pencils", "get_x_pencils", "return_x_pencils", "get_y_pencils",
+                 "return_y_pencils"):
+        if name == "return_y_pencils":  # the parity copy fills Buff2 first
+            b2 = b1.copy()
+            hp.b2.copy_(hp.b1)
+        b1, b2 = getattr(oracle, name)(b1, b2, d)
+        getattr(hp, name)()
+        assert np.array_equal(hp.b1.numpy().reshape(P, -1), b1), name
+        assert np.array_equal(hp.b2.numpy().reshape(P, -1), b2), name
+    if ng <= 32:
+        hp.b1.copy_(torch.from_numpy(b.ravel()))
+        hp.run(False)
+        assert oracle.rel_l2(hp.b1.numpy().reshape(P, -1), oracle.forward(b, d)) <= 1e-12
+        hp.run(True)
+        assert oracle.rel_l2(hp.b1.numpy().reshape(P, -1), b) <= 1e-12
