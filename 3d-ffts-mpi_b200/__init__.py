@@ -407,6 +407,11 @@ class a2adfft:
         call("a2a_dfft_execute_pass_blocks", self._h, arr, len(vals), int(pass_index), int(bool(inverse)), int(part),
              int(nparts), ctypes.c_void_p(handle))
 
+    def set_blocks_kernel(self, persistent: bool) -> None:
+        """Multi-block pass body: persistent register-pipelined CTAs (default,
+        where compiled) or one tile per CTA."""
+        call("a2a_dfft_set_blocks_kernel", self._h, int(bool(persistent)))
+
     @property
     def launches_per_transform(self) -> int:
         n = ctypes.c_int()

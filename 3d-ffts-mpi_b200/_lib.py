@@ -106,6 +106,7 @@ SIGNATURES = {
     "a2a_write_rank_dumps": [_I, _I, _I, ctypes.c_char_p, _P, _P, _P],
     "a2a_lines_fft_noalloc": [_P, _I, ctypes.c_int64, _I, _I, _P],
     "a2a_dfft_execute_pass_blocks": [_P, _PP, _I, _I, _I, _I, _I, _P],
+    "a2a_dfft_set_blocks_kernel": [_P, _I],
     "a2a_ipc_export": [_P, _P, ctypes.POINTER(ctypes.c_uint64)],
     "a2a_ipc_import": [_P, ctypes.c_uint64, ctypes.POINTER(_P)],
     "a2a_ipc_release": [_P],

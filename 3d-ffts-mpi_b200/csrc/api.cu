@@ -40,6 +40,8 @@ struct a2a_dfft {
     void* d_tc = nullptr;
     const void* tc_tw[3] = {nullptr, nullptr, nullptr};
     const void* tc_b[2] = {nullptr, nullptr};
+    // multi-block pass body: persistent register-pipelined where compiled
+    bool mb_persistent = true;
 };
 
 namespace {
@@ -1194,16 +1196,28 @@ a2a_status a2a_dfft_execute_pass_blocks(a2a_dfft* f, void** blocks, int nblocks,
     }
     const SlotGeom g = slot_geom(d, pass);
     PassKernel k;
-    if (!a2a::find_mb_kernel(d.prec, g.n, g.mode, inverse != 0, &k))
-        return fail(A2A_ERROR_UNSUPPORTED, "no multi-block pass kernel of length %d (lengths 4, 8, 16 have none)",
-                    g.n);
-    if (g.NV % k.lines && !(a2a::find_mb_kernel_small(d.prec, g.n, g.mode, inverse != 0, &k) && g.NV % k.lines == 0))
-        return fail(A2A_ERROR_UNSUPPORTED, "%d lines are not a multiple of a 4-line tile", g.NV);
+    const bool persistent = f->mb_persistent && a2a::find_mb_rpipe_kernel(d.prec, g.n, g.mode, inverse != 0, &k) &&
+                            g.NV % k.lines == 0;
+    if (!persistent) {
+        if (!a2a::find_mb_kernel(d.prec, g.n, g.mode, inverse != 0, &k))
+            return fail(A2A_ERROR_UNSUPPORTED, "no multi-block pass kernel of length %d (lengths 4, 8, 16 have none)",
+                        g.n);
+        if (g.NV % k.lines &&
+            !(a2a::find_mb_kernel_small(d.prec, g.n, g.mode, inverse != 0, &k) && g.NV % k.lines == 0))
+            return fail(A2A_ERROR_UNSUPPORTED, "%d lines are not a multiple of a 4-line tile", g.NV);
+    }
     A2A_CUDA(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem),
              "cudaFuncSetAttribute");
     const int64_t tiles = (int64_t)g.NU * (g.NV / k.lines);
     const int64_t t0 = tiles * part / nparts, t1 = tiles * (part + 1) / nparts;
     if (t1 <= t0) return A2A_SUCCESS;
+    int64_t grid = t1 - t0;
+    if (persistent) {  // one wave of resident CTAs works through the part's tiles
+        int occ = 0;
+        A2A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k.fn, k.threads, k.smem),
+                 "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+        grid = std::min<int64_t>(grid, (int64_t)std::max(occ, 1) * d.sms);
+    }
     const double scale = (inverse && pass == 2) ? 1.0 / ((double)d.ng[0] * d.ng[1] * d.ng[2]) : 1.0;
     const uint32_t block_elems = (uint32_t)((uint64_t)(d.P / nblocks) * d.nlocal);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -1228,11 +1242,18 @@ a2a_status a2a_dfft_execute_pass_blocks(a2a_dfft* f, void** blocks, int nblocks,
         mb.fbe = a2a::FastDiv(block_elems);
         mb.nblk = nblocks;
         mb.tile0 = (int)t0;
+        mb.tile1 = (int)t1;
         void* args[] = {&a, &mb};
-        return cudaLaunchKernel(k.fn, dim3((unsigned)(t1 - t0)), dim3(k.threads), args, k.smem, st);
+        return cudaLaunchKernel(k.fn, dim3((unsigned)grid), dim3(k.threads), args, k.smem, st);
     };
     e = d.prec == A2A_C128 ? launch(double()) : launch(float());
     A2A_CUDA(e, "multi-block pass launch");
+    return A2A_SUCCESS;
+}
+
+a2a_status a2a_dfft_set_blocks_kernel(a2a_dfft* f, int persistent) {
+    if (!f) return fail(A2A_ERROR_INVALID_VALUE, "dfft is NULL");
+    f->mb_persistent = persistent != 0;
     return A2A_SUCCESS;
 }
 

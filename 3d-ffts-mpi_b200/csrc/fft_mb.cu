@@ -22,6 +22,23 @@ template <typename T, int N, int B, int TH, int MB, int MODE, bool INV> PassKern
     return k;
 }
 
+template <typename T, int N, int B, int TH, int MB, int LPT, int MODE, bool INV> PassKernel make_mb_rpipe_kernel() {
+    using P = typename PassPlan<T, N>::Plan;
+    PassKernel k;
+    k.fn = reinterpret_cast<const void*>(&fft_mb_rpipe_kernel<T, P, B, TH, MODE, INV, MB, LPT>);
+    k.kind = KIND_RPIPE;
+    k.n = N;
+    k.threads = TH;
+    k.lines = B;
+    k.min_blocks = MB;
+    k.lpt = LPT;
+    k.smem = pass_smem_bytes<T, P, B, MODE, KIND_RPIPE, LPT>();
+    k.nstages = P::S;
+    for (int s = 0; s < P::S; ++s) k.radix[s] = P::r[s];
+    k.twtotal = P::twtotal();
+    return k;
+}
+
 template <typename T, int N, int B, int TH, int MB> PassKernel mb_pick(int mode, bool inv) {
     if (mode == MODE_LINE)
         return inv ? make_mb_kernel<T, N, B, TH, MB, MODE_LINE, true>() : make_mb_kernel<T, N, B, TH, MB, MODE_LINE, false>();
@@ -44,6 +61,38 @@ template <typename T, int N, int B, int TH, int MB> PassKernel mb_pick(int mode,
     X(12, 4, 64, 1) X(24, 4, 64, 1) X(32, 4, 64, 1) X(48, 4, 64, 1) X(64, 4, 64, 1) X(96, 4, 64, 1)              \
     X(128, 4, 64, 1) X(192, 4, 64, 1) X(256, 4, 128, 1) X(384, 4, 128, 1) X(512, 4, 128, 1)                      \
     X(768, 4, 128, 1) X(1024, 4, 128, 1)
+
+// Persistent register-pipelined configurations (N, lines, threads, min
+// blocks, lines per thread in batch mode): the single-buffer registry's
+// register-pipelined tiles for the long lengths.
+#define A2A_MB_RPIPE_F32(X) \
+    X(256, 16, 256, 2, 1) X(512, 8, 256, 2, 1) X(1024, 4, 256, 2, 1)
+#define A2A_MB_RPIPE_F64(X) \
+    X(512, 8, 512, 1, 1) X(1024, 4, 256, 1, 1)
+
+bool find_mb_rpipe_kernel(a2a_precision prec, int n, int mode, bool inverse, PassKernel* out) {
+#define A2A_MB_CASE(T_, N_, B_, TH_, MB_, LPT_)                                                              \
+    if (n == N_) {                                                                                          \
+        if (mode == MODE_LINE)                                                                              \
+            *out = inverse ? make_mb_rpipe_kernel<T_, N_, B_, TH_, MB_, 1, MODE_LINE, true>()               \
+                           : make_mb_rpipe_kernel<T_, N_, B_, TH_, MB_, 1, MODE_LINE, false>();             \
+        else                                                                                                \
+            *out = inverse ? make_mb_rpipe_kernel<T_, N_, B_, TH_, MB_, LPT_, MODE_BATCH, true>()           \
+                           : make_mb_rpipe_kernel<T_, N_, B_, TH_, MB_, LPT_, MODE_BATCH, false>();         \
+        return true;                                                                                        \
+    }
+#define A2A_MB_F32_CASE(N_, B_, TH_, MB_, LPT_) A2A_MB_CASE(float, N_, B_, TH_, MB_, LPT_)
+#define A2A_MB_F64_CASE(N_, B_, TH_, MB_, LPT_) A2A_MB_CASE(double, N_, B_, TH_, MB_, LPT_)
+    if (prec == A2A_C128) {
+        A2A_MB_RPIPE_F64(A2A_MB_F64_CASE)
+    } else {
+        A2A_MB_RPIPE_F32(A2A_MB_F32_CASE)
+    }
+#undef A2A_MB_F32_CASE
+#undef A2A_MB_F64_CASE
+#undef A2A_MB_CASE
+    return false;
+}
 
 bool find_mb_kernel_small(a2a_precision prec, int n, int mode, bool inverse, PassKernel* out) {
 #define A2A_MB_CASE(N_, B_, TH_, MB_)                                                                       \

@@ -361,6 +361,7 @@ template <typename T> struct MbArgs {
     FastDiv fbe;               // elements per block
     int nblk;
     int tile0;                 // first tile of this launch
+    int tile1;                 // one past its last tile (persistent kernels)
 };
 template <typename T> __device__ __forceinline__ cx<T>* mb_addr(const MbArgs<T>& m, uint32_t o) {
     uint32_t b, r;
@@ -417,11 +418,12 @@ __device__ __forceinline__ void run_stage(const PassArgs<T>& a, typename ElemOf<
             }
             Dft<R, INV, E>::run(x[k]);
             if constexpr (LAST && MB) {
-                static_assert(LPT == 1, "the multi-block pass moves single lines");
+                // a line pair (LPT = 2) never straddles two blocks: both lines
+                // lie in one brick, blocks hold whole bricks
                 const uint32_t line = (uint32_t)base_s[b];
 #pragma unroll
                 for (int r = 0; r < R; ++r)
-                    st_stream(mb_addr(*mb, line + offA_s[j + r * NBL]), scl(x[k][r], a.scale));
+                    st_stream(reinterpret_cast<E*>(mb_addr(*mb, line + offA_s[j + r * NBL])), scl(x[k][r], a.scale));
             } else if constexpr (LAST) {
                 cx<T>* line = a.dst + base_s[b];
                 if (a.split) {

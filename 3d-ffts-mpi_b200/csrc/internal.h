@@ -87,6 +87,8 @@ a2a_status record_error(a2a_status s, const char* what, const char* detail);
 // false for lengths with a single-stage plan (4 8 16) or none
 bool find_mb_kernel(a2a_precision prec, int n, int mode, bool inverse, PassKernel* out);
 bool find_mb_kernel_small(a2a_precision prec, int n, int mode, bool inverse, PassKernel* out);  // 4-line tiles
+// the persistent register-pipelined multi-block kernel of length n, where compiled
+bool find_mb_rpipe_kernel(a2a_precision prec, int n, int mode, bool inverse, PassKernel* out);
 
 // batch.cu: the batched persistent kernel per (precision, direction), its
 // dynamic shared memory, and the tile height of a length's variant (0: the

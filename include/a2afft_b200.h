@@ -270,6 +270,13 @@ a2a_status a2a_dfft_launches_per_transform(const a2a_dfft* dfft, int* out);
 a2a_status a2a_dfft_execute_pass_blocks(a2a_dfft* dfft, void** blocks, int nblocks, int pass, int inverse, int part,
                                         int nparts, void* cuda_stream);
 
+/* The kernel body a2a_dfft_execute_pass_blocks uses: 1 (default) one wave of
+ * persistent CTAs per call, each working through its share of the part's
+ * tiles with the next tile's gathers in flight in registers (lengths 256,
+ * 512, 1024 complex float; 512, 1024 complex double), else 0: one tile per
+ * CTA.  Both give the same result.  No reference counterpart. */
+a2a_status a2a_dfft_set_blocks_kernel(a2a_dfft* dfft, int persistent);
+
 /* Sharing a device buffer with another process (CUDA IPC): export writes an
  * opaque handle of A2A_IPC_HANDLE_BYTES bytes and the buffer's offset inside
  * its allocation; import maps it in this process (on its current device)

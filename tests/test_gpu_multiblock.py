@@ -31,10 +31,13 @@ def _transform(dfft, blocks, inverse, nparts):
         torch.cuda.synchronize()
 
 
+@pytest.mark.parametrize("persistent", [True, False])
 @pytest.mark.parametrize("prec", ["c64", "c128"])
 @pytest.mark.parametrize("P,shape,G,nparts", [(4, 64, 2, 1), (16, 128, 4, 3), (64, 256, 8, 2), (8, 32, 2, 5),
-                                             (4, (64, 128, 32), 4, 2), (16, (96, 64, 192), 2, 1), (16, (96, 48, 192), 2, 1)])
-def test_multiblock_passes_vs_oracle(pkg, oracle, cuda, P, shape, G, nparts, prec):
+                                             (4, (64, 128, 32), 4, 2), (16, (96, 64, 192), 2, 1), (16, (96, 48, 192), 2, 1),
+                                             # long lines for the persistent kernels (512, 1024)
+                                             (16, (512, 64, 128), 4, 3), (4, (64, 1024, 32), 2, 2)])
+def test_multiblock_passes_vs_oracle(pkg, oracle, cuda, P, shape, G, nparts, prec, persistent):
     import torch
 
     shape = (shape,) * 3 if isinstance(shape, int) else tuple(shape)
@@ -47,6 +50,7 @@ def test_multiblock_passes_vs_oracle(pkg, oracle, cuda, P, shape, G, nparts, pre
     single = torch.from_numpy(bricks.ravel().copy()).to(cuda)
     f = pkg.a2adfft(dist)
     f.make_plans()
+    f.set_blocks_kernel(persistent)
     _transform(f, blocks, False, nparts)
     f.forward(single)
     fwd = torch.cat(blocks).cpu().numpy()
