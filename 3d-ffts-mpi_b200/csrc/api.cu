@@ -1365,8 +1365,18 @@ a2a_status a2a_dfft_inverse_host(a2a_dfft* f, void* host_data, void** d_buffer) 
 
 // ---- CUDA IPC for the multi-block pass ----
 
+// Imported allocations, one entry per (device, handle): opened once and
+// closed when the last import of it is released, so two objects of one
+// process that import the same peer buffer share one mapping.
+struct IpcMapping {
+    int device;
+    unsigned char handle[sizeof(cudaIpcMemHandle_t)];
+    void* base;
+    int refs;
+};
 static std::mutex g_ipc_mutex;
-static std::vector<std::pair<void*, void*>> g_ipc_maps;  // (imported address, allocation base)
+static std::vector<IpcMapping> g_ipc_open;
+static std::vector<std::pair<void*, size_t>> g_ipc_maps;  // (imported address, index into g_ipc_open)
 
 using MemRangeFn = CUresult (*)(CUdeviceptr*, size_t*, CUdeviceptr);
 
@@ -1402,29 +1412,52 @@ a2a_status a2a_ipc_export(const void* dev_ptr, void* handle, uint64_t* offset) {
 
 a2a_status a2a_ipc_import(const void* handle, uint64_t offset, void** dev_ptr) {
     if (!handle || !dev_ptr) return fail(A2A_ERROR_INVALID_VALUE, "NULL argument");
-    cudaIpcMemHandle_t h;
-    std::memcpy(&h, handle, sizeof(h));
-    void* base = nullptr;
-    A2A_CUDA(cudaIpcOpenMemHandle(&base, h, cudaIpcMemLazyEnablePeerAccess), "cudaIpcOpenMemHandle");
-    *dev_ptr = static_cast<char*>(base) + offset;
+    int dev = 0;
+    A2A_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
     std::lock_guard<std::mutex> lock(g_ipc_mutex);
-    g_ipc_maps.emplace_back(*dev_ptr, base);
+    size_t idx = g_ipc_open.size();
+    for (size_t i = 0; i < g_ipc_open.size(); ++i)
+        if (g_ipc_open[i].refs > 0 && g_ipc_open[i].device == dev &&
+            std::memcmp(g_ipc_open[i].handle, handle, sizeof(cudaIpcMemHandle_t)) == 0)
+            idx = i;
+    if (idx == g_ipc_open.size()) {
+        cudaIpcMemHandle_t h;
+        std::memcpy(&h, handle, sizeof(h));
+        void* base = nullptr;
+        A2A_CUDA(cudaIpcOpenMemHandle(&base, h, cudaIpcMemLazyEnablePeerAccess), "cudaIpcOpenMemHandle");
+        IpcMapping m;
+        m.device = dev;
+        std::memcpy(m.handle, handle, sizeof(m.handle));
+        m.base = base;
+        m.refs = 0;
+        idx = g_ipc_open.size();
+        for (size_t i = 0; i < g_ipc_open.size(); ++i)  // reuse a closed slot
+            if (g_ipc_open[i].refs == 0) {
+                idx = i;
+                break;
+            }
+        if (idx == g_ipc_open.size()) g_ipc_open.push_back(m);
+        else g_ipc_open[idx] = m;
+    }
+    ++g_ipc_open[idx].refs;
+    *dev_ptr = static_cast<char*>(g_ipc_open[idx].base) + offset;
+    g_ipc_maps.emplace_back(*dev_ptr, idx);
     return A2A_SUCCESS;
 }
 
 a2a_status a2a_ipc_release(void* dev_ptr) {
-    void* base = nullptr;
+    void* close = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_ipc_mutex);
-        for (auto it = g_ipc_maps.begin(); it != g_ipc_maps.end(); ++it)
-            if (it->first == dev_ptr) {
-                base = it->second;
-                g_ipc_maps.erase(it);
-                break;
-            }
+        auto it = g_ipc_maps.begin();
+        while (it != g_ipc_maps.end() && it->first != dev_ptr) ++it;
+        if (it == g_ipc_maps.end())
+            return fail(A2A_ERROR_INVALID_VALUE, "dev_ptr was not imported with a2a_ipc_import");
+        IpcMapping& m = g_ipc_open[it->second];
+        g_ipc_maps.erase(it);
+        if (--m.refs == 0) close = m.base;
     }
-    if (!base) return fail(A2A_ERROR_INVALID_VALUE, "dev_ptr was not imported with a2a_ipc_import");
-    A2A_CUDA(cudaIpcCloseMemHandle(base), "cudaIpcCloseMemHandle");
+    if (close) A2A_CUDA(cudaIpcCloseMemHandle(close), "cudaIpcCloseMemHandle");
     return A2A_SUCCESS;
 }
 

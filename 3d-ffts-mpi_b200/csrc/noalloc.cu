@@ -34,6 +34,10 @@ __device__ __align__(256) unsigned char g_lines_scratch[kScratchBytes];
 // (with that device current) by the first call made on it.
 std::mutex g_mutex;
 void* g_scratch_ptr[kMaxDevices] = {};
+// kernels whose dynamic shared-memory limit is already raised, per device
+// (a host round trip saved on every later call)
+constexpr int kMaxAttrFns = 64;
+const void* g_attr_fn[kMaxDevices][kMaxAttrFns] = {};
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
@@ -157,8 +161,16 @@ extern "C" a2a_status a2a_lines_fft_noalloc(void* data, int n, int64_t nlines, a
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "table kernel launch");
 
-    e = cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+    {
+        std::lock_guard<std::mutex> lock(g_mutex);
+        int slot = 0;
+        while (slot < kMaxAttrFns && g_attr_fn[dev][slot] && g_attr_fn[dev][slot] != k.fn) ++slot;
+        if (slot == kMaxAttrFns || g_attr_fn[dev][slot] != k.fn) {
+            e = cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+            if (slot < kMaxAttrFns) g_attr_fn[dev][slot] = k.fn;
+        }
+    }
     const unsigned grid = unsigned(NU * (NV / k.lines));
     const uint32_t* offA = reinterpret_cast<const uint32_t*>(s + l.offA);
     const uint32_t* offU = reinterpret_cast<const uint32_t*>(s + l.offU);

@@ -172,7 +172,9 @@ a2a_status a2a_inverse_1d_fft(a2a_distribution* dist, void** d_data);
  * in a fixed file-scope device array of A2A_LINES_NOALLOC_SCRATCH_BYTES,
  * which every GPU that loads the library holds until the process exits.
  * The first call on a device resolves that array's address (with the device
- * current); make that first call before any stream capture.  Each call
+ * current) and keeps it for the life of the process; make that first call
+ * before any stream capture, and do not use this entry point on a device
+ * after cudaDeviceReset (the module may then reload elsewhere).  Each call
  * rebuilds the tables on `stream` and then transforms; calls share the array,
  * so calls that overlap on the GPU race.  Sizes whose tables exceed the
  * array (more than about 64K groups of up to 1024 lines) return
@@ -280,8 +282,9 @@ a2a_status a2a_dfft_set_blocks_kernel(a2a_dfft* dfft, int persistent);
 /* Sharing a device buffer with another process (CUDA IPC): export writes an
  * opaque handle of A2A_IPC_HANDLE_BYTES bytes and the buffer's offset inside
  * its allocation; import maps it in this process (on its current device)
- * and returns the buffer's address there; release unmaps it.  No reference
- * counterpart. */
+ * and returns the buffer's address there; release undoes one import.  A
+ * handle imported more than once on one device shares one mapping, which is
+ * unmapped when its last import is released.  No reference counterpart. */
 #define A2A_IPC_HANDLE_BYTES 64
 a2a_status a2a_ipc_export(const void* dev_ptr, void* handle, uint64_t* offset);
 a2a_status a2a_ipc_import(const void* handle, uint64_t offset, void** dev_ptr);

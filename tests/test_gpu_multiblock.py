@@ -155,3 +155,50 @@ def test_fused_distributed_two_processes_one_gpu(cuda, P, ng, prec):
         assert r[0] == "ok", r
         assert r[2] <= TOL[prec] and r[3] <= TOL[prec], r
     assert all(p.exitcode == 0 for p in procs)
+
+
+def test_ipc_import_twice_shares_one_mapping(pkg, cuda):
+    """Two imports of one handle in one process (e.g. two fused objects
+    binding the same peer buffer): the same address, the buffer still
+    readable through the second import after the first is released, and each
+    import released exactly once.  (CUDA refuses imports in the exporting
+    process itself, so the handle comes from a child process.)"""
+    import torch
+
+    ctx = mp.get_context("spawn")
+    q_in, q_out = ctx.Queue(), ctx.Queue()
+    p = ctx.Process(target=_exporter, args=(q_in, q_out))
+    p.start()
+    try:
+        h, off = q_out.get(timeout=120)
+        a = pkg.ipc_import(h, off)
+        b = pkg.ipc_import(h, off)
+        assert a == b
+        pkg.ipc_release(a)
+        # read the 64 floats through the remaining import
+        host = torch.empty(64, dtype=torch.float32).pin_memory()
+        from cuda.bindings import runtime as cudart
+
+        (err,) = cudart.cudaMemcpy(host.data_ptr(), b, 256, cudart.cudaMemcpyKind.cudaMemcpyDeviceToHost)
+        assert err == cudart.cudaError_t.cudaSuccess
+        assert torch.equal(host, torch.arange(64, dtype=torch.float32))
+        pkg.ipc_release(b)
+        with pytest.raises(pkg.A2AError):
+            pkg.ipc_release(b)
+    finally:
+        q_in.put("done")
+        p.join(timeout=60)
+    assert p.exitcode == 0
+
+
+def _exporter(q_in, q_out):
+    sys.path.insert(0, ROOT)
+    import torch
+
+    import __graft_entry__ as entry
+
+    torch.cuda.set_device(0)
+    pkg = entry.load_package()
+    x = torch.arange(64, dtype=torch.float32, device="cuda")
+    q_out.put(pkg.ipc_export(x))
+    q_in.get(timeout=300)
