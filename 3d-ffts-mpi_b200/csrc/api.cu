@@ -36,7 +36,14 @@ struct a2a_dfft {
     a2a_method method = A2A_METHOD_PLAIN;
     // split tensor-core method: kernels per pass [Z, X, Y][inverse], twiddles
     // of their radix plans per axis, split radix-16 operands per direction
-    PassKernel tc[3][2];
+    PassKernel tc[3][2];  // the kernel in use per pass and direction
+    // candidates per pass, direction: 0 = one tile per CTA, 1 = persistent
+    // CTAs fed by the TMA ring (where the plan and geometry allow it)
+    PassKernel tcv[3][2][2];
+    bool tcv_fits[3][2] = {};
+    int tcv_occ[3][2] = {};
+    float tcv_ms[3][2] = {};
+    int tc_chosen[3] = {0, 0, 0};
     void* d_tc = nullptr;
     const void* tc_tw[3] = {nullptr, nullptr, nullptr};
     const void* tc_b[2] = {nullptr, nullptr};
@@ -608,6 +615,19 @@ cudaError_t run_tc_pass(const a2a_dfft* f, int pass, bool inv, void* p, cudaStre
     const int axis = pass == 0 ? 2 : pass == 1 ? 0 : 1;
     const PassKernel& k = f->tc[pass][inv ? 1 : 0];
     const double scale = (inv && pass == 2) ? 1.0 / ((double)d.ng[0] * d.ng[1] * d.ng[2]) : 1.0;
+    const void* maps = nullptr;
+    unsigned grid = unsigned((uint64_t)g.NU * (g.NV / k.lines));
+    if (k.kind == a2a::KIND_TCR) {  // tensor maps of this pass for buffer p, one wave of persistent CTAs
+        a2a::TmatEntry& ce = d.tmat[pass];
+        if (ce.ptr != p || ce.lines != k.lines) {
+            ce.ptr = nullptr;
+            if (!build_tmat(d, pass, k.lines, p, &ce.maps)) return cudaErrorInvalidValue;
+            ce.ptr = p;
+            ce.lines = k.lines;
+        }
+        maps = &ce.maps;
+        grid = (unsigned)std::min<uint64_t>(grid, (uint64_t)std::max(f->tcv_occ[pass][1], 1) * d.sms);
+    }
     a2a::PassArgs<float> a;
     a.src = static_cast<const float2*>(p);
     a.dst = static_cast<float2*>(p);
@@ -621,8 +641,7 @@ cudaError_t run_tc_pass(const a2a_dfft* f, int pass, bool inv, void* p, cudaStre
     a.split = 0;
     a.err = d.d_err;
     a.tcb = f->tc_b[inv ? 1 : 0];
-    void* args[] = {&a};
-    const unsigned grid = unsigned((uint64_t)g.NU * (g.NV / k.lines));
+    void* args[] = {&a, const_cast<void*>(maps)};
     return cudaLaunchKernel(k.fn, dim3(grid), dim3(k.threads), args, k.smem, st);
 }
 
@@ -732,17 +751,41 @@ a2a_status setup_tc(a2a_dfft* f, a2a_method m) {
     for (int p = 0; p < 3; ++p) {
         const SlotGeom g = slot_geom(d, p);
         for (int inv = 0; inv < 2; ++inv)
-            if (!a2a::find_tc_kernel(g.n, g.mode, inv, fmt, &f->tc[p][inv]))
+            if (!a2a::find_tc_kernel(g.n, g.mode, inv, fmt, &f->tcv[p][inv][0]))
                 return fail(A2A_ERROR_NOT_IMPLEMENTED,
                             "%s pass: no tensor-core kernel of length %d (available: 64 128 256 512 1024)", names[p],
                             g.n);
-        if (g.NV % f->tc[p][0].lines)
+        if (g.NV % f->tcv[p][0][0].lines)
             return fail(A2A_ERROR_UNSUPPORTED, "%s pass: %d lines are not a multiple of the %d-line tile", names[p],
-                        g.NV, f->tc[p][0].lines);
+                        g.NV, f->tcv[p][0][0].lines);
+        // the ring form where its plan exists and every tile is whole
+        // tensor-map boxes (probed against a stand-in aligned address)
+        bool ring = true;
         for (int inv = 0; inv < 2; ++inv)
-            A2A_CUDA(cudaFuncSetAttribute(f->tc[p][inv].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)f->tc[p][inv].smem),
-                     "cudaFuncSetAttribute");
+            ring = ring && a2a::find_tc_ring_kernel(g.n, g.mode, inv, fmt, &f->tcv[p][inv][1]);
+        if (ring) {
+            a2a::TmatMaps probe;
+            ring = g.NV % f->tcv[p][0][1].lines == 0 &&
+                   build_tmat(d, p, f->tcv[p][0][1].lines, reinterpret_cast<const void*>(uintptr_t(1) << 20), &probe);
+        }
+        f->tcv_fits[p][0] = true;
+        f->tcv_fits[p][1] = ring;
+        for (int c = 0; c < 2; ++c) {
+            f->tcv_ms[p][c] = 0.f;
+            if (!f->tcv_fits[p][c]) continue;
+            for (int inv = 0; inv < 2; ++inv)
+                A2A_CUDA(cudaFuncSetAttribute(f->tcv[p][inv][c].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)f->tcv[p][inv][c].smem),
+                         "cudaFuncSetAttribute");
+            A2A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&f->tcv_occ[p][c], f->tcv[p][0][c].fn,
+                                                                   f->tcv[p][0][c].threads, f->tcv[p][0][c].smem),
+                     "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+            if (f->tcv_occ[p][c] < 1) f->tcv_fits[p][c] = false;
+        }
+        if (!f->tcv_fits[p][0] && !f->tcv_fits[p][1])
+            return fail(A2A_ERROR_UNSUPPORTED, "%s pass: no tensor-core kernel fits an SM", names[p]);
+        f->tc_chosen[p] = f->tcv_fits[p][1] ? 1 : 0;  // the ring form by default
+        for (int inv = 0; inv < 2; ++inv) f->tc[p][inv] = f->tcv[p][inv][f->tc_chosen[p]];
     }
     // twiddles of the tensor-core radix plans (per axis) and the operands
     std::vector<float> tw;
@@ -1079,6 +1122,55 @@ a2a_status a2a_dfft_make_plans(a2a_dfft* f, void** d_scratch) {
         cudaEventDestroy(e1);
         if (status != A2A_SUCCESS) return status;
     }
+    if (f->scratch && f->autotune && f->method != A2A_METHOD_PLAIN) {
+        if (reinterpret_cast<uintptr_t>(f->scratch) % 16)
+            return fail(A2A_ERROR_MISALIGNED, "d_scratch[0] is not 16-byte aligned");
+        // the same sweep over the tensor-core kernels: one tile per CTA or
+        // the persistent ring form, per pass, timed inside a whole forward +
+        // inverse on the scratch buffer
+        cudaStream_t st = d.stream;
+        cudaEvent_t e0, e1;
+        A2A_CUDA(cudaEventCreate(&e0), "cudaEventCreate");
+        A2A_CUDA(cudaEventCreate(&e1), "cudaEventCreate");
+        cudaError_t e = cudaSuccess;
+        auto transform = [&]() {
+            cudaError_t r = cudaSuccess;
+            for (int inv = 0; inv < 2 && r == cudaSuccess; ++inv)
+                for (int p = 0; p < 3 && r == cudaSuccess; ++p) r = run_tc_pass(f, p, inv != 0, f->scratch, st);
+            return r;
+        };
+        for (int p = 0; p < 3 && e == cudaSuccess; ++p) {
+            int best = f->tc_chosen[p];
+            float best_ms = 1e30f;
+            for (int c = 0; c < 2 && e == cudaSuccess; ++c) {
+                if (!f->tcv_fits[p][c]) continue;
+                for (int inv = 0; inv < 2; ++inv) f->tc[p][inv] = f->tcv[p][inv][c];
+                e = transform();  // warm-up
+                float ms = 1e30f;
+                for (int rep = 0; rep < 3 && e == cudaSuccess; ++rep) {
+                    e = cudaEventRecord(e0, st);
+                    if (e == cudaSuccess) e = transform();
+                    if (e == cudaSuccess) e = cudaEventRecord(e1, st);
+                    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+                    float t = 0.f;
+                    if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+                    if (e == cudaSuccess) ms = std::min(ms, t);
+                }
+                f->tcv_ms[p][c] = ms;
+                if (e == cudaSuccess && ms < best_ms) {
+                    best_ms = ms;
+                    best = c;
+                }
+            }
+            f->tc_chosen[p] = best;
+            for (int inv = 0; inv < 2; ++inv) f->tc[p][inv] = f->tcv[p][inv][best];
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (e != cudaSuccess) return cuda_fail(e, "autotune launch");
+        a2a_status s2 = check_device_flag(d);
+        if (s2 != A2A_SUCCESS) return s2;
+    }
     f->plans_made = true;
     return A2A_SUCCESS;
 }
@@ -1091,7 +1183,7 @@ a2a_status a2a_dfft_check_device(const a2a_dfft* f) {
 a2a_status a2a_dfft_variant_count(const a2a_dfft* f, int pass, int* count) {
     if (!f || !count) return fail(A2A_ERROR_INVALID_VALUE, "NULL argument");
     if (pass < 0 || pass > 2) return fail(A2A_ERROR_INVALID_VALUE, "pass must be 0 (Z), 1 (X) or 2 (Y)");
-    *count = f->dist->d.slot[pass][0].ncand;
+    *count = f->method == A2A_METHOD_PLAIN ? f->dist->d.slot[pass][0].ncand : 2;
     return A2A_SUCCESS;
 }
 
@@ -1099,6 +1191,15 @@ a2a_status a2a_dfft_select_variant(a2a_dfft* f, int pass, int variant) {
     if (!f) return fail(A2A_ERROR_INVALID_VALUE, "dfft is NULL");
     if (pass < 0 || pass > 2) return fail(A2A_ERROR_INVALID_VALUE, "pass must be 0 (Z), 1 (X) or 2 (Y)");
     Dist& d = f->dist->d;
+    if (f->method != A2A_METHOD_PLAIN) {  // 0: one tile per CTA, 1: the persistent ring form
+        if (!f->tcv[pass][0][0].fn) return fail(A2A_ERROR_NO_PLANS, "the tensor-core kernels are not set up");
+        if (variant < 0 || variant > 1) return fail(A2A_ERROR_INVALID_VALUE, "variant %d outside [0, 2)", variant);
+        if (!f->tcv_fits[pass][variant])
+            return fail(A2A_ERROR_UNSUPPORTED, "tensor-core variant %d does not fit this pass", variant);
+        f->tc_chosen[pass] = variant;
+        for (int inv = 0; inv < 2; ++inv) f->tc[pass][inv] = f->tcv[pass][inv][variant];
+        return A2A_SUCCESS;
+    }
     if (variant < 0 || variant >= d.slot[pass][0].ncand)
         return fail(A2A_ERROR_INVALID_VALUE, "variant %d outside [0, %d)", variant, d.slot[pass][0].ncand);
     if (!d.slot[pass][0].fits[variant] || !d.slot[pass][1].fits[variant])
@@ -1138,14 +1239,19 @@ a2a_status a2a_dfft_plan_report(const a2a_dfft* f, char* buf, size_t len) {
         }
     }
     if (f->method != A2A_METHOD_PLAIN)
-        for (int p = 0; p < 3; ++p) {
-            const PassKernel& k = f->tc[p][0];
-            char line[256];
-            snprintf(line, sizeof line, "%s pass n=%d tensor-core %s lines=%d threads=%d smem=%zu radix=%d,%d,%d <- in use\n",
-                     names[p], k.n, f->method == A2A_METHOD_SPLIT_FP16 ? "split-fp16" : "split-bf16", k.lines, k.threads,
-                     k.smem, k.radix[0], k.radix[1], k.radix[2]);
-            out += line;
-        }
+        for (int p = 0; p < 3; ++p)
+            for (int c = 0; c < 2; ++c) {
+                if (!f->tcv_fits[p][c]) continue;
+                const PassKernel& k = f->tcv[p][0][c];
+                char line[256];
+                snprintf(line, sizeof line,
+                         "%s pass n=%d tensor-core %s %s lines=%d threads=%d smem=%zu occ=%d radix=%d,%d,%d "
+                         "tuned_ms=%.4f%s\n",
+                         names[p], k.n, f->method == A2A_METHOD_SPLIT_FP16 ? "split-fp16" : "split-bf16",
+                         c ? "ring" : "tile", k.lines, k.threads, k.smem, f->tcv_occ[p][c], k.radix[0], k.radix[1],
+                         k.radix[2], f->tcv_ms[p][c], c == f->tc_chosen[p] ? " <- in use" : "");
+                out += line;
+            }
     snprintf(buf, len, "%s", out.c_str());
     return out.size() < len ? A2A_SUCCESS : fail(A2A_ERROR_INVALID_VALUE, "report truncated (%zu bytes)", out.size());
 }

@@ -293,5 +293,7 @@ constexpr int kMaxVariants = 32;
 // fft_tc.cu: the split-precision tensor-core kernel of length n (fmt 0 =
 // fp16, 1 = bf16); false when n has none.
 bool find_tc_kernel(int n, int mode, bool inverse, int fmt, PassKernel* out);
+// the persistent TMA-ring form of it, where the plan has one (not 256)
+bool find_tc_ring_kernel(int n, int mode, bool inverse, int fmt, PassKernel* out);
 
 }  // namespace a2a

@@ -13,40 +13,60 @@ template <> struct TcPlan<256> { using Plan = RadixPlan<16, 16>; static constexp
 template <> struct TcPlan<512> { using Plan = RadixPlan<2, 16, 16>; static constexpr int B = 8; };
 template <> struct TcPlan<1024> { using Plan = RadixPlan<4, 16, 16>; static constexpr int B = 4; };
 
-template <int N, int MODE, bool INV, int FMT> PassKernel make_tc_kernel() {
+template <int N, int MODE, bool INV, int FMT, bool RING> PassKernel make_tc_kernel() {
     using P = typename TcPlan<N>::Plan;
     constexpr int B = TcPlan<N>::B;
     PassKernel k;
-    k.fn = reinterpret_cast<const void*>(&fft_tc_kernel<P, B, MODE, INV, FMT>);
-    k.kind = KIND_TC;
+    if constexpr (RING) {
+        k.fn = reinterpret_cast<const void*>(&fft_tc_ring_kernel<P, B, MODE, INV, FMT>);
+        k.kind = KIND_TCR;
+        k.smem = tc_ring_smem_bytes<P, B, MODE, FMT>();
+    } else {
+        k.fn = reinterpret_cast<const void*>(&fft_tc_kernel<P, B, MODE, INV, FMT>);
+        k.kind = KIND_TC;
+        k.smem = tc_smem_bytes<P, B, MODE, FMT>();
+    }
     k.n = N;
     k.threads = B * N / 16;
     k.lines = B;
     k.min_blocks = 1;
     k.lpt = 1;
-    k.smem = tc_smem_bytes<P, B, MODE, FMT>();
     k.nstages = P::S;
     for (int s = 0; s < P::S; ++s) k.radix[s] = P::r[s];
     k.twtotal = P::twtotal();
     return k;
 }
 
-template <int N> PassKernel tc_pick(int mode, bool inv, int fmt) {
+template <int N, bool RING> PassKernel tc_pick(int mode, bool inv, int fmt) {
     if (mode == MODE_LINE) {
-        if (fmt == TC_FP16) return inv ? make_tc_kernel<N, MODE_LINE, true, TC_FP16>() : make_tc_kernel<N, MODE_LINE, false, TC_FP16>();
-        return inv ? make_tc_kernel<N, MODE_LINE, true, TC_BF16>() : make_tc_kernel<N, MODE_LINE, false, TC_BF16>();
+        if (fmt == TC_FP16)
+            return inv ? make_tc_kernel<N, MODE_LINE, true, TC_FP16, RING>() : make_tc_kernel<N, MODE_LINE, false, TC_FP16, RING>();
+        return inv ? make_tc_kernel<N, MODE_LINE, true, TC_BF16, RING>() : make_tc_kernel<N, MODE_LINE, false, TC_BF16, RING>();
     }
-    if (fmt == TC_FP16) return inv ? make_tc_kernel<N, MODE_BATCH, true, TC_FP16>() : make_tc_kernel<N, MODE_BATCH, false, TC_FP16>();
-    return inv ? make_tc_kernel<N, MODE_BATCH, true, TC_BF16>() : make_tc_kernel<N, MODE_BATCH, false, TC_BF16>();
+    if (fmt == TC_FP16)
+        return inv ? make_tc_kernel<N, MODE_BATCH, true, TC_FP16, RING>() : make_tc_kernel<N, MODE_BATCH, false, TC_FP16, RING>();
+    return inv ? make_tc_kernel<N, MODE_BATCH, true, TC_BF16, RING>() : make_tc_kernel<N, MODE_BATCH, false, TC_BF16, RING>();
 }
 
 bool find_tc_kernel(int n, int mode, bool inverse, int fmt, PassKernel* out) {
     switch (n) {
-        case 64: *out = tc_pick<64>(mode, inverse, fmt); return true;
-        case 128: *out = tc_pick<128>(mode, inverse, fmt); return true;
-        case 256: *out = tc_pick<256>(mode, inverse, fmt); return true;
-        case 512: *out = tc_pick<512>(mode, inverse, fmt); return true;
-        case 1024: *out = tc_pick<1024>(mode, inverse, fmt); return true;
+        case 64: *out = tc_pick<64, false>(mode, inverse, fmt); return true;
+        case 128: *out = tc_pick<128, false>(mode, inverse, fmt); return true;
+        case 256: *out = tc_pick<256, false>(mode, inverse, fmt); return true;
+        case 512: *out = tc_pick<512, false>(mode, inverse, fmt); return true;
+        case 1024: *out = tc_pick<1024, false>(mode, inverse, fmt); return true;
+        default: return false;
+    }
+}
+
+// Lengths whose tensor-core plan starts with a CUDA-core stage have a ring
+// form (256 = 16 x 16 has none).
+bool find_tc_ring_kernel(int n, int mode, bool inverse, int fmt, PassKernel* out) {
+    switch (n) {
+        case 64: *out = tc_pick<64, true>(mode, inverse, fmt); return true;
+        case 128: *out = tc_pick<128, true>(mode, inverse, fmt); return true;
+        case 512: *out = tc_pick<512, true>(mode, inverse, fmt); return true;
+        case 1024: *out = tc_pick<1024, true>(mode, inverse, fmt); return true;
         default: return false;
     }
 }

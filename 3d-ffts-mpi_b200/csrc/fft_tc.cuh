@@ -30,6 +30,7 @@
 #include <cuda_fp16.h>
 
 #include "fft_tile.cuh"
+#include "fft_tmat.cuh"
 
 namespace a2a {
 
@@ -417,6 +418,182 @@ __global__ void __launch_bounds__(B * PLAN::N / 16, (tc_min_blocks<PLAN, B, FMT>
     // allocated (freeing them under running MMAs would hand them to another
     // CTA while they are written); the error flag is already set.
     if (!ok && !ctx.drained) return;
+    tc_fence_after();
+    if (tid < 32)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(ctx.tmem), "r"(TCOLS)
+                     : "memory");
+}
+
+// Persistent form fed by the TMA ring: each CTA allocates its tensor memory,
+// loads the split operand, twiddles and offsets once, then works through
+// tiles blockIdx.x, blockIdx.x + gridDim.x, ...  Every tile arrives as whole
+// tensor-map copies (the single-GPU ring of fft_tmat.cuh, no multicast) in a
+// 2-slot shared-memory ring; each slot is also its tile's Stockham tile
+// (transformed in place), and is refilled with the tile two ahead as soon as
+// its tile's last stage has read it, so one tile's copy is in flight while
+// the other is transformed.  Plans whose first stage is not radix 16 (the
+// CUDA-core stage 0 reads the slot into registers before rewriting it).
+template <class PLAN, int B, int MODE, int FMT> __host__ __device__ constexpr uint32_t tc_ring_slot_bytes() {
+    return tmat_slot_bytes_for<float, PLAN, B, MODE, 1, true>();
+}
+template <class PLAN, int B, int MODE, int FMT> __host__ __device__ constexpr size_t tc_ring_smem_bytes() {
+    size_t bytes = kTmatAlign;  // room to align the ring
+    bytes += 2 * (size_t)tc_ring_slot_bytes<PLAN, B, MODE, FMT>();
+    bytes += tc_b_bytes(FMT);
+    bytes += sizeof(float2) * (size_t)PLAN::twtotal();
+    bytes += sizeof(uint32_t) * (size_t)PLAN::N;
+    bytes = (bytes + 15) & ~size_t(15);
+    bytes += sizeof(size_t) * (size_t)B;
+    bytes += sizeof(unsigned long long) * 3 + 16;  // two ring barriers, the MMA barrier, tensor-memory address
+    return bytes;
+}
+
+template <class PLAN, int B, int MODE, bool INV, int FMT>
+__global__ void __launch_bounds__(B * PLAN::N / 16, (tc_min_blocks<PLAN, B, FMT>()))
+    fft_tc_ring_kernel(const PassArgs<float> a, const __grid_constant__ TmatMaps m) {
+    constexpr int N = PLAN::N;
+    constexpr int THREADS = B * N / 16;
+    constexpr uint32_t TCOLS = tc_tcols<PLAN, B, FMT>();
+    using G = TileGeom<MODE, B, N, sizeof(float2), tc_tile_swizzle<PLAN, B, MODE>()>;
+    constexpr int TWN = PLAN::twtotal();
+    constexpr int R0 = PLAN::r[0];
+    static_assert(R0 != 16, "the ring form starts with a CUDA-core stage");
+    constexpr int NBL = N / R0;
+    constexpr int NBT = B * NBL;
+    constexpr int K = (NBT + THREADS - 1) / THREADS;
+    constexpr bool EXACT = (NBT % THREADS) == 0;
+    constexpr bool BFAST0 = (MODE == MODE_BATCH);
+    constexpr int NSTG = 2;
+    constexpr uint32_t SLOT = tc_ring_slot_bytes<PLAN, B, MODE, FMT>();
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const uint32_t s0 = smem_u32(smem_raw);
+    unsigned char* ring = smem_raw + (((s0 + kTmatAlign - 1) & ~(kTmatAlign - 1)) - s0);
+    unsigned char* bmat = ring + NSTG * SLOT;
+    float2* tw = reinterpret_cast<float2*>(bmat + tc_b_bytes(FMT));
+    uint32_t* offA_s = reinterpret_cast<uint32_t*>(tw + TWN);
+    size_t* base_s = reinterpret_cast<size_t*>(
+        reinterpret_cast<unsigned char*>(tw) + ((sizeof(float2) * TWN + sizeof(uint32_t) * N + 15) & ~size_t(15)));
+    unsigned long long* rbar = reinterpret_cast<unsigned long long*>(base_s + B);  // ring slots
+    unsigned long long* mbar = rbar + NSTG;                                        // MMA completion
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 1);
+
+    const int tid = threadIdx.x;
+    const int tilesV = a.NV / B;
+    const int ntiles = a.NU * tilesV;
+    const int mine = (int)blockIdx.x < ntiles ? (ntiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x : 0;
+
+    if (tid < 32) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TCOLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int i = 0; i < NSTG; ++i) mbar_init(rbar + i, 1);
+        mbar_init(mbar, 1);
+        fence_mbar_init();
+    }
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(a.tcb);
+        uint4* dst = reinterpret_cast<uint4*>(bmat);
+        for (int i = tid; i < tc_b_bytes(FMT) / 16; i += THREADS) dst[i] = src[i];
+    }
+    for (int i = tid; i < TWN; i += THREADS) tw[i] = a.tw[i];
+    for (int i = tid; i < N; i += THREADS) offA_s[i] = a.offA[i];
+    fence_proxy_async_smem();  // B operand visible to the tensor cores
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+
+    TcCtx ctx;
+    ctx.b_addr = smem_u32(bmat);
+    ctx.tmem = *tmem_slot;
+    ctx.bar = mbar;
+    ctx.phase = 0;
+    ctx.drained = true;
+
+    int issued = 0;  // thread 0: tiles of this CTA whose copies were issued
+    if (tid == 0)
+        for (; issued < NSTG && issued < mine; ++issued)
+            tmat_issue<float, B, N>(m, blockIdx.x + issued * gridDim.x, tilesV, ring + issued * SLOT, rbar + issued);
+
+    bool ok = true;
+    int i = 0;
+    for (; i < mine; ++i) {
+        const int t = blockIdx.x + i * gridDim.x;
+        const int s = i % NSTG;
+        const int u = t / tilesV;
+        const int v0 = (t - u * tilesV) * B;
+        const size_t ubase = __ldg(a.offU + u);
+        for (int b = tid; b < B; b += THREADS) base_s[b] = ubase + __ldg(a.offV + v0 + b);
+        if (__syncthreads_or(!mbar_wait_bounded(rbar + s, (uint32_t)((i / NSTG) & 1)))) {
+            if (tid == 0) atomicExch(a.err, 1);
+            ok = false;
+            break;
+        }
+        // stage 0 on the CUDA cores: the slot into registers, then the
+        // Stockham tile written over it
+        const float2* src = reinterpret_cast<const float2*>(ring + s * SLOT);
+        float2* tile = reinterpret_cast<float2*>(ring + s * SLOT);
+        float2 x[K][R0];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int q = tid + k * THREADS;
+            if (EXACT || q < NBT) {
+                int b, j;
+                bf_map<BFAST0, B, NBL>(q, b, j);
+#pragma unroll
+                for (int r = 0; r < R0; ++r) {
+                    const int n = j + r * NBL;
+                    if constexpr (MODE == MODE_BATCH) {
+                        x[k][r] = src[n * B + b];
+                    } else {  // [z chunk][b][z within the chunk]
+                        int q2, zl;
+                        if (m.chunk_shift >= 0) {
+                            q2 = n >> m.chunk_shift;
+                            zl = n & (m.chunk - 1);
+                        } else {
+                            q2 = n / m.chunk;
+                            zl = n - q2 * m.chunk;
+                        }
+                        x[k][r] = src[(q2 * B + b) * m.chunk + zl];
+                    }
+                }
+            }
+        }
+        __syncthreads();  // every read of the slot before it is rewritten
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int q = tid + k * THREADS;
+            if (EXACT || q < NBT) {
+                int b, j;
+                bf_map<BFAST0, B, NBL>(q, b, j);
+                Dft<R0, INV, float2>::run(x[k]);
+#pragma unroll
+                for (int r = 0; r < R0; ++r) tile[G::idx(b, j * R0 + r)] = x[k][r];
+            }
+        }
+        __syncthreads();
+        if (!tc_stage<PLAN, B, THREADS, MODE, INV, FMT, 1, false>(a, tile, tw, offA_s, base_s, ctx, tid, ubase, v0)) {
+            ok = false;
+            ++i;  // tile i's copy has landed
+            break;
+        }
+        // the last stage read the slot (tc_stage ends with a block barrier):
+        // refill it with the tile NSTG ahead
+        if (tid == 0 && issued < mine) {
+            fence_proxy_async_smem();  // the generic accesses of the slot come before the async writes
+            tmat_issue<float, B, N>(m, blockIdx.x + issued * gridDim.x, tilesV, ring + s * SLOT, rbar + s);
+            ++issued;
+        }
+    }
+    if (!ok && tid == 0)  // wait (bounded) for this CTA's copies still in flight before leaving
+        for (int j = i; j < issued; ++j) mbar_wait_bounded(rbar + j % NSTG, (uint32_t)((j / NSTG) & 1));
+    __syncthreads();
+    // after an abandoned stage whose MMAs were never seen to finish, the
+    // columns stay allocated (see fft_tc_kernel)
+    if (!ctx.drained) return;
     tc_fence_after();
     if (tid < 32)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(ctx.tmem), "r"(TCOLS)

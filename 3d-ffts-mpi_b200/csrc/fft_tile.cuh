@@ -458,7 +458,8 @@ enum PassKind : int {
     KIND_TMAT2 = 5,   // persistent CTAs, whole tiles fetched by TMA tensor copies into a 2-slot ring
     KIND_TMAT3 = 6,   // the same with a 3-slot ring
     KIND_TMAT2W = 7,  // the 2-slot ring with the length's two-stage wide-radix plan (radix 16/32)
-    KIND_TMATI = 8    // the 2-slot ring with each slot transformed in place (no separate tile)
+    KIND_TMATI = 8,   // the 2-slot ring with each slot transformed in place (no separate tile)
+    KIND_TCR = 9      // tensor-core stages, persistent CTAs fed by the in-place 2-slot TMA ring
 };
 
 constexpr int kTmaBuffers = 2;

@@ -52,6 +52,42 @@ def test_split_with_tones(pkg, oracle, cuda, method):
     assert oracle.rel_l2(inv, g) <= 2 * TOL[method]
 
 
+@pytest.mark.parametrize("method", ["split_fp16", "split_bf16"])
+@pytest.mark.parametrize("P,shape", [(4, 64), (16, 128), (16, (512, 64, 64)), (4, (64, 64, 512)),
+                                     (4, (64, 1024, 64)), (4, (32, 64, 1024))])
+def test_split_both_kernel_forms(pkg, oracle, cuda, P, shape, method):
+    """Each tensor-core kernel form -- one tile per CTA, and the persistent
+    form fed by the TMA ring -- on every pass gives the FP64 oracle's
+    transform (relative L2 <= 1e-6)."""
+    import torch
+
+    shape = (shape,) * 3 if isinstance(shape, int) else tuple(shape)
+    dist = pkg.a2aDistribution(P, shape, 64, precision="c64")
+    d = oracle.Decomp(shape, P)
+    g = oracle.make_input("uniform", shape, seed=21, dtype=np.complex64, tones=2)
+    x0 = torch.from_numpy(oracle.global_to_bricks(g, d).ravel()).to(cuda)
+    ref = oracle.fft3_fp64(g)
+    f = pkg.a2adfft(dist, method=method)
+    f.make_plans()
+    assert f.variant_count(0) == 2
+    tested = 0
+    for form in (0, 1):
+        for p in range(3):
+            try:
+                f.select_variant(p, form)
+            except pkg.A2AError:
+                assert form == 1  # the ring form does not fit every geometry
+                f.select_variant(p, 0)
+        x = x0.clone()
+        f.forward(x)
+        fwd = oracle.bricks_to_global(x.cpu().numpy().reshape(P, -1), d)
+        assert oracle.rel_l2(fwd, ref) <= TOL[method], f"form {form}"
+        f.inverse(x)
+        assert oracle.rel_l2(x.cpu().numpy(), x0.cpu().numpy()) <= 2 * TOL[method], f"form {form} round trip"
+        tested += 1
+    assert tested == 2
+
+
 def test_split_rejects_double_and_unsupported_lengths(pkg, cuda):
     with pytest.raises(pkg.A2AError) as e:
         pkg.a2adfft(pkg.a2aDistribution(4, 64, 64, precision="c128"), method="split_fp16")
