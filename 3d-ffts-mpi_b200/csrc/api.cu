@@ -780,6 +780,12 @@ a2a_status setup_tc(a2a_dfft* f, a2a_method m) {
             A2A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&f->tcv_occ[p][c], f->tcv[p][0][c].fn,
                                                                    f->tcv[p][0][c].threads, f->tcv[p][0][c].smem),
                      "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+            // tensor memory holds 512 columns per SM: a persistent CTA that
+            // waited for columns would only start once another one finished
+            const int need = (f->tcv[p][0][c].threads / a2a::kTcRows) * a2a::tc_block_cols(fmt);
+            int cols = 32;
+            while (cols < need) cols *= 2;
+            f->tcv_occ[p][c] = std::min(f->tcv_occ[p][c], 512 / cols);
             if (f->tcv_occ[p][c] < 1) f->tcv_fits[p][c] = false;
         }
         if (!f->tcv_fits[p][0] && !f->tcv_fits[p][1])
