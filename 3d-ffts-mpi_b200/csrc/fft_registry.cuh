@@ -75,7 +75,9 @@ template <typename T, int N> struct PlanOf<T, N, KIND_TMAT2W> { using Plan = typ
 // Launch variants X(T, N, KIND, B lines per tile, THREADS, MINB, LPT).  The first
 // entry per N is the default; make_plans can time the others on the scratch
 // buffer and keep the fastest (a2a_dfft_make_plans).  DIRECT tiles are about
-// 32-64 KB so two or three CTAs share an SM; PIPE CTAs hold two tiles.
+// 32-64 KB so two or three CTAs share an SM; PIPE CTAs hold two tiles.  LPT =
+// 2 (complex float, batch mode): a thread moves two adjacent lines as one
+// 16-byte access, which halves the shared-memory instructions of a tile.
 #define A2A_VARIANTS_F32(X)                            \
     X(float,    4, KIND_DIRECT,  4,  32, 1, 1)      \
     X(float,    8, KIND_DIRECT,  8,  32, 1, 1)      \
@@ -176,7 +178,14 @@ template <typename T, int N> struct PlanOf<T, N, KIND_TMAT2W> { using Plan = typ
     X(float, 1024, KIND_TMAT2W,  8, 256, 1, 1)      \
     X(float, 1024, KIND_TMAT2W,  4, 128, 2, 1)      \
     X(float,  768, KIND_TMAT2,   4, 128, 3, 1)      \
-    X(float,  768, KIND_TMATI,   8, 256, 2, 1)
+    X(float,  768, KIND_TMATI,   8, 256, 2, 1)      \
+    X(float,  256, KIND_TMAT2,  16, 128, 3, 2)      \
+    X(float,  512, KIND_TMAT2,   8, 128, 3, 2)      \
+    X(float,  512, KIND_TMAT2,   8, 256, 2, 2)      \
+    X(float,  512, KIND_TMATI,   8, 128, 3, 2)      \
+    X(float,  512, KIND_TMAT3,   8, 128, 2, 2)      \
+    X(float, 1024, KIND_TMAT2,   4, 128, 2, 2)      \
+    X(float, 1024, KIND_TMATI,   4, 128, 3, 2)
 
 #define A2A_VARIANTS_F64(X)                         \
     X(double,    4, KIND_DIRECT,  4,  32, 1, 1)     \
