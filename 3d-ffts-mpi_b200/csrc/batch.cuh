@@ -257,16 +257,21 @@ __device__ __forceinline__ void prefetch_tile(const BatchBox& bx, int pass, int 
 // previous pass of its box done) once per (box, pass) change, with an acquire
 // fence after the wait, and publishes finished tiles per (box, pass) with a
 // release (fence, then one counter increment).  It
-// publishes before it waits and before it takes more items, so a CTA never
-// waits while holding unpublished tiles; an item waits only on items taken
-// before it, so the lowest unfinished taken item always runs and the waits
-// end.
+// publishes before it waits, so a CTA never waits while holding unpublished
+// tiles.  Thread 0 takes its claims one ahead (the next claim is taken when
+// the current one starts), so a CTA's claims are consecutive in the queue
+// order and it runs them in that order: an item waits only on items taken
+// before it, and the lowest unfinished taken item is always the current run
+// of the CTA holding it, so it always runs and the waits end.
 template <typename T, bool INV>
 __global__ void __launch_bounds__(kBatchThreads, 2) fft_batch_kernel(const BatchArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_box, s_pass, s_tile, s_count, s_nbox, s_npass, s_ntile;
     const int tid = threadIdx.x;
     int next = 0, end = 0;           // thread 0: taken items not yet run
+    // thread 0: the claim after [next, end), taken one claim ahead so that
+    // its queue round trip overlaps the current run (-1: none yet)
+    int pre_lo = -1, pre_n = 0;
     int ok_box = -1, ok_pass = -1;   // thread 0: last dependency seen complete
     int pend_box = 0, pend_pass = 0, pend = 0;  // thread 0: finished, unpublished tiles
     auto publish = [&]() {
@@ -279,14 +284,24 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fft_batch_kernel(const Batch
     for (;;) {
         if (tid == 0) {
             int count = -1, box = 0, pass = 0, tile = 0, nbox = -1, npass = 0, ntile = 0;
+            // guided claims: up to `claim` items, fewer as the queue drains,
+            // so the last runs end close together; the items left are
+            // estimated from the queue position this CTA last saw (no read
+            // of the counter, whose round trip would not overlap anything)
+            auto claim = [&](int seen, int& lo, int& n) {
+                const int left = a.item_hi - seen;
+                n = max(1, min(a.claim, left / (2 * (int)gridDim.x)));
+                lo = a.item_lo + atomicAdd(a.taken, n);
+            };
             if (next >= end) {
                 if (a.fused) publish();
-                // guided claims: up to `claim` items, fewer as the queue
-                // drains, so the last runs end close together
-                const int left = (a.item_hi - a.item_lo) - *reinterpret_cast<volatile int*>(a.taken);
-                const int c = max(1, min(a.claim, left / (2 * (int)gridDim.x)));
-                next = a.item_lo + atomicAdd(a.taken, c);
-                end = next + c;
+                if (pre_lo < 0) claim(a.item_lo, pre_lo, pre_n);  // first claim of this CTA
+                next = pre_lo;
+                end = pre_lo + pre_n;
+                // the following claim: its result is not read before this
+                // claim's items have run
+                if (next < a.item_hi) claim(end, pre_lo, pre_n);
+                else pre_lo = a.item_hi;
             }
             const int i = next;
             if (i < a.item_hi && !*reinterpret_cast<volatile int*>(a.abort)) {
