@@ -54,7 +54,7 @@ def test_split_with_tones(pkg, oracle, cuda, method):
 
 @pytest.mark.parametrize("method", ["split_fp16", "split_bf16"])
 @pytest.mark.parametrize("P,shape", [(4, 64), (16, 128), (16, (512, 64, 64)), (4, (64, 64, 512)),
-                                     (4, (64, 1024, 64)), (4, (32, 64, 1024))])
+                                     (4, (64, 1024, 64)), (4, (64, 64, 1024))])
 def test_split_both_kernel_forms(pkg, oracle, cuda, P, shape, method):
     """Each tensor-core kernel form -- one tile per CTA, and the persistent
     form fed by the TMA ring -- on every pass gives the FP64 oracle's
