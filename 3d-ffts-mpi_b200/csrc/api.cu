@@ -773,10 +773,18 @@ a2a_status setup_tc(a2a_dfft* f, a2a_method m) {
         for (int c = 0; c < 2; ++c) {
             f->tcv_ms[p][c] = 0.f;
             if (!f->tcv_fits[p][c]) continue;
-            for (int inv = 0; inv < 2; ++inv)
+            for (int inv = 0; inv < 2; ++inv) {
                 A2A_CUDA(cudaFuncSetAttribute(f->tcv[p][inv][c].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               (int)f->tcv[p][inv][c].smem),
                          "cudaFuncSetAttribute");
+                // the ring form's tiles arrive by TMA, not through L1: give
+                // the SM's unified memory to shared memory, so that two rings
+                // fit per SM
+                if (c == 1)
+                    A2A_CUDA(cudaFuncSetAttribute(f->tcv[p][inv][c].fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                                  100),
+                             "cudaFuncSetAttribute");
+            }
             A2A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&f->tcv_occ[p][c], f->tcv[p][0][c].fn,
                                                                    f->tcv[p][0][c].threads, f->tcv[p][0][c].smem),
                      "cudaOccupancyMaxActiveBlocksPerMultiprocessor");

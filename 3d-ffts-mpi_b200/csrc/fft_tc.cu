@@ -13,9 +13,17 @@ template <> struct TcPlan<256> { using Plan = RadixPlan<16, 16>; static constexp
 template <> struct TcPlan<512> { using Plan = RadixPlan<2, 16, 16>; static constexpr int B = 8; };
 template <> struct TcPlan<1024> { using Plan = RadixPlan<4, 16, 16>; static constexpr int B = 4; };
 
+// Tile height: bf16 rows take 80 tensor-memory columns per 128-row block (three
+// A parts), so its 256-thread tiles are halved to one block (128 columns per
+// CTA, four CTAs per SM instead of two) where that still leaves whole blocks.
+template <int N, int FMT> constexpr int tc_lines() {
+    constexpr int B = TcPlan<N>::B;
+    return (FMT == TC_BF16 && B * N / 16 >= 2 * kTcRows) ? B / 2 : B;
+}
+
 template <int N, int MODE, bool INV, int FMT, bool RING> PassKernel make_tc_kernel() {
     using P = typename TcPlan<N>::Plan;
-    constexpr int B = TcPlan<N>::B;
+    constexpr int B = tc_lines<N, FMT>();
     PassKernel k;
     if constexpr (RING) {
         k.fn = reinterpret_cast<const void*>(&fft_tc_ring_kernel<P, B, MODE, INV, FMT>);

@@ -6,8 +6,9 @@
 // One radix-16 butterfly is y = F16 x with F16 the 16-point DFT matrix.  As a
 // real GEMM row: [y_re | y_im] = [x_re | x_im] R with the 32 x 32 matrix
 //   R = [[C, S], [-S, C]],  C = cos(2 pi r k / 16),  S = -+ sin(2 pi r k / 16).
-// Both operands are split into 16-bit parts after scaling each row by a power
-// of two into [-1, 1); R is split on the host from FP64 values.
+// Both operands are split into 16-bit parts (fp16 rows first scaled by a power
+// of two into [-1, 1), which bf16's 8-bit exponent does not need); R is split
+// on the host from FP64 values.
 //   fp16 (11-bit significands): x = xh + xl, R = Rh + Rl, and the product
 //     keeps xh Rh + xh Rl + xl Rh (xl Rl is below FP32 rounding): 22 bits.
 //   bf16 (8-bit significands): two parts carry only 16 bits, which leaves a
@@ -58,19 +59,25 @@ __host__ __device__ constexpr uint32_t umma_idesc_f16(int fmt) {
     return (1u << 4) | ((uint32_t)fmt << 7) | ((uint32_t)fmt << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
 }
 
-// v = p[0] + p[1] (+ p[2]) in 16-bit parts, each the rounding of what the
-// previous parts leave.
-template <int FMT> __device__ __forceinline__ void split16(float v, uint16_t (&p)[tc_parts(FMT)]) {
+// (a, b) = w[0] + w[1] (+ w[2]) in 16-bit parts, a in the low and b in the
+// high half of each 32-bit word (the A operand's layout: two consecutive K
+// values per tensor-memory column); each part is the rounding of what the
+// previous parts leave, converted two at a time.
+template <int FMT> __device__ __forceinline__ void split_pair(float a, float b, uint32_t (&w)[tc_parts(FMT)]) {
 #pragma unroll
     for (int i = 0; i < tc_parts(FMT); ++i) {
         if constexpr (FMT == TC_FP16) {
-            const __half h = __float2half_rn(v);
-            p[i] = __half_as_ushort(h);
-            v -= __half2float(h);
+            const __half2 h = __floats2half2_rn(a, b);
+            w[i] = *reinterpret_cast<const uint32_t*>(&h);
+            const float2 f = __half22float2(h);
+            a -= f.x;
+            b -= f.y;
         } else {
-            const __nv_bfloat16 h = __float2bfloat16_rn(v);
-            p[i] = __bfloat16_as_ushort(h);
-            v -= __bfloat162float(h);
+            const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+            w[i] = *reinterpret_cast<const uint32_t*>(&h);
+            const float2 f = __bfloat1622float2(h);
+            a -= f.x;
+            b -= f.y;
         }
     }
 }
@@ -187,15 +194,20 @@ __device__ __forceinline__ bool tc_stage(const PassArgs<float>& a, float2* tile,
 #pragma unroll
         for (int r = 1; r < 16; ++r) x[r] = cmulw<INV>(x[r], tw[TWO + (r - 1) * NS + m]);
     }
-    // scale the row into [-1, 1) by a power of two: e = exponent of the largest
-    // component (as frexp would give it), scale factors built from exponent bits
-    float mx = 0.f;
+    // fp16 (5-bit exponent): scale the row into [-1, 1) by a power of two,
+    // e = exponent of the largest component (as frexp would give it), scale
+    // factors built from exponent bits.  bf16 has FP32's exponent range and
+    // needs no scaling.
+    float down = 1.f, up = 1.f;
+    if constexpr (FMT == TC_FP16) {
+        float mx = 0.f;
 #pragma unroll
-    for (int r = 0; r < 16; ++r) mx = fmaxf(mx, fmaxf(fabsf(x[r].x), fabsf(x[r].y)));
-    int e = ((__float_as_int(mx) >> 23) & 0xFF) - 126;
-    e = mx > 0.f ? min(max(e, -125), 126) : 0;
-    const float down = __int_as_float((127 - e) << 23);  // 2^-e
-    const float up = __int_as_float((127 + e) << 23);    // 2^e
+        for (int r = 0; r < 16; ++r) mx = fmaxf(mx, fmaxf(fabsf(x[r].x), fabsf(x[r].y)));
+        int e = ((__float_as_int(mx) >> 23) & 0xFF) - 126;
+        e = mx > 0.f ? min(max(e, -125), 126) : 0;
+        down = __int_as_float((127 - e) << 23);  // 2^-e
+        up = __int_as_float((127 + e) << 23);    // 2^e
+    }
     const int warp = tid / 32;
     const uint32_t lane_row = ((uint32_t)((warp % 4) * 32) << 16) + (uint32_t)((warp / 4) * BCOLS);
     {
@@ -205,15 +217,13 @@ __device__ __forceinline__ bool tc_stage(const PassArgs<float>& a, float2* tile,
         uint32_t w[16 * NP];
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
-            uint16_t r0[NP], r1[NP], i0[NP], i1[NP];
-            split16<FMT>(x[2 * i].x * down, r0);
-            split16<FMT>(x[2 * i + 1].x * down, r1);
-            split16<FMT>(x[2 * i].y * down, i0);
-            split16<FMT>(x[2 * i + 1].y * down, i1);
+            uint32_t pr[NP], pi[NP];
+            split_pair<FMT>(x[2 * i].x * down, x[2 * i + 1].x * down, pr);
+            split_pair<FMT>(x[2 * i].y * down, x[2 * i + 1].y * down, pi);
 #pragma unroll
             for (int q = 0; q < NP; ++q) {
-                w[16 * q + i] = r0[q] | (uint32_t(r1[q]) << 16);
-                w[16 * q + 8 + i] = i0[q] | (uint32_t(i1[q]) << 16);
+                w[16 * q + i] = pr[q];
+                w[16 * q + 8 + i] = pi[q];
             }
         }
         if constexpr (NP == 2) {

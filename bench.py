@@ -747,7 +747,8 @@ def run_ours(args, rank, world, local_rank):
             "per_pass_ms": {n: round(v, 4) for n, v in zip(PASS_NAMES, mm)},
             "roofline": method_roofline(mm, ng, esz, prec, peak, peak_kind, m),
             "rel_l2_vs_fp64": acc[m]["rel_l2_vs_fp64"], "roundtrip_rel_l2": acc[m]["roundtrip_rel_l2"],
-            "plan": [ln for ln in f.plan_report().splitlines() if "chosen" in ln],
+            "plan": [ln for ln in f.plan_report().splitlines()
+                     if ("in use" in ln if m != "plain" else "chosen" in ln)],
             "clocks": ck, "gpu_launches": 6 * args.steps,
         }
     line = {
