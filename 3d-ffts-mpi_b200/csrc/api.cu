@@ -785,15 +785,30 @@ a2a_status setup_tc(a2a_dfft* f, a2a_method m) {
                                                   100),
                              "cudaFuncSetAttribute");
             }
-            A2A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&f->tcv_occ[p][c], f->tcv[p][0][c].fn,
-                                                                   f->tcv[p][0][c].threads, f->tcv[p][0][c].smem),
-                     "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-            // tensor memory holds 512 columns per SM: a persistent CTA that
-            // waited for columns would only start once another one finished
-            const int need = (f->tcv[p][0][c].threads / a2a::kTcRows) * a2a::tc_block_cols(fmt);
+            // resident CTAs per SM, counted from the kernel's registers and
+            // shared memory and the SM's limits (the runtime's occupancy
+            // query answers 1 for these tensor-memory kernels although four
+            // one-tile CTAs are resident per SM), and from tensor memory: an
+            // SM has 512 columns, and a persistent CTA that waited for
+            // columns would only start once another one finished
+            const PassKernel& kk = f->tcv[p][0][c];
+            cudaFuncAttributes fa;
+            A2A_CUDA(cudaFuncGetAttributes(&fa, kk.fn), "cudaFuncGetAttributes");
+            int dev = 0, smem_sm = 0, smem_rsv = 0, regs_sm = 0, thr_sm = 0;
+            A2A_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+            A2A_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev), "attr");
+            A2A_CUDA(cudaDeviceGetAttribute(&smem_rsv, cudaDevAttrReservedSharedMemoryPerBlock, dev), "attr");
+            A2A_CUDA(cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev), "attr");
+            A2A_CUDA(cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev), "attr");
+            const size_t smem_cta = kk.smem + fa.sharedSizeBytes + (size_t)smem_rsv;
+            const int regs_warp = (fa.numRegs * 32 + 255) / 256 * 256;  // allocated per warp, 256 at a time
+            const int by_smem = (int)((size_t)smem_sm / smem_cta);
+            const int by_regs = regs_sm / (regs_warp * (kk.threads / 32));
+            const int by_thr = thr_sm / kk.threads;
+            const int need = (kk.threads / a2a::kTcRows) * a2a::tc_block_cols(fmt);
             int cols = 32;
             while (cols < need) cols *= 2;
-            f->tcv_occ[p][c] = std::min(f->tcv_occ[p][c], 512 / cols);
+            f->tcv_occ[p][c] = std::min(std::min(by_smem, by_regs), std::min(by_thr, 512 / cols));
             if (f->tcv_occ[p][c] < 1) f->tcv_fits[p][c] = false;
         }
         if (!f->tcv_fits[p][0] && !f->tcv_fits[p][1])
