@@ -65,11 +65,12 @@ template <typename T, int N, int B, int TH, int MB> PassKernel mb_pick(int mode,
 // Persistent register-pipelined configurations (N, lines, threads, min
 // blocks, lines per thread in batch mode): the single-buffer registry's
 // register-pipelined tiles for the long lengths.
-// Line mode (the Z pass) and batch mode (X, Y) have their own entries.
-#define A2A_MB_RPIPE_F32_LINE(X) \
+// Line mode (the Z pass) only: at 512^3 on one GPU the persistent body took
+// the Z pass from 0.50 to 0.46 ms but was slower than one tile per CTA in
+// batch mode (X, Y: 0.60-0.65 vs 0.57 ms), so batch-mode passes keep the
+// one-tile body.
+#define A2A_MB_RPIPE_F32(X) \
     X(256, 16, 256, 2, 1) X(512, 8, 256, 2, 1) X(1024, 4, 256, 2, 1)
-#define A2A_MB_RPIPE_F32_BATCH(X) \
-    X(256, 16, 256, 2, 1) X(512, 8, 128, 4, 1) X(1024, 4, 256, 2, 1)
 #define A2A_MB_RPIPE_F64(X) \
     X(512, 8, 512, 1, 1) X(1024, 4, 256, 1, 1)
 
@@ -86,12 +87,11 @@ bool find_mb_rpipe_kernel(a2a_precision prec, int n, int mode, bool inverse, Pas
     }
 #define A2A_MB_F32_CASE(N_, B_, TH_, MB_, LPT_) A2A_MB_CASE(float, N_, B_, TH_, MB_, LPT_)
 #define A2A_MB_F64_CASE(N_, B_, TH_, MB_, LPT_) A2A_MB_CASE(double, N_, B_, TH_, MB_, LPT_)
+    if (mode != MODE_LINE) return false;
     if (prec == A2A_C128) {
         A2A_MB_RPIPE_F64(A2A_MB_F64_CASE)
-    } else if (mode == MODE_LINE) {
-        A2A_MB_RPIPE_F32_LINE(A2A_MB_F32_CASE)
     } else {
-        A2A_MB_RPIPE_F32_BATCH(A2A_MB_F32_CASE)
+        A2A_MB_RPIPE_F32(A2A_MB_F32_CASE)
     }
 #undef A2A_MB_F32_CASE
 #undef A2A_MB_F64_CASE

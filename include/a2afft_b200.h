@@ -276,9 +276,11 @@ a2a_status a2a_dfft_execute_pass_blocks(a2a_dfft* dfft, void** blocks, int nbloc
 
 /* The kernel body a2a_dfft_execute_pass_blocks uses: 1 (default) one wave of
  * persistent CTAs per call, each working through its share of the part's
- * tiles with the next tile's gathers in flight in registers (lengths 256,
- * 512, 1024 complex float; 512, 1024 complex double), else 0: one tile per
- * CTA.  Both give the same result.  No reference counterpart. */
+ * tiles with the next tile's gathers in flight in registers (the Z pass at
+ * lengths 256, 512, 1024 complex float and 512, 1024 complex double; the
+ * other passes keep one tile per CTA, which measured faster there), else 0:
+ * one tile per CTA everywhere.  Both give the same result.  No reference
+ * counterpart. */
 a2a_status a2a_dfft_set_blocks_kernel(a2a_dfft* dfft, int persistent);
 
 /* Sharing a device buffer with another process (CUDA IPC): export writes an
