@@ -37,7 +37,7 @@ def _transform(dfft, blocks, inverse, nparts):
                                              (4, (64, 128, 32), 4, 2), (16, (96, 64, 192), 2, 1), (16, (96, 48, 192), 2, 1),
                                              # long lines for the persistent kernels (512, 1024)
                                              (16, (512, 64, 128), 4, 3), (4, (64, 1024, 32), 2, 2),
-                                             (4, (32, 64, 512), 2, 3), (4, (16, 32, 1024), 4, 2)])
+                                             (4, (32, 64, 512), 2, 3), (4, (32, 64, 1024), 4, 2)])
 def test_multiblock_passes_vs_oracle(pkg, oracle, cuda, P, shape, G, nparts, prec, persistent):
     import torch
 
