@@ -152,56 +152,47 @@ template <class PLAN, int B, int MODE> __host__ __device__ constexpr int tc_tile
     return MODE == MODE_BATCH ? tile_swizzle_shift<PLAN, B, (int)sizeof(float2)>() : -1;
 }
 
-// Geometry of tensor-core stage s of a tile of B lines with THREADS threads:
-// thread q owns butterfly q, i.e. A row q % 128 of block q / 128.
-template <class PLAN, int B, int THREADS, int MODE, int s, bool SRC_GLOBAL> struct TcStageGeom {
-    static constexpr int N = PLAN::N;
-    static constexpr int R = PLAN::r[s];
-    static_assert(R == 16, "tensor-core stages are radix 16");
-    static constexpr int NS = PLAN::ns(s);
-    static constexpr int NBL = N / R;
-    static_assert(B * NBL == THREADS, "one butterfly per thread in a tensor-core stage");
-    static constexpr int NBLK = THREADS / kTcRows;
-    static_assert(THREADS % kTcRows == 0, "whole 128-row MMA blocks");
-    static constexpr bool LAST = (s == PLAN::S - 1);
-    static constexpr bool BFAST = (MODE == MODE_BATCH) || !(LAST || SRC_GLOBAL);
-    static constexpr int TWO = PLAN::twoff(s);
-};
-
-__device__ __forceinline__ uint32_t tc_lane_row(int tid, int bcols) {
-    const int warp = tid / 32;
-    return ((uint32_t)((warp % 4) * 32) << 16) + (uint32_t)((warp / 4) * bcols);
-}
-
-// First half of a tensor-core stage: this thread's butterfly inputs (from the
-// tile, or from global memory for a first stage), the stage twiddles, the
-// row scale (fp16), the split A row into tensor memory, a block barrier, and
-// thread 0 issues the block's MMAs and commits them to ctx.bar.  Returns the
-// factor that undoes the row scale.
+// One radix-16 stage on the tensor cores.  THREADS == butterflies per stage;
+// thread q owns butterfly q, i.e. A row q % 128 of block q / 128.  Returns
+// false when the MMA completion wait gave up (the device error flag is then
+// set, the rest of the pass is skipped, and ctx.drained says whether the
+// stage's MMAs were seen to finish by a second bounded wait, i.e. whether the
+// tensor memory may be freed).
 template <class PLAN, int B, int THREADS, int MODE, bool INV, int FMT, int s, bool SRC_GLOBAL>
-__device__ __forceinline__ float tc_front(const PassArgs<float>& a, const float2* tile, const float2* tw,
-                                          const TcCtx& ctx, int tid, size_t ubase, int v0) {
-    using SG = TcStageGeom<PLAN, B, THREADS, MODE, s, SRC_GLOBAL>;
+__device__ __forceinline__ bool tc_stage(const PassArgs<float>& a, float2* tile, const float2* tw,
+                                         const uint32_t* offA_s, const size_t* base_s, TcCtx& ctx, int tid,
+                                         size_t ubase, int v0) {
     using G = TileGeom<MODE, B, PLAN::N, sizeof(float2), tc_tile_swizzle<PLAN, B, MODE>()>;
+    constexpr int N = PLAN::N;
+    constexpr int R = PLAN::r[s];
+    static_assert(R == 16, "tensor-core stages are radix 16");
+    constexpr int NS = PLAN::ns(s);
+    constexpr int NBL = N / R;
+    static_assert(B * NBL == THREADS, "one butterfly per thread in a tensor-core stage");
+    constexpr int NBLK = THREADS / kTcRows;
+    static_assert(THREADS % kTcRows == 0, "whole 128-row MMA blocks");
+    constexpr bool LAST = (s == PLAN::S - 1);
+    constexpr bool BFAST = (MODE == MODE_BATCH) || !(LAST || SRC_GLOBAL);
+    constexpr int TWO = PLAN::twoff(s);
     constexpr int NP = tc_parts(FMT);
     constexpr int BCOLS = tc_block_cols(FMT);
     constexpr int ACC = tc_acc_col(FMT);
 
     int b, j;
-    bf_map<SG::BFAST, B, SG::NBL>(tid, b, j);
+    bf_map<BFAST, B, NBL>(tid, b, j);
     float2 x[16];
     if constexpr (SRC_GLOBAL) {
         const float2* line = a.src + ubase + __ldg(a.offV + v0 + b);
 #pragma unroll
-        for (int r = 0; r < 16; ++r) x[r] = ld_stream(line + __ldg(a.offA + j + r * SG::NBL));
+        for (int r = 0; r < 16; ++r) x[r] = ld_stream(line + __ldg(a.offA + j + r * NBL));
     } else {
 #pragma unroll
-        for (int r = 0; r < 16; ++r) x[r] = tile[G::idx(b, j + r * SG::NBL)];
+        for (int r = 0; r < 16; ++r) x[r] = tile[G::idx(b, j + r * NBL)];
     }
-    const int m = j % SG::NS;
+    const int m = j % NS;
     if constexpr (s > 0) {
 #pragma unroll
-        for (int r = 1; r < 16; ++r) x[r] = cmulw<INV>(x[r], tw[SG::TWO + (r - 1) * SG::NS + m]);
+        for (int r = 1; r < 16; ++r) x[r] = cmulw<INV>(x[r], tw[TWO + (r - 1) * NS + m]);
     }
     // fp16 (5-bit exponent): scale the row into [-1, 1) by a power of two,
     // e = exponent of the largest component (as frexp would give it), scale
@@ -217,7 +208,8 @@ __device__ __forceinline__ float tc_front(const PassArgs<float>& a, const float2
         down = __int_as_float((127 - e) << 23);  // 2^-e
         up = __int_as_float((127 + e) << 23);    // 2^e
     }
-    const uint32_t lane_row = tc_lane_row(tid, BCOLS);
+    const int warp = tid / 32;
+    const uint32_t lane_row = ((uint32_t)((warp % 4) * 32) << 16) + (uint32_t)((warp / 4) * BCOLS);
     {
         // the row into this warp's lanes of its block's A columns: part q at
         // columns 16q..16q+15 (real values k, k+1 in the low and high half of
@@ -251,7 +243,7 @@ __device__ __forceinline__ float tc_front(const PassArgs<float>& a, const float2
         auto bre = [&](int q) { return umma_smem_desc(ctx.b_addr + q * kTcMatB, kTcChunkB, 128); };
         auto bim = [&](int q) { return umma_smem_desc(ctx.b_addr + q * kTcMatB + 2 * kTcChunkB, kTcChunkB, 128); };
 #pragma unroll
-        for (int blk = 0; blk < SG::NBLK; ++blk) {
+        for (int blk = 0; blk < NBLK; ++blk) {
             const uint32_t ab = ctx.tmem + blk * BCOLS;  // lane 0 of the block's A columns
             const uint32_t dacc = ab + ACC;
             // one term x_p R_q: the real and the imaginary half of K
@@ -276,73 +268,36 @@ __device__ __forceinline__ float tc_front(const PassArgs<float>& a, const float2
         }
         tc_commit(ctx.bar);
     }
-    return up;
-}
-
-// The bounded wait for the stage's MMAs.  False when it gave up: the device
-// error flag is raised and ctx.drained says whether a second bounded wait saw
-// the MMAs finish, i.e. whether the tensor memory may be freed.
-__device__ __forceinline__ bool tc_wait(const PassArgs<float>& a, TcCtx& ctx, int tid) {
     const bool ok = mbar_wait_bounded(ctx.bar, ctx.phase);
     if (__syncthreads_or(!ok)) {
+        // the MMAs did not complete in time: flag it, skip the rest of the
+        // pass, and look once more (bounded) for their completion before the
+        // caller may free the tensor memory they write
         if ((tid % 32) == 0) atomicExch(a.err, 1);
         ctx.drained = __syncthreads_and(mbar_wait_bounded(ctx.bar, ctx.phase)) != 0;
         return false;
     }
     ctx.phase ^= 1u;
     tc_fence_after();
-    return true;
-}
-
-// Second half of a stage, after tc_wait: the accumulator row back into
-// registers, the row scale undone, and the 16 outputs written to the tile
-// (Stockham position) or, for the last stage, to global memory.
-template <class PLAN, int B, int THREADS, int MODE, int FMT, int s, bool SRC_GLOBAL>
-__device__ __forceinline__ void tc_back(const PassArgs<float>& a, float2* tile, const uint32_t* offA_s,
-                                        const size_t* base_s, const TcCtx& ctx, int tid, float up) {
-    using SG = TcStageGeom<PLAN, B, THREADS, MODE, s, SRC_GLOBAL>;
-    using G = TileGeom<MODE, B, PLAN::N, sizeof(float2), tc_tile_swizzle<PLAN, B, MODE>()>;
-    int b, j;
-    bf_map<SG::BFAST, B, SG::NBL>(tid, b, j);
     float y[32];
-    tc_ld32(ctx.tmem + tc_lane_row(tid, tc_block_cols(FMT)) + tc_acc_col(FMT), y);
-    float2 x[16];
+    tc_ld32(ctx.tmem + lane_row + ACC, y);
 #pragma unroll
     for (int k = 0; k < 16; ++k) x[k] = make_float2(y[k] * up, y[16 + k] * up);
-    if constexpr (SG::LAST) {
+    if constexpr (LAST) {
         float2* line = a.dst + base_s[b];
 #pragma unroll
-        for (int r = 0; r < 16; ++r) st_stream(line + offA_s[j + r * SG::NBL], scl(x[r], a.scale));
+        for (int r = 0; r < 16; ++r) st_stream(line + offA_s[j + r * NBL], scl(x[r], a.scale));
     } else {
-        const int m = j % SG::NS;
-        const int jd = (j / SG::NS) * SG::NS * SG::R + m;
+        const int jd = (j / NS) * NS * R + m;
 #pragma unroll
-        for (int r = 0; r < 16; ++r) tile[G::idx(b, jd + r * SG::NS)] = x[r];
+        for (int r = 0; r < 16; ++r) tile[G::idx(b, jd + r * NS)] = x[r];
     }
-}
-
-// Tensor-core stages s .. S-1 (STOP: s .. S-2, leaving the last stage to the
-// caller), each a full round trip ending in a block barrier.  Returns false
-// when an MMA completion wait gave up (see tc_wait; the rest of the pass is
-// then skipped).
-template <class PLAN, int B, int THREADS, int MODE, bool INV, int FMT, int s, bool SRC_GLOBAL, bool STOP = false>
-__device__ __forceinline__ bool tc_stage(const PassArgs<float>& a, float2* tile, const float2* tw,
-                                         const uint32_t* offA_s, const size_t* base_s, TcCtx& ctx, int tid,
-                                         size_t ubase, int v0) {
-    constexpr bool LAST = (s == PLAN::S - 1);
-    if constexpr (STOP && LAST) {
-        return true;
-    } else {
-        const float up = tc_front<PLAN, B, THREADS, MODE, INV, FMT, s, SRC_GLOBAL>(a, tile, tw, ctx, tid, ubase, v0);
-        if (!tc_wait(a, ctx, tid)) return false;
-        tc_back<PLAN, B, THREADS, MODE, FMT, s, SRC_GLOBAL>(a, tile, offA_s, base_s, ctx, tid, up);
-        tc_fence_before();
-        __syncthreads();  // tile written; accumulators read before the next stage's MMAs
-        if constexpr (!LAST)
-            return tc_stage<PLAN, B, THREADS, MODE, INV, FMT, s + 1, false, STOP>(a, tile, tw, offA_s, base_s, ctx,
-                                                                                 tid, ubase, v0);
-        return true;
-    }
+    tc_fence_before();
+    __syncthreads();  // tile written; accumulators read before the next stage's MMAs
+    if constexpr (!LAST)
+        return tc_stage<PLAN, B, THREADS, MODE, INV, FMT, s + 1, false>(a, tile, tw, offA_s, base_s, ctx, tid, ubase,
+                                                                        v0);
+    return true;
 }
 
 template <class PLAN, int B, int MODE, int FMT>
@@ -498,7 +453,7 @@ template <class PLAN, int B, int MODE, int FMT> __host__ __device__ constexpr si
     bytes += sizeof(float2) * (size_t)PLAN::twtotal();
     bytes += sizeof(uint32_t) * (size_t)PLAN::N;
     bytes = (bytes + 15) & ~size_t(15);
-    bytes += sizeof(size_t) * (size_t)(2 * B);   // line bases per slot
+    bytes += sizeof(size_t) * (size_t)B;
     bytes += sizeof(unsigned long long) * 3 + 16;  // two ring barriers, the MMA barrier, tensor-memory address
     return bytes;
 }
@@ -527,9 +482,9 @@ __global__ void __launch_bounds__(B * PLAN::N / 16, (tc_min_blocks<PLAN, B, FMT>
     unsigned char* bmat = ring + NSTG * SLOT;
     float2* tw = reinterpret_cast<float2*>(bmat + tc_b_bytes(FMT));
     uint32_t* offA_s = reinterpret_cast<uint32_t*>(tw + TWN);
-    size_t* base_s = reinterpret_cast<size_t*>(  // line bases, one set per ring slot
+    size_t* base_s = reinterpret_cast<size_t*>(
         reinterpret_cast<unsigned char*>(tw) + ((sizeof(float2) * TWN + sizeof(uint32_t) * N + 15) & ~size_t(15)));
-    unsigned long long* rbar = reinterpret_cast<unsigned long long*>(base_s + NSTG * B);  // ring slots
+    unsigned long long* rbar = reinterpret_cast<unsigned long long*>(base_s + B);  // ring slots
     unsigned long long* mbar = rbar + NSTG;                                        // MMA completion
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 1);
 
@@ -573,20 +528,22 @@ __global__ void __launch_bounds__(B * PLAN::N / 16, (tc_min_blocks<PLAN, B, FMT>
         for (; issued < NSTG && issued < mine; ++issued)
             tmat_issue<float, B, N>(m, blockIdx.x + issued * gridDim.x, tilesV, ring + issued * SLOT, rbar + issued);
 
-    // stage 0 of the CTA's i-th tile on the CUDA cores: its line bases, the
-    // wait for its slot, the slot into registers, then the Stockham tile
-    // written over it.  False when the slot's copy did not arrive in time.
-    auto stage0 = [&](int i) -> bool {
+    bool ok = true;
+    int i = 0;
+    for (; i < mine; ++i) {
         const int t = blockIdx.x + i * gridDim.x;
         const int s = i % NSTG;
         const int u = t / tilesV;
         const int v0 = (t - u * tilesV) * B;
         const size_t ubase = __ldg(a.offU + u);
-        for (int b = tid; b < B; b += THREADS) base_s[s * B + b] = ubase + __ldg(a.offV + v0 + b);
+        for (int b = tid; b < B; b += THREADS) base_s[b] = ubase + __ldg(a.offV + v0 + b);
         if (__syncthreads_or(!mbar_wait_bounded(rbar + s, (uint32_t)((i / NSTG) & 1)))) {
             if (tid == 0) atomicExch(a.err, 1);
-            return false;
+            ok = false;
+            break;
         }
+        // stage 0 on the CUDA cores: the slot into registers, then the
+        // Stockham tile written over it
         const float2* src = reinterpret_cast<const float2*>(ring + s * SLOT);
         float2* tile = reinterpret_cast<float2*>(ring + s * SLOT);
         float2 x[K][R0];
@@ -628,49 +585,17 @@ __global__ void __launch_bounds__(B * PLAN::N / 16, (tc_min_blocks<PLAN, B, FMT>
             }
         }
         __syncthreads();
-        return true;
-    };
-
-    // Software pipeline over the CTA's tiles: the last stage's MMAs of tile
-    // i run while tile i+1's stage 0 reads its slot; only then are tile i's
-    // accumulators read back and stored.
-    // On leaving, the copies of tiles [i, issued) may still be in flight (the
-    // drain below waits for them); those of tiles before i have landed.
-    int i = 0;
-    bool ok = mine == 0 || stage0(0);
-    if (ok) {
-        for (; i < mine; ++i) {
-            const int s = i % NSTG;
-            float2* tile = reinterpret_cast<float2*>(ring + s * SLOT);
-            const size_t* bs = base_s + s * B;
-            // middle tensor-core stages (none for two-stage plans), full round trips
-            if (!tc_stage<PLAN, B, THREADS, MODE, INV, FMT, 1, false, true>(a, tile, tw, offA_s, bs, ctx, tid, 0,
-                                                                             0)) {
-                ok = false;
-                ++i;  // tile i's copy has landed
-                break;
-            }
-            constexpr int SL = PLAN::S - 1;
-            const float up = tc_front<PLAN, B, THREADS, MODE, INV, FMT, SL, false>(a, tile, tw, ctx, tid, 0, 0);
-            // the last stage has read the slot (tc_front ends with a block
-            // barrier): refill it with the tile NSTG ahead
-            if (tid == 0 && issued < mine) {
-                fence_proxy_async_smem();  // the generic accesses of the slot come before the async writes
-                tmat_issue<float, B, N>(m, blockIdx.x + issued * gridDim.x, tilesV, ring + s * SLOT, rbar + s);
-                ++issued;
-            }
-            const bool next_ok = i + 1 >= mine || stage0(i + 1);
-            if (!tc_wait(a, ctx, tid)) {
-                ok = false;
-                i += next_ok ? 2 : 1;
-                break;
-            }
-            tc_back<PLAN, B, THREADS, MODE, FMT, SL, false>(a, tile, offA_s, bs, ctx, tid, up);
-            if (!next_ok) {
-                ok = false;
-                i += 1;  // tile i+1's copy is the one that did not arrive
-                break;
-            }
+        if (!tc_stage<PLAN, B, THREADS, MODE, INV, FMT, 1, false>(a, tile, tw, offA_s, base_s, ctx, tid, ubase, v0)) {
+            ok = false;
+            ++i;  // tile i's copy has landed
+            break;
+        }
+        // the last stage read the slot (tc_stage ends with a block barrier):
+        // refill it with the tile NSTG ahead
+        if (tid == 0 && issued < mine) {
+            fence_proxy_async_smem();  // the generic accesses of the slot come before the async writes
+            tmat_issue<float, B, N>(m, blockIdx.x + issued * gridDim.x, tilesV, ring + s * SLOT, rbar + s);
+            ++issued;
         }
     }
     if (!ok && tid == 0)  // wait (bounded) for this CTA's copies still in flight before leaving
