@@ -236,7 +236,7 @@ bool build_tmat(const Dist& d, int slot, int B, const void* data, a2a::TmatMaps*
 
 bool is_tmat(const PassKernel& k) {
     return k.kind == a2a::KIND_TMAT2 || k.kind == a2a::KIND_TMAT3 || k.kind == a2a::KIND_TMAT2W ||
-           k.kind == a2a::KIND_TMATI;
+           k.kind == a2a::KIND_TMATI || k.kind == a2a::KIND_TMAT2S;
 }
 
 // Does variant k fit the slot's geometry?  Every kernel needs whole tiles.
@@ -1261,7 +1261,8 @@ a2a_status a2a_dfft_plan_report(const a2a_dfft* f, char* buf, size_t len) {
                      k.kind == a2a::KIND_PIPE ? "pipe" : k.kind == a2a::KIND_TMA ? "tma"
                      : k.kind == a2a::KIND_RPIPE ? "rpipe" : k.kind == a2a::KIND_TMAT2 ? "tmat2"
                      : k.kind == a2a::KIND_TMAT3 ? "tmat3" : k.kind == a2a::KIND_TMAT2W ? "tmat2w"
-                     : k.kind == a2a::KIND_TMATI ? "tmati" : "direct", k.lines, k.lpt, k.threads, k.smem,
+                     : k.kind == a2a::KIND_TMATI ? "tmati" : k.kind == a2a::KIND_TMAT2S ? "tmat2s" : "direct",
+                     k.lines, k.lpt, k.threads, k.smem,
                      ps.occ[c], k.radix[0], k.radix[1], k.radix[2], k.radix[3], (int)ps.fits[c], ps.tuned_ms[c],
                      c == ps.chosen ? " <- chosen" : "");
             out += line;

@@ -185,7 +185,8 @@ template <typename T, int N> struct PlanOf<T, N, KIND_TMAT2W> { using Plan = typ
     X(float,  512, KIND_TMATI,   8, 128, 3, 2)      \
     X(float,  512, KIND_TMAT3,   8, 128, 2, 2)      \
     X(float, 1024, KIND_TMAT2,   4, 128, 2, 2)      \
-    X(float, 1024, KIND_TMATI,   4, 128, 3, 2)
+    X(float, 1024, KIND_TMATI,   4, 128, 3, 2)      \
+    X(float,  512, KIND_TMAT2S,  8, 128, 2, 1)
 
 #define A2A_VARIANTS_F64(X)                         \
     X(double,    4, KIND_DIRECT,  4,  32, 1, 1)     \
@@ -247,7 +248,11 @@ template <typename T, int N, int KIND, int B, int TH, int MB, int LPT, int MODE,
 PassKernel make_pass_kernel() {
     using P = typename PlanOf<T, N, KIND>::Plan;
     PassKernel k;
-    if constexpr (KIND == KIND_TMAT2 || KIND == KIND_TMAT3 || KIND == KIND_TMAT2W || KIND == KIND_TMATI)
+    if constexpr (KIND == KIND_TMAT2S) {
+        static_assert(sizeof(T) == 4 && N == 512 && B == 8 && TH == 128 && LPT == 1 && MODE == MODE_BATCH,
+                      "the shuffle ring kernel is compiled for 8-line 512 batch tiles of complex float only");
+        k.fn = reinterpret_cast<const void*>(&fft_tmat_shfl_kernel<INV, MB>);
+    } else if constexpr (KIND == KIND_TMAT2 || KIND == KIND_TMAT3 || KIND == KIND_TMAT2W || KIND == KIND_TMATI)
         k.fn = reinterpret_cast<const void*>(
             &fft_tmat_kernel<T, P, B, TH, MODE, INV, MB, LPT, (KIND == KIND_TMAT3 ? 3 : 2), KIND == KIND_TMATI>);
     else if constexpr (KIND == KIND_PIPE)
@@ -264,7 +269,8 @@ PassKernel make_pass_kernel() {
     k.lines = B;
     k.min_blocks = MB;
     k.lpt = LPT;
-    if constexpr (KIND == KIND_TMAT2 || KIND == KIND_TMAT3 || KIND == KIND_TMAT2W || KIND == KIND_TMATI)
+    if constexpr (KIND == KIND_TMAT2 || KIND == KIND_TMAT3 || KIND == KIND_TMAT2W || KIND == KIND_TMATI ||
+                  KIND == KIND_TMAT2S)
         k.smem = tmat_smem_bytes<T, P, B, MODE, LPT, (KIND == KIND_TMAT3 ? 3 : 2), KIND == KIND_TMATI>();
     else
         k.smem = pass_smem_bytes<T, P, B, MODE, KIND, LPT>();
@@ -279,7 +285,7 @@ PassKernel make_pass_kernel() {
 template <typename T, int N, int KIND, int B, int TH, int MB, int LPT>
 bool make_variant(int mode, bool inv, PassKernel* out) {
     if (mode == MODE_LINE) {
-        if constexpr (LPT != 1 || KIND == KIND_TMA) {
+        if constexpr (LPT != 1 || KIND == KIND_TMA || KIND == KIND_TMAT2S) {
             return false;
         } else {
             *out = inv ? make_pass_kernel<T, N, KIND, B, TH, MB, 1, MODE_LINE, true>()

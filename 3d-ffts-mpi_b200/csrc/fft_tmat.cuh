@@ -234,4 +234,144 @@ __global__ void __launch_bounds__(THREADS, MINB) fft_tmat_kernel(const PassArgs<
     }
 }
 
+// KIND_TMAT2S: the 2-slot ring for batch-mode tiles of 8 lines of length 512
+// = 8 x 8 x 8 (complex float, 128 threads), with the exchange between the
+// first two stages done by warp shuffles instead of shared memory.
+//
+// Stage 0's radix-8 butterfly j writes positions 8 j + r, and stage 1's
+// butterfly j' reads j' + 64 r'': so the eight stage-0 butterflies
+// {a + 8 r''} of a line feed exactly the eight stage-1 butterflies
+// {8 a + r} (a = 0..7), a closed 8 x 8 exchange.  Each such group of a line
+// belongs to one pair of lanes (lane = b + 8 (a % 2) + 16 h, partner lane ^
+// 16): lane h runs stage-0 butterflies a + 8 (4 h + t) and stage-1
+// butterflies 8 a + 4 h + u (t, u = 0..3), keeps the half of its outputs its
+// own stage-1 butterflies need and trades the other half with its partner
+// (16 complex values each way).  So that every register's role is the same
+// in both lanes (no per-lane selects), lane h = 1 computes its stage-0 DFTs
+// on inputs multiplied by (-1)^n, which rotates the outputs by four
+// (X[k ^ 4]), and its stage-1 DFTs on inputs held in that rotated order,
+// which multiplies output k by (-1)^k.  Stage 1 then writes the Stockham tile
+// and stage 2 is the shared-memory stage of the other ring kernels.  The
+// tile's row swizzle uses bit 6 of the row (rows 64 apart, which stage 1's
+// half-warps write together, land in different bank halves).  Shared-memory
+// traffic per element: the slot read, one tile write and one tile read,
+// against five accesses in the three-exchange schedule.
+constexpr int kShflSwsh = 6;
+
+template <bool INV, int MINB>
+__global__ void __launch_bounds__(128, MINB) fft_tmat_shfl_kernel(const PassArgs<float> a,
+                                                                   const __grid_constant__ TmatMaps m) {
+    using PLAN = RadixPlan<8, 8, 8>;
+    constexpr int B = 8, N = 512, THREADS = 128, NSTG = 2;
+    using G = TileGeom<MODE_BATCH, B, N, sizeof(float2), kShflSwsh>;
+    constexpr int TWN = PLAN::twtotal();
+    constexpr int TWO1 = PLAN::twoff(1);
+    constexpr uint32_t SLOT = tmat_slot_bytes_for<float, PLAN, B, MODE_BATCH, 1, false>();
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const uint32_t s0 = smem_u32(smem_raw);
+    unsigned char* ring = smem_raw + (((s0 + kTmatAlign - 1) & ~(kTmatAlign - 1)) - s0);
+    float2* const tile = reinterpret_cast<float2*>(ring + NSTG * SLOT);
+    float2* tw = reinterpret_cast<float2*>(tile + G::elems);
+    uint32_t* offA_s = reinterpret_cast<uint32_t*>(tw + TWN);
+    size_t* base_s = reinterpret_cast<size_t*>(
+        reinterpret_cast<unsigned char*>(tw) + ((sizeof(float2) * TWN + sizeof(uint32_t) * N + 15) & ~size_t(15)));
+    unsigned long long* bar = reinterpret_cast<unsigned long long*>(base_s + B);
+
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int b = lane & 7;                       // line of the tile
+    const int ga = 2 * (tid >> 5) + ((lane >> 3) & 1);  // group a = 0..7
+    const int h = lane >> 4;                      // half of the pair
+    const float sgn = h ? -1.f : 1.f;
+    const int tilesV = a.NV / B;
+    const int ntiles = a.NU * tilesV;
+    const int mine = (int)blockIdx.x < ntiles ? (ntiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x : 0;
+    if (tid == 0) {
+        for (int i = 0; i < NSTG; ++i) mbar_init(bar + i, 1);
+        fence_mbar_init();
+    }
+    for (int i = tid; i < TWN; i += THREADS) tw[i] = a.tw[i];
+    for (int i = tid; i < N; i += THREADS) offA_s[i] = a.offA[i];
+    __syncthreads();
+    int issued = 0;  // thread 0: tiles of this CTA whose copies were issued
+    if (tid == 0)
+        for (; issued < NSTG && issued < mine; ++issued)
+            tmat_issue<float, B, N>(m, blockIdx.x + issued * gridDim.x, tilesV, ring + issued * SLOT, bar + issued);
+
+    for (int i = 0; i < mine; ++i) {
+        const int t = blockIdx.x + i * gridDim.x;
+        const int s = i % NSTG;
+        {
+            const int u = t / tilesV;
+            const int v0 = (t - u * tilesV) * B;
+            const size_t ubase = __ldg(a.offU + u);
+            for (int bb = tid; bb < B; bb += THREADS) base_s[bb] = ubase + __ldg(a.offV + v0 + bb);
+        }
+        const bool ok = mbar_wait_bounded(bar + s, (uint32_t)((i / NSTG) & 1));
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) {
+                atomicExch(a.err, 1);
+                for (int j = i; j < issued; ++j) mbar_wait_bounded(bar + j % NSTG, (uint32_t)((j / NSTG) & 1));
+            }
+            return;
+        }
+        const float2* src = reinterpret_cast<const float2*>(ring + s * SLOT);
+        // stage 0: butterflies j = a + 8 (4 h + tt), inputs n = j + 64 r
+        float2 y[4][8];
+#pragma unroll
+        for (int tt = 0; tt < 4; ++tt) {
+            const int j = ga + 8 * (4 * h + tt);
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                const float2 v = src[(j + 64 * r) * B + b];
+                y[tt][r] = (r & 1) ? make_float2(v.x * sgn, v.y * sgn) : v;
+            }
+            Dft<8, INV, float2>::run(y[tt]);  // register k holds output k ^ 4h
+        }
+        // exchange: keep registers 0-3 (outputs 4h + u), trade 4-7 (outputs
+        // 4(1-h) + u, the partner's stage-1 butterflies)
+        float2 x[4][8];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int tt = 0; tt < 4; ++tt) {
+                x[u][tt] = y[tt][u];
+                x[u][4 + tt].x = __shfl_xor_sync(0xffffffffu, y[tt][4 + u].x, 16);
+                x[u][4 + tt].y = __shfl_xor_sync(0xffffffffu, y[tt][4 + u].y, 16);
+            }
+        __syncthreads();  // slot s read out
+        if (tid == 0 && issued < mine) {
+            fence_proxy_async_smem();  // the generic reads of slot s come before the async writes
+            tmat_issue<float, B, N>(m, blockIdx.x + issued * gridDim.x, tilesV, ring + s * SLOT, bar + s);
+            ++issued;
+        }
+        // stage 1: butterfly j' = 8 a + 4 h + u; register rho holds input
+        // r'' = rho ^ 4h; twiddle index m = j' % 8 = 4 h + u
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int mm = 4 * h + u;
+#pragma unroll
+            for (int rho = 0; rho < 8; ++rho) {
+                const int rr = rho ^ (4 * h);
+                if (rho == 0 || rho == 4) {
+                    if (rr != 0) x[u][rho] = cmulw<INV>(x[u][rho], tw[TWO1 + (rr - 1) * 8 + mm]);
+                } else {
+                    x[u][rho] = cmulw<INV>(x[u][rho], tw[TWO1 + (rr - 1) * 8 + mm]);
+                }
+            }
+            Dft<8, INV, float2>::run(x[u]);  // output k times (-1)^k for h = 1
+            const int jd = 64 * ga + mm;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const float2 v = (k & 1) ? make_float2(x[u][k].x * sgn, x[u][k].y * sgn) : x[u][k];
+                tile[G::idx(b, jd + 8 * k)] = v;
+            }
+        }
+        __syncthreads();  // the tile is written
+        run_stage<float, PLAN, B, THREADS, MODE_BATCH, INV, 1, 2, kShflSwsh>(a, tile, tw, offA_s, base_s, tid);
+        __syncthreads();  // tile and line bases free for the next tile
+    }
+}
+
 }  // namespace a2a

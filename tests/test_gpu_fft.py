@@ -174,3 +174,41 @@ def test_autotune_report(pkg, oracle, cuda):
     f.forward(x)
     fwd = oracle.bricks_to_global(x.cpu().numpy().reshape(16, -1), d)
     assert oracle.rel_l2(fwd, oracle.fft3_global(g)) <= 1e-6
+
+
+@pytest.mark.parametrize("inverse_first", [False, True])
+@pytest.mark.parametrize("P,shape", [(16, (512, 64, 64)), (16, (64, 512, 64)), (64, (512, 256, 128))])
+def test_shuffle_exchange_variant(pkg, oracle, cuda, P, shape, inverse_first):
+    """The ring kernel whose first exchange runs through warp shuffles
+    (``tmat2s``: 512 = 8 x 8 x 8, complex float batch tiles), forced on every
+    pass it fits, against the oracle's complex128 transform of the whole box
+    (relative L2 <= 1e-6), in both directions."""
+    import torch
+
+    dist = pkg.a2aDistribution(P, shape, 64, precision="c64")
+    d = oracle.Decomp(shape, P)
+    g = oracle.make_input("uniform", shape, seed=23, dtype=np.complex64, tones=2)
+    x = torch.from_numpy(oracle.global_to_bricks(g, d).ravel()).to(cuda)
+    f = pkg.a2adfft(dist)
+    f.make_plans()
+    forced = 0
+    for p, line in enumerate(_pass_reports(f)):
+        idx = [i for i, ln in enumerate(line) if " tmat2s " in ln and "fits=1" in ln]
+        if idx:
+            f.select_variant(p, idx[0])
+            forced += 1
+    assert forced >= 1
+    if inverse_first:
+        f.inverse(x)
+        ref = oracle.fft3_fp64(g, inverse=True)
+    else:
+        f.forward(x)
+        ref = oracle.fft3_fp64(g)
+    out = oracle.bricks_to_global(x.cpu().numpy().reshape(P, -1), d)
+    assert oracle.rel_l2(out, ref) <= 1e-6
+
+
+def _pass_reports(f):
+    """The plan report's variant lines grouped by pass (Z, X, Y), in variant order."""
+    lines = f.plan_report().splitlines()
+    return [[ln for ln in lines if ln.startswith(name + " pass")] for name in ("Z", "X", "Y")]
