@@ -77,7 +77,10 @@ template <typename T, int N> struct PlanOf<T, N, KIND_TMAT2W> { using Plan = typ
 // buffer and keep the fastest (a2a_dfft_make_plans).  DIRECT tiles are about
 // 32-64 KB so two or three CTAs share an SM; PIPE CTAs hold two tiles.  LPT =
 // 2 (complex float, batch mode): a thread moves two adjacent lines as one
-// 16-byte access, which halves the shared-memory instructions of a tile.
+// 16-byte access, which halves the shared-memory instructions of a tile.  The
+// first entry of each length is its default in both access modes (entries a
+// mode cannot use are skipped): at 512 the shuffle ring kernel for batch-mode
+// passes, the register-pipelined kernel for line mode.
 #define A2A_VARIANTS_F32(X)                            \
     X(float,    4, KIND_DIRECT,  4,  32, 1, 1)      \
     X(float,    8, KIND_DIRECT,  8,  32, 1, 1)      \
@@ -123,6 +126,7 @@ template <typename T, int N> struct PlanOf<T, N, KIND_TMAT2W> { using Plan = typ
     X(float,  384, KIND_DIRECT, 16, 256, 1, 1)      \
     X(float,  384, KIND_PIPE,    8, 256, 2, 1)      \
     X(float,  384, KIND_DIRECT,  4,  64, 1, 1)      \
+    X(float,  512, KIND_TMAT2S,  8, 128, 2, 1)      \
     X(float,  512, KIND_RPIPE,  16, 512, 1, 2)      \
     X(float,  512, KIND_RPIPE,   8, 256, 2, 1)      \
     X(float,  512, KIND_DIRECT, 16, 512, 1, 2)      \
@@ -185,8 +189,7 @@ template <typename T, int N> struct PlanOf<T, N, KIND_TMAT2W> { using Plan = typ
     X(float,  512, KIND_TMATI,   8, 128, 3, 2)      \
     X(float,  512, KIND_TMAT3,   8, 128, 2, 2)      \
     X(float, 1024, KIND_TMAT2,   4, 128, 2, 2)      \
-    X(float, 1024, KIND_TMATI,   4, 128, 3, 2)      \
-    X(float,  512, KIND_TMAT2S,  8, 128, 2, 1)
+    X(float, 1024, KIND_TMATI,   4, 128, 3, 2)
 
 #define A2A_VARIANTS_F64(X)                         \
     X(double,    4, KIND_DIRECT,  4,  32, 1, 1)     \
