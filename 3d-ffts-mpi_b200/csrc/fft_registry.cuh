@@ -147,6 +147,7 @@ template <typename T, int N> struct PlanOf<T, N, KIND_TMAT2W> { using Plan = typ
     X(float,  768, KIND_PIPE,    8, 384, 1, 1)      \
     X(float,  768, KIND_DIRECT,  4, 128, 1, 1)      \
     X(float, 1024, KIND_DIRECT,  8, 512, 1, 1)      \
+    X(float, 1024, KIND_TMAT2S,  4, 128, 2, 1)      \
     X(float, 1024, KIND_DIRECT, 16, 512, 1, 2)      \
     X(float, 1024, KIND_RPIPE,   8, 512, 1, 1)      \
     X(float, 1024, KIND_TMA,     8, 512, 1, 1)      \
@@ -252,9 +253,9 @@ PassKernel make_pass_kernel() {
     using P = typename PlanOf<T, N, KIND>::Plan;
     PassKernel k;
     if constexpr (KIND == KIND_TMAT2S) {
-        static_assert(sizeof(T) == 4 && N == 512 && B == 8 && TH == 128 && LPT == 1 && MODE == MODE_BATCH,
-                      "the shuffle ring kernel is compiled for 8-line 512 batch tiles of complex float only");
-        k.fn = reinterpret_cast<const void*>(&fft_tmat_shfl_kernel<INV, MB>);
+        static_assert(sizeof(T) == 4 && B == ShflGeom<P>::B && TH == 128 && LPT == 1 && MODE == MODE_BATCH,
+                      "the shuffle ring kernel moves complex float batch tiles with 128 threads");
+        k.fn = reinterpret_cast<const void*>(&fft_tmat_shfl_kernel<P, INV, MB>);
     } else if constexpr (KIND == KIND_TMAT2 || KIND == KIND_TMAT3 || KIND == KIND_TMAT2W || KIND == KIND_TMATI)
         k.fn = reinterpret_cast<const void*>(
             &fft_tmat_kernel<T, P, B, TH, MODE, INV, MB, LPT, (KIND == KIND_TMAT3 ? 3 : 2), KIND == KIND_TMATI>);

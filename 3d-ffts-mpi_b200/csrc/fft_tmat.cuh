@@ -234,38 +234,54 @@ __global__ void __launch_bounds__(THREADS, MINB) fft_tmat_kernel(const PassArgs<
     }
 }
 
-// KIND_TMAT2S: the 2-slot ring for batch-mode tiles of 8 lines of length 512
-// = 8 x 8 x 8 (complex float, 128 threads), with the exchange between the
-// first two stages done by warp shuffles instead of shared memory.
+// KIND_TMAT2S: the 2-slot ring for batch-mode tiles of complex float (128
+// threads) whose first two stages exchange through warp shuffles instead of
+// shared memory.  Plans R0 x R1 x R2 with R0 R1 = 64: 512 = 8 x 8 x 8 (8-line
+// tiles) and 1024 = 4 x 16 x 16 (4-line tiles).
 //
-// Stage 0's radix-8 butterfly j writes positions 8 j + r, and stage 1's
-// butterfly j' reads j' + 64 r'': so the eight stage-0 butterflies
-// {a + 8 r''} of a line feed exactly the eight stage-1 butterflies
-// {8 a + r} (a = 0..7), a closed 8 x 8 exchange.  Each such group of a line
-// belongs to one pair of lanes (lane = b + 8 (a % 2) + 16 h, partner lane ^
-// 16): lane h runs stage-0 butterflies a + 8 (4 h + t) and stage-1
-// butterflies 8 a + 4 h + u (t, u = 0..3), keeps the half of its outputs its
-// own stage-1 butterflies need and trades the other half with its partner
-// (16 complex values each way).  So that every register's role is the same
-// in both lanes (no per-lane selects), lane h = 1 computes its stage-0 DFTs
-// on inputs multiplied by (-1)^n, which rotates the outputs by four
-// (X[k ^ 4]), and its stage-1 DFTs on inputs held in that rotated order,
-// which multiplies output k by (-1)^k.  Stage 1 then writes the Stockham tile
-// and stage 2 is the shared-memory stage of the other ring kernels.  The
-// tile's row swizzle uses bit 6 of the row (rows 64 apart, which stage 1's
-// half-warps write together, land in different bank halves).  Shared-memory
-// traffic per element: the slot read, one tile write and one tile read,
-// against five accesses in the three-exchange schedule.
+// Stage 0's radix-R0 butterfly j writes positions R0 j + r, and stage 1's
+// radix-R1 butterfly j' reads j' + (N / R1) r'': so with NG = N / 64 the R1
+// stage-0 butterflies {a + NG r''} of a line feed exactly the R0 stage-1
+// butterflies {R0 a + r} (a = 0 .. NG-1), a closed 64-element exchange.  Each
+// such group of a line belongs to one pair of lanes (lane = b + B (a mod
+// 16/B) + 16 h, partner lane ^ 16): lane h runs stage-0 butterflies
+// a + NG (R1/2 h + t) and stage-1 butterflies R0 a + R0/2 h + u
+// (t < R1/2, u < R0/2), keeps the half of its outputs its own stage-1
+// butterflies need and trades the other half with its partner (16 complex
+// values each way).  So that every register has the same role in both lanes
+// (no per-lane selects), lane h = 1 runs its stage-0 DFTs on inputs times
+// (-1)^n, which rotates the outputs by R0/2 (X[k ^ R0/2]), and its stage-1
+// DFTs on inputs held in the order rotated by R1/2, which multiplies output k
+// by (-1)^k.  Stage 1 then writes the Stockham tile and the last stage is the
+// shared-memory stage of the other ring kernels.  The tile's row swizzle
+// uses row bits 6 and up (rows 64 apart, which stage 1's half-warps write
+// together, land in different bank slots).  Shared-memory traffic per
+// element: the slot read, one tile write and one tile read, against five
+// accesses in the three-exchange schedule.
 constexpr int kShflSwsh = 6;
 
-template <bool INV, int MINB>
+template <class PLAN> struct ShflGeom {
+    static constexpr int N = PLAN::N;
+    static constexpr int R0 = PLAN::r[0];
+    static constexpr int R1 = PLAN::r[1];
+    static_assert(PLAN::S == 3 && R0 * R1 == 64, "the shuffle exchange pairs 64-element groups");
+    static constexpr int NG = N / 64;      // groups per line
+    static constexpr int B = 64 / NG;      // lines per tile (128 threads = 64 lane pairs)
+    static_assert(B >= 2 && B <= 16 && 16 % B == 0, "a half-warp spans whole groups of lines");
+    static constexpr int H0 = R1 / 2;      // stage-0 butterflies per lane
+    static constexpr int H1 = R0 / 2;      // stage-1 butterflies per lane
+};
+
+template <class PLAN, bool INV, int MINB>
 __global__ void __launch_bounds__(128, MINB) fft_tmat_shfl_kernel(const PassArgs<float> a,
                                                                    const __grid_constant__ TmatMaps m) {
-    using PLAN = RadixPlan<8, 8, 8>;
-    constexpr int B = 8, N = 512, THREADS = 128, NSTG = 2;
+    using SG = ShflGeom<PLAN>;
+    constexpr int N = SG::N, R0 = SG::R0, R1 = SG::R1, B = SG::B, H0 = SG::H0, H1 = SG::H1;
+    constexpr int THREADS = 128, NSTG = 2;
     using G = TileGeom<MODE_BATCH, B, N, sizeof(float2), kShflSwsh>;
     constexpr int TWN = PLAN::twtotal();
     constexpr int TWO1 = PLAN::twoff(1);
+    constexpr int NS1 = PLAN::ns(1);  // = R0
     constexpr uint32_t SLOT = tmat_slot_bytes_for<float, PLAN, B, MODE_BATCH, 1, false>();
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -280,9 +296,9 @@ __global__ void __launch_bounds__(128, MINB) fft_tmat_shfl_kernel(const PassArgs
 
     const int tid = threadIdx.x;
     const int lane = tid & 31;
-    const int b = lane & 7;                       // line of the tile
-    const int ga = 2 * (tid >> 5) + ((lane >> 3) & 1);  // group a = 0..7
-    const int h = lane >> 4;                      // half of the pair
+    const int b = lane % B;                                        // line of the tile
+    const int ga = (tid >> 5) * (16 / B) + (lane / B) % (16 / B);  // group a = 0 .. NG-1
+    const int h = lane >> 4;                                       // half of the pair
     const float sgn = h ? -1.f : 1.f;
     const int tilesV = a.NV / B;
     const int ntiles = a.NU * tilesV;
@@ -317,28 +333,28 @@ __global__ void __launch_bounds__(128, MINB) fft_tmat_shfl_kernel(const PassArgs
             return;
         }
         const float2* src = reinterpret_cast<const float2*>(ring + s * SLOT);
-        // stage 0: butterflies j = a + 8 (4 h + tt), inputs n = j + 64 r
-        float2 y[4][8];
+        // stage 0: butterflies j = a + NG (H0 h + tt), inputs n = j + (N/R0) r
+        float2 y[H0][R0];
 #pragma unroll
-        for (int tt = 0; tt < 4; ++tt) {
-            const int j = ga + 8 * (4 * h + tt);
+        for (int tt = 0; tt < H0; ++tt) {
+            const int j = ga + SG::NG * (H0 * h + tt);
 #pragma unroll
-            for (int r = 0; r < 8; ++r) {
-                const float2 v = src[(j + 64 * r) * B + b];
+            for (int r = 0; r < R0; ++r) {
+                const float2 v = src[(j + (N / R0) * r) * B + b];
                 y[tt][r] = (r & 1) ? make_float2(v.x * sgn, v.y * sgn) : v;
             }
-            Dft<8, INV, float2>::run(y[tt]);  // register k holds output k ^ 4h
+            Dft<R0, INV, float2>::run(y[tt]);  // register k holds output k ^ (R0/2) h
         }
-        // exchange: keep registers 0-3 (outputs 4h + u), trade 4-7 (outputs
-        // 4(1-h) + u, the partner's stage-1 butterflies)
-        float2 x[4][8];
+        // exchange: keep registers 0 .. H1-1 (outputs H1 h + u), trade the
+        // others (outputs H1 (1-h) + u, the partner's stage-1 butterflies)
+        float2 x[H1][R1];
 #pragma unroll
-        for (int u = 0; u < 4; ++u)
+        for (int u = 0; u < H1; ++u)
 #pragma unroll
-            for (int tt = 0; tt < 4; ++tt) {
+            for (int tt = 0; tt < H0; ++tt) {
                 x[u][tt] = y[tt][u];
-                x[u][4 + tt].x = __shfl_xor_sync(0xffffffffu, y[tt][4 + u].x, 16);
-                x[u][4 + tt].y = __shfl_xor_sync(0xffffffffu, y[tt][4 + u].y, 16);
+                x[u][H0 + tt].x = __shfl_xor_sync(0xffffffffu, y[tt][H1 + u].x, 16);
+                x[u][H0 + tt].y = __shfl_xor_sync(0xffffffffu, y[tt][H1 + u].y, 16);
             }
         __syncthreads();  // slot s read out
         if (tid == 0 && issued < mine) {
@@ -346,26 +362,26 @@ __global__ void __launch_bounds__(128, MINB) fft_tmat_shfl_kernel(const PassArgs
             tmat_issue<float, B, N>(m, blockIdx.x + issued * gridDim.x, tilesV, ring + s * SLOT, bar + s);
             ++issued;
         }
-        // stage 1: butterfly j' = 8 a + 4 h + u; register rho holds input
-        // r'' = rho ^ 4h; twiddle index m = j' % 8 = 4 h + u
+        // stage 1: butterfly j' = R0 a + H1 h + u; register rho holds input
+        // r'' = rho ^ H0 h; twiddle index j' mod R0 = H1 h + u
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int mm = 4 * h + u;
+        for (int u = 0; u < H1; ++u) {
+            const int mm = H1 * h + u;
 #pragma unroll
-            for (int rho = 0; rho < 8; ++rho) {
-                const int rr = rho ^ (4 * h);
-                if (rho == 0 || rho == 4) {
-                    if (rr != 0) x[u][rho] = cmulw<INV>(x[u][rho], tw[TWO1 + (rr - 1) * 8 + mm]);
+            for (int rho = 0; rho < R1; ++rho) {
+                const int rr = rho ^ (H0 * h);
+                if (rho == 0 || rho == H0) {
+                    if (rr != 0) x[u][rho] = cmulw<INV>(x[u][rho], tw[TWO1 + (rr - 1) * NS1 + mm]);
                 } else {
-                    x[u][rho] = cmulw<INV>(x[u][rho], tw[TWO1 + (rr - 1) * 8 + mm]);
+                    x[u][rho] = cmulw<INV>(x[u][rho], tw[TWO1 + (rr - 1) * NS1 + mm]);
                 }
             }
-            Dft<8, INV, float2>::run(x[u]);  // output k times (-1)^k for h = 1
+            Dft<R1, INV, float2>::run(x[u]);  // output k times (-1)^k for h = 1
             const int jd = 64 * ga + mm;
 #pragma unroll
-            for (int k = 0; k < 8; ++k) {
+            for (int k = 0; k < R1; ++k) {
                 const float2 v = (k & 1) ? make_float2(x[u][k].x * sgn, x[u][k].y * sgn) : x[u][k];
-                tile[G::idx(b, jd + 8 * k)] = v;
+                tile[G::idx(b, jd + NS1 * k)] = v;
             }
         }
         __syncthreads();  // the tile is written

@@ -177,12 +177,13 @@ def test_autotune_report(pkg, oracle, cuda):
 
 
 @pytest.mark.parametrize("inverse_first", [False, True])
-@pytest.mark.parametrize("P,shape", [(16, (512, 64, 64)), (16, (64, 512, 64)), (64, (512, 256, 128))])
+@pytest.mark.parametrize("P,shape", [(16, (512, 64, 64)), (16, (64, 512, 64)), (64, (512, 256, 128)),
+                                     (16, (1024, 64, 64)), (4, (64, 1024, 64))])
 def test_shuffle_exchange_variant(pkg, oracle, cuda, P, shape, inverse_first):
     """The ring kernel whose first exchange runs through warp shuffles
-    (``tmat2s``: 512 = 8 x 8 x 8, complex float batch tiles), forced on every
-    pass it fits, against the oracle's complex128 transform of the whole box
-    (relative L2 <= 1e-6), in both directions."""
+    (``tmat2s``: 512 = 8 x 8 x 8 and 1024 = 4 x 16 x 16, complex float batch
+    tiles), forced on every pass it fits, against the oracle's complex128
+    transform of the whole box (relative L2 <= 1e-6), in both directions."""
     import torch
 
     dist = pkg.a2aDistribution(P, shape, 64, precision="c64")
