@@ -343,7 +343,8 @@ cudaError_t launch_slot(const Dist& d, int slot, bool inv, int c, void* p, doubl
     const SlotGeom g = slot_geom(d, slot);
     const uint64_t tiles = (uint64_t)g.NU * (g.NV / k.lines);
     uint64_t grid = tiles;
-    if (k.kind == a2a::KIND_PIPE || k.kind == a2a::KIND_TMA || k.kind == a2a::KIND_RPIPE || is_tmat(k)) {
+    if (k.kind == a2a::KIND_PIPE || k.kind == a2a::KIND_TMA || k.kind == a2a::KIND_RPIPE ||
+        k.kind == a2a::KIND_RPIPES || is_tmat(k)) {
         const uint64_t resident = (uint64_t)std::max(ps.occ[c], 1) * d.sms;
         grid = std::min(tiles, resident);
     }
@@ -1259,7 +1260,8 @@ a2a_status a2a_dfft_plan_report(const a2a_dfft* f, char* buf, size_t len) {
                      "tuned_ms=%.4f%s\n",
                      names[p], k.n,
                      k.kind == a2a::KIND_PIPE ? "pipe" : k.kind == a2a::KIND_TMA ? "tma"
-                     : k.kind == a2a::KIND_RPIPE ? "rpipe" : k.kind == a2a::KIND_TMAT2 ? "tmat2"
+                     : k.kind == a2a::KIND_RPIPE ? "rpipe" : k.kind == a2a::KIND_RPIPES ? "rpipes"
+                     : k.kind == a2a::KIND_TMAT2 ? "tmat2"
                      : k.kind == a2a::KIND_TMAT3 ? "tmat3" : k.kind == a2a::KIND_TMAT2W ? "tmat2w"
                      : k.kind == a2a::KIND_TMATI ? "tmati" : k.kind == a2a::KIND_TMAT2S ? "tmat2s" : "direct",
                      k.lines, k.lpt, k.threads, k.smem,

@@ -129,6 +129,7 @@ template <typename T, int N> struct PlanOf<T, N, KIND_TMAT2W> { using Plan = typ
     X(float,  512, KIND_TMAT2S,  8, 128, 2, 1)      \
     X(float,  512, KIND_RPIPE,  16, 512, 1, 2)      \
     X(float,  512, KIND_RPIPE,   8, 256, 2, 1)      \
+    X(float,  512, KIND_RPIPES,  8, 128, 2, 1)      \
     X(float,  512, KIND_DIRECT, 16, 512, 1, 2)      \
     X(float,  512, KIND_DIRECT,  8, 128, 4, 1)      \
     X(float,  512, KIND_RPIPE,  16, 512, 1, 1)      \
@@ -252,7 +253,11 @@ template <typename T, int N, int KIND, int B, int TH, int MB, int LPT, int MODE,
 PassKernel make_pass_kernel() {
     using P = typename PlanOf<T, N, KIND>::Plan;
     PassKernel k;
-    if constexpr (KIND == KIND_TMAT2S) {
+    if constexpr (KIND == KIND_RPIPES) {
+        static_assert(sizeof(T) == 4 && B == 8 && TH == 128 && LPT == 1 && MODE == MODE_LINE,
+                      "the line-mode shuffle kernel moves 8-line complex float tiles with 128 threads");
+        k.fn = reinterpret_cast<const void*>(&fft_rpipe_shfl_kernel<P, INV, MB>);
+    } else if constexpr (KIND == KIND_TMAT2S) {
         static_assert(sizeof(T) == 4 && B == ShflGeom<P>::B && TH == 128 && LPT == 1 && MODE == MODE_BATCH,
                       "the shuffle ring kernel moves complex float batch tiles with 128 threads");
         k.fn = reinterpret_cast<const void*>(&fft_tmat_shfl_kernel<P, INV, MB>);
@@ -288,18 +293,25 @@ PassKernel make_pass_kernel() {
 // line mode the lookup skips those variants.
 template <typename T, int N, int KIND, int B, int TH, int MB, int LPT>
 bool make_variant(int mode, bool inv, PassKernel* out) {
-    if (mode == MODE_LINE) {
-        if constexpr (LPT != 1 || KIND == KIND_TMA || KIND == KIND_TMAT2S) {
-            return false;
-        } else {
-            *out = inv ? make_pass_kernel<T, N, KIND, B, TH, MB, 1, MODE_LINE, true>()
-                       : make_pass_kernel<T, N, KIND, B, TH, MB, 1, MODE_LINE, false>();
-            return true;
+    if constexpr (KIND == KIND_RPIPES) {  // line mode only
+        if (mode != MODE_LINE) return false;
+        *out = inv ? make_pass_kernel<T, N, KIND, B, TH, MB, 1, MODE_LINE, true>()
+                   : make_pass_kernel<T, N, KIND, B, TH, MB, 1, MODE_LINE, false>();
+        return true;
+    } else {
+        if (mode == MODE_LINE) {
+            if constexpr (LPT != 1 || KIND == KIND_TMA || KIND == KIND_TMAT2S) {
+                return false;
+            } else {
+                *out = inv ? make_pass_kernel<T, N, KIND, B, TH, MB, 1, MODE_LINE, true>()
+                           : make_pass_kernel<T, N, KIND, B, TH, MB, 1, MODE_LINE, false>();
+                return true;
+            }
         }
+        *out = inv ? make_pass_kernel<T, N, KIND, B, TH, MB, LPT, MODE_BATCH, true>()
+                   : make_pass_kernel<T, N, KIND, B, TH, MB, LPT, MODE_BATCH, false>();
+        return true;
     }
-    *out = inv ? make_pass_kernel<T, N, KIND, B, TH, MB, LPT, MODE_BATCH, true>()
-               : make_pass_kernel<T, N, KIND, B, TH, MB, LPT, MODE_BATCH, false>();
-    return true;
 }
 
 // Defined in fft_pass_f32.cu / fft_pass_f64.cu: fills up to `max` variants of

@@ -460,7 +460,8 @@ enum PassKind : int {
     KIND_TMAT2W = 7,  // the 2-slot ring with the length's two-stage wide-radix plan (radix 16/32)
     KIND_TMATI = 8,   // the 2-slot ring with each slot transformed in place (no separate tile)
     KIND_TCR = 9,     // tensor-core stages, persistent CTAs fed by the in-place 2-slot TMA ring
-    KIND_TMAT2S = 10  // the 2-slot ring, 512 = 8 x 8 x 8 batch tiles, first exchange by warp shuffles
+    KIND_TMAT2S = 10, // the 2-slot ring, batch tiles, first exchange by warp shuffles (R0 R1 = 64 plans)
+    KIND_RPIPES = 11  // register-pipelined line-mode tiles, first exchange by warp shuffles (512)
 };
 
 constexpr int kTmaBuffers = 2;

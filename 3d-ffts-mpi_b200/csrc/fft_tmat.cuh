@@ -390,4 +390,118 @@ __global__ void __launch_bounds__(128, MINB) fft_tmat_shfl_kernel(const PassArgs
     }
 }
 
+// KIND_RPIPES: the same shuffle exchange for line-mode tiles (the Z pass),
+// fed by the register-pipelined persistent loop of fft_rpipe_kernel instead
+// of the ring: stage 0's inputs come straight from global memory into the
+// lanes' registers (lane = a mod 8 + 8 (line mod 2) + 16 h, so a half-warp
+// reads 8 consecutive elements of each of two lines), and once stage 1 has
+// written the tile the same registers receive the next tile's loads, which
+// stay in flight through the last stage.
+template <class PLAN, bool INV, int MINB>
+__global__ void __launch_bounds__(128, MINB) fft_rpipe_shfl_kernel(const PassArgs<float> a) {
+    using SG = ShflGeom<PLAN>;
+    constexpr int N = SG::N, R0 = SG::R0, R1 = SG::R1, B = SG::B, H0 = SG::H0, H1 = SG::H1, NG = SG::NG;
+    static_assert(NG == 8 && B == 8, "line-mode pairing laid out for 8 groups of 8 lines");
+    constexpr int THREADS = 128;
+    using G = TileGeom<MODE_LINE, B, N, sizeof(float2)>;
+    constexpr int TWN = PLAN::twtotal();
+    constexpr int TWO1 = PLAN::twoff(1);
+    constexpr int NS1 = PLAN::ns(1);
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* tile = reinterpret_cast<float2*>(smem_raw);
+    float2* tw = reinterpret_cast<float2*>(tile + G::elems);
+    uint32_t* offA_s = reinterpret_cast<uint32_t*>(tw + TWN);
+    size_t* base_s = reinterpret_cast<size_t*>(
+        smem_raw + ((sizeof(float2) * (size_t)G::elems + sizeof(float2) * TWN + sizeof(uint32_t) * N + 15) & ~size_t(15)));
+
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int ga = lane & 7;                            // group a
+    const int b = 2 * (tid >> 5) + ((lane >> 3) & 1);   // line of the tile
+    const int h = lane >> 4;                            // half of the pair
+    const float sgn = h ? -1.f : 1.f;
+    const int tilesV = a.NV / B;
+    const int ntiles = a.NU * tilesV;
+    uint32_t d0[R0];
+    if (a.split) {
+#pragma unroll
+        for (int r = 0; r < R0; ++r) d0[r] = __ldg(a.offA + r * (N / R0));
+    }
+    // stage 0's inputs of tile t: butterflies j = a + NG (H0 h + tt), inputs
+    // n = j + (N/R0) r of this lane's line
+    auto load_tile = [&](int t, float2 (&y)[H0][R0]) {
+        const int u = t / tilesV;
+        const int v0 = (t - u * tilesV) * B;
+        const float2* line = a.src + (size_t)__ldg(a.offU + u) + __ldg(a.offV + v0 + b);
+#pragma unroll
+        for (int tt = 0; tt < H0; ++tt) {
+            const int j = ga + NG * (H0 * h + tt);
+            if (a.split) {
+                const float2* q = line + __ldg(a.offA + j);
+#pragma unroll
+                for (int r = 0; r < R0; ++r) y[tt][r] = ld_stream(q + d0[r]);
+            } else {
+#pragma unroll
+                for (int r = 0; r < R0; ++r) y[tt][r] = ld_stream(line + __ldg(a.offA + j + (N / R0) * r));
+            }
+        }
+    };
+    int t = blockIdx.x;
+    float2 y[H0][R0];
+    if (t < ntiles) load_tile(t, y);
+    for (int i = tid; i < TWN; i += THREADS) tw[i] = a.tw[i];
+    for (int i = tid; i < N; i += THREADS) offA_s[i] = a.offA[i];
+    for (; t < ntiles; t += gridDim.x) {
+        {
+            const int u = t / tilesV;
+            const int v0 = (t - u * tilesV) * B;
+            const size_t ubase = __ldg(a.offU + u);
+            for (int bb = tid; bb < B; bb += THREADS) base_s[bb] = ubase + __ldg(a.offV + v0 + bb);
+        }
+        // stage 0 (register k of lane h = 1 holds output k ^ R0/2)
+#pragma unroll
+        for (int tt = 0; tt < H0; ++tt) {
+#pragma unroll
+            for (int r = 1; r < R0; r += 2) y[tt][r] = make_float2(y[tt][r].x * sgn, y[tt][r].y * sgn);
+            Dft<R0, INV, float2>::run(y[tt]);
+        }
+        float2 x[H1][R1];
+#pragma unroll
+        for (int u = 0; u < H1; ++u)
+#pragma unroll
+            for (int tt = 0; tt < H0; ++tt) {
+                x[u][tt] = y[tt][u];
+                x[u][H0 + tt].x = __shfl_xor_sync(0xffffffffu, y[tt][H1 + u].x, 16);
+                x[u][H0 + tt].y = __shfl_xor_sync(0xffffffffu, y[tt][H1 + u].y, 16);
+            }
+        // stage 1 (register rho holds input rho ^ H0 h; output k times (-1)^k for h = 1)
+#pragma unroll
+        for (int u = 0; u < H1; ++u) {
+            const int mm = H1 * h + u;
+#pragma unroll
+            for (int rho = 0; rho < R1; ++rho) {
+                const int rr = rho ^ (H0 * h);
+                if (rho == 0 || rho == H0) {
+                    if (rr != 0) x[u][rho] = cmulw<INV>(x[u][rho], tw[TWO1 + (rr - 1) * NS1 + mm]);
+                } else {
+                    x[u][rho] = cmulw<INV>(x[u][rho], tw[TWO1 + (rr - 1) * NS1 + mm]);
+                }
+            }
+            Dft<R1, INV, float2>::run(x[u]);
+            const int jd = 64 * ga + mm;
+#pragma unroll
+            for (int k = 0; k < R1; ++k) {
+                const float2 v = (k & 1) ? make_float2(x[u][k].x * sgn, x[u][k].y * sgn) : x[u][k];
+                tile[G::idx(b, jd + NS1 * k)] = v;
+            }
+        }
+        const int tn = t + gridDim.x;
+        if (tn < ntiles) load_tile(tn, y);  // in flight through the last stage
+        __syncthreads();
+        run_stage<float, PLAN, B, THREADS, MODE_LINE, INV, 1, 2>(a, tile, tw, offA_s, base_s, tid);
+        __syncthreads();  // tile and line bases free for the next tile
+    }
+}
+
 }  // namespace a2a

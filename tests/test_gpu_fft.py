@@ -178,12 +178,14 @@ def test_autotune_report(pkg, oracle, cuda):
 
 @pytest.mark.parametrize("inverse_first", [False, True])
 @pytest.mark.parametrize("P,shape", [(16, (512, 64, 64)), (16, (64, 512, 64)), (64, (512, 256, 128)),
-                                     (16, (1024, 64, 64)), (4, (64, 1024, 64))])
+                                     (16, (1024, 64, 64)), (4, (64, 1024, 64)), (16, (64, 64, 512)),
+                                     (4, (32, 64, 512))])
 def test_shuffle_exchange_variant(pkg, oracle, cuda, P, shape, inverse_first):
-    """The ring kernel whose first exchange runs through warp shuffles
-    (``tmat2s``: 512 = 8 x 8 x 8 and 1024 = 4 x 16 x 16, complex float batch
-    tiles), forced on every pass it fits, against the oracle's complex128
-    transform of the whole box (relative L2 <= 1e-6), in both directions."""
+    """The kernels whose first exchange runs through warp shuffles (the
+    batch-mode ring ``tmat2s``: 512 = 8 x 8 x 8 and 1024 = 4 x 16 x 16; the
+    line-mode register-pipelined ``rpipes``: 512), forced on every pass they
+    fit, against the oracle's complex128 transform of the whole box (relative
+    L2 <= 1e-6), in both directions."""
     import torch
 
     dist = pkg.a2aDistribution(P, shape, 64, precision="c64")
@@ -194,7 +196,7 @@ def test_shuffle_exchange_variant(pkg, oracle, cuda, P, shape, inverse_first):
     f.make_plans()
     forced = 0
     for p, line in enumerate(_pass_reports(f)):
-        idx = [i for i, ln in enumerate(line) if " tmat2s " in ln and "fits=1" in ln]
+        idx = [i for i, ln in enumerate(line) if (" tmat2s " in ln or " rpipes " in ln) and "fits=1" in ln]
         if idx:
             f.select_variant(p, idx[0])
             forced += 1
