@@ -178,7 +178,7 @@ def test_autotune_report(pkg, oracle, cuda):
 
 @pytest.mark.parametrize("inverse_first", [False, True])
 @pytest.mark.parametrize("P,shape", [(16, (512, 64, 64)), (16, (64, 512, 64)), (64, (512, 256, 128)),
-                                     (16, (1024, 64, 64)), (4, (64, 1024, 64)), (16, (64, 64, 512)),
+                                     (16, (1024, 64, 64)), (64, (64, 1024, 64)), (16, (64, 64, 512)),
                                      (4, (32, 64, 512))])
 def test_shuffle_exchange_variant(pkg, oracle, cuda, P, shape, inverse_first):
     """The kernels whose first exchange runs through warp shuffles (the
