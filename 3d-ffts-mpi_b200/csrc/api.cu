@@ -18,6 +18,7 @@
 #include <cuda_fp16.h>
 
 #include "batch.cuh"
+#include "fft_mb.cuh"
 #include "fft_tc.cuh"
 #include "internal.h"
 
@@ -49,6 +50,11 @@ struct a2a_dfft {
     const void* tc_b[2] = {nullptr, nullptr};
     // multi-block pass body: persistent register-pipelined where compiled
     bool mb_persistent = true;
+    // batch-mode multi-block passes: per-rank tensor maps (device memory),
+    // [pass 1, 2][rank], and what they were built for
+    void* d_mbmaps = nullptr;
+    std::vector<const void*> mbmaps_key[3];
+    int mbmaps_lines[3] = {0, 0, 0};
 };
 
 namespace {
@@ -1334,8 +1340,18 @@ a2a_status a2a_dfft_execute_pass_blocks(a2a_dfft* f, void** blocks, int nblocks,
     }
     const SlotGeom g = slot_geom(d, pass);
     PassKernel k;
-    const bool persistent = f->mb_persistent && a2a::find_mb_rpipe_kernel(d.prec, g.n, g.mode, inverse != 0, &k) &&
-                            g.NV % k.lines == 0;
+    // batch-mode passes: the TMA-fed kernel where its boxes fit the bricks
+    bool tma = false;
+    if (f->mb_persistent && g.mode == a2a::MODE_BATCH && a2a::find_mb_tmat_kernel(d.prec, g.n, inverse != 0, &k)) {
+        const int w = d.prec == A2A_C128 ? 2 : 1;
+        const int l = pass == 1 ? d.local[0] : d.local[1];
+        tma = g.NV % k.lines == 0 && d.local[2] % k.lines == 0 && l <= 256 && w * k.lines <= 256 &&
+              ((size_t)k.lines * l * d.elem_bytes) % 128 == 0 && (d.nlocal * d.elem_bytes) % 16 == 0 &&
+              d.P <= 4096 && tmap_encoder() != nullptr;
+    }
+    const bool persistent = tma || (f->mb_persistent &&
+                                    a2a::find_mb_rpipe_kernel(d.prec, g.n, g.mode, inverse != 0, &k) &&
+                                    g.NV % k.lines == 0);
     if (!persistent) {
         if (!a2a::find_mb_kernel(d.prec, g.n, g.mode, inverse != 0, &k))
             return fail(A2A_ERROR_UNSUPPORTED, "no multi-block pass kernel of length %d (lengths 4, 8, 16 have none)",
@@ -1359,6 +1375,49 @@ a2a_status a2a_dfft_execute_pass_blocks(a2a_dfft* f, void** blocks, int nblocks,
     const double scale = (inverse && pass == 2) ? 1.0 / ((double)d.ng[0] * d.ng[1] * d.ng[2]) : 1.0;
     const uint32_t block_elems = (uint32_t)((uint64_t)(d.P / nblocks) * d.nlocal);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    a2a::MbTmaMaps mm;
+    std::memset(&mm, 0, sizeof(mm));
+    if (tma) {
+        // one 3-D tensor map per virtual rank over its brick [x_l][y_l][z_l]
+        // at its block's address, box [B, 1, lx] (X) or [B, ly, 1] (Y) words;
+        // rebuilt when the blocks or the tile height change
+        const int w = d.prec == A2A_C128 ? 2 : 1;
+        const int lx = d.local[0], ly = d.local[1], lz = d.local[2];
+        std::vector<const void*> key(blocks, blocks + nblocks);
+        const size_t per = sizeof(CUtensorMap) * (size_t)d.P;
+        if (!f->d_mbmaps) A2A_CUDA(cudaMalloc(&f->d_mbmaps, 3 * per), "cudaMalloc(multi-block tensor maps)");
+        CUtensorMap* dmaps = reinterpret_cast<CUtensorMap*>(static_cast<char*>(f->d_mbmaps) + pass * per);
+        if (f->mbmaps_key[pass] != key || f->mbmaps_lines[pass] != k.lines) {
+            std::vector<CUtensorMap> hmaps((size_t)d.P);
+            const TmapEncodeFn enc = tmap_encoder();
+            const cuuint64_t dims[3] = {(cuuint64_t)w * lz, (cuuint64_t)ly, (cuuint64_t)lx};
+            const cuuint64_t strides[2] = {(cuuint64_t)lz * d.elem_bytes, (cuuint64_t)ly * lz * d.elem_bytes};
+            const cuuint32_t box[3] = {(cuuint32_t)(w * k.lines), (cuuint32_t)(pass == 1 ? 1 : ly),
+                                       (cuuint32_t)(pass == 1 ? lx : 1)};
+            const cuuint32_t estr[3] = {1, 1, 1};
+            const int L = d.P / nblocks;
+            for (int r = 0; r < d.P; ++r) {
+                void* base = static_cast<char*>(blocks[r / L]) + (size_t)(r % L) * d.nlocal * d.elem_bytes;
+                if (enc(&hmaps[r], CU_TENSOR_MAP_DATA_TYPE_INT64, 3, base, dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+                    return fail(A2A_ERROR_CUDA, "cuTensorMapEncodeTiled refused a brick of the multi-block pass");
+            }
+            A2A_CUDA(cudaStreamSynchronize(st), "cudaStreamSynchronize");  // earlier passes may read the old maps
+            A2A_CUDA(cudaMemcpy(dmaps, hmaps.data(), per, cudaMemcpyHostToDevice), "cudaMemcpy(tensor maps)");
+            f->mbmaps_key[pass] = key;
+            f->mbmaps_lines[pass] = k.lines;
+        }
+        mm.map = dmaps;
+        mm.pass = pass;
+        mm.lx = lx;
+        mm.ly = ly;
+        mm.lz = lz;
+        mm.words = w;
+        mm.d1 = d.dims[1];
+        mm.d2 = d.dims[2];
+        mm.nbox = pass == 1 ? d.dims[0] : d.dims[1];
+    }
     cudaError_t e;
     auto launch = [&](auto tag) {
         using T = decltype(tag);
@@ -1381,7 +1440,7 @@ a2a_status a2a_dfft_execute_pass_blocks(a2a_dfft* f, void** blocks, int nblocks,
         mb.nblk = nblocks;
         mb.tile0 = (int)t0;
         mb.tile1 = (int)t1;
-        void* args[] = {&a, &mb};
+        void* args[] = {&a, &mb, &mm};
         return cudaLaunchKernel(k.fn, dim3((unsigned)grid), dim3(k.threads), args, k.smem, st);
     };
     e = d.prec == A2A_C128 ? launch(double()) : launch(float());
@@ -1403,6 +1462,7 @@ a2a_status a2a_dfft_launches_per_transform(const a2a_dfft* f, int* out) {
 
 a2a_status a2a_dfft_destroy(a2a_dfft* f) {
     if (f && f->d_tc) cudaFree(f->d_tc);
+    if (f && f->d_mbmaps) cudaFree(f->d_mbmaps);
     delete f;
     return A2A_SUCCESS;
 }

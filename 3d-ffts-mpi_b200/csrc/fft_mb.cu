@@ -99,6 +99,47 @@ bool find_mb_rpipe_kernel(a2a_precision prec, int n, int mode, bool inverse, Pas
     return false;
 }
 
+// Batch-mode passes fed by TMA from per-rank tensor maps (N, lines, threads,
+// min blocks): the single-buffer ring kernel's tiles.
+template <typename T, int N, int B, int TH, int MB, bool INV> PassKernel make_mb_tmat_kernel() {
+    using P = typename PassPlan<T, N>::Plan;
+    PassKernel k;
+    k.fn = reinterpret_cast<const void*>(&fft_mb_tmat_kernel<T, P, B, TH, INV, MB>);
+    k.kind = KIND_TMAT2;
+    k.n = N;
+    k.threads = TH;
+    k.lines = B;
+    k.min_blocks = MB;
+    k.lpt = 1;
+    k.smem = mb_tmat_smem_bytes<T, P, B>();
+    k.nstages = P::S;
+    for (int s = 0; s < P::S; ++s) k.radix[s] = P::r[s];
+    k.twtotal = P::twtotal();
+    return k;
+}
+#define A2A_MB_TMAT_F32(X) X(256, 16, 256, 2) X(512, 8, 128, 2) X(1024, 4, 256, 2)
+#define A2A_MB_TMAT_F64(X) X(512, 4, 256, 2) X(1024, 4, 256, 1)
+
+bool find_mb_tmat_kernel(a2a_precision prec, int n, bool inverse, PassKernel* out) {
+#define A2A_MB_CASE(T_, N_, B_, TH_, MB_)                                                                   \
+    if (n == N_) {                                                                                          \
+        *out = inverse ? make_mb_tmat_kernel<T_, N_, B_, TH_, MB_, true>()                                  \
+                       : make_mb_tmat_kernel<T_, N_, B_, TH_, MB_, false>();                                \
+        return true;                                                                                        \
+    }
+#define A2A_MB_F32_CASE(N_, B_, TH_, MB_) A2A_MB_CASE(float, N_, B_, TH_, MB_)
+#define A2A_MB_F64_CASE(N_, B_, TH_, MB_) A2A_MB_CASE(double, N_, B_, TH_, MB_)
+    if (prec == A2A_C128) {
+        A2A_MB_TMAT_F64(A2A_MB_F64_CASE)
+    } else {
+        A2A_MB_TMAT_F32(A2A_MB_F32_CASE)
+    }
+#undef A2A_MB_F32_CASE
+#undef A2A_MB_F64_CASE
+#undef A2A_MB_CASE
+    return false;
+}
+
 bool find_mb_kernel_small(a2a_precision prec, int n, int mode, bool inverse, PassKernel* out) {
 #define A2A_MB_CASE(N_, B_, TH_, MB_)                                                                       \
     if (n == N_) {                                                                                          \

@@ -89,6 +89,8 @@ bool find_mb_kernel(a2a_precision prec, int n, int mode, bool inverse, PassKerne
 bool find_mb_kernel_small(a2a_precision prec, int n, int mode, bool inverse, PassKernel* out);  // 4-line tiles
 // the persistent register-pipelined multi-block kernel of length n, where compiled
 bool find_mb_rpipe_kernel(a2a_precision prec, int n, int mode, bool inverse, PassKernel* out);
+// the batch-mode multi-block kernel fed by TMA from per-rank tensor maps
+bool find_mb_tmat_kernel(a2a_precision prec, int n, bool inverse, PassKernel* out);
 
 // batch.cu: the batched persistent kernel per (precision, direction), its
 // dynamic shared memory, and the tile height of a length's variant (0: the

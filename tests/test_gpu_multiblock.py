@@ -140,7 +140,7 @@ def _worker(rank, world, port, P, ng, prec, q):
         raise
 
 
-@pytest.mark.parametrize("P,ng,prec", [(8, 64, "c64"), (16, 32, "c128")])
+@pytest.mark.parametrize("P,ng,prec", [(8, 64, "c64"), (16, 32, "c128"), (16, 256, "c64")])
 def test_fused_distributed_two_processes_one_gpu(cuda, P, ng, prec):
     world = 2
     ctx = mp.get_context("spawn")
