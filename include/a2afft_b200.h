@@ -274,13 +274,14 @@ a2a_status a2a_dfft_launches_per_transform(const a2a_dfft* dfft, int* out);
 a2a_status a2a_dfft_execute_pass_blocks(a2a_dfft* dfft, void** blocks, int nblocks, int pass, int inverse, int part,
                                         int nparts, void* cuda_stream);
 
-/* The kernel body a2a_dfft_execute_pass_blocks uses: 1 (default) one wave of
- * persistent CTAs per call, each working through its share of the part's
- * tiles with the next tile's gathers in flight in registers (the Z pass at
- * lengths 256, 512, 1024 complex float and 512, 1024 complex double; the
- * other passes keep one tile per CTA, which measured faster there), else 0:
- * one tile per CTA everywhere.  Both give the same result.  No reference
- * counterpart. */
+/* The kernel bodies a2a_dfft_execute_pass_blocks uses: 1 (default) one wave
+ * of persistent CTAs per call, each working through its share of the part's
+ * tiles -- the X and Y passes fed by TMA tensor-map copies of each brick
+ * (one map per virtual rank, built from `blocks` and kept until they change;
+ * plain loads, also from peer memory), the Z pass with the next tile's
+ * gathers in flight in registers -- at lengths 256, 512, 1024 complex float
+ * and 512, 1024 complex double where the tiles fit; elsewhere, or with 0, one
+ * tile per CTA.  All give the same result.  No reference counterpart. */
 a2a_status a2a_dfft_set_blocks_kernel(a2a_dfft* dfft, int persistent);
 
 /* Sharing a device buffer with another process (CUDA IPC): export writes an
