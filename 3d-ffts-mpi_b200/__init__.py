@@ -408,8 +408,9 @@ class a2adfft:
              int(nparts), ctypes.c_void_p(handle))
 
     def set_blocks_kernel(self, persistent: bool) -> None:
-        """Multi-block pass body: persistent register-pipelined CTAs (default,
-        where compiled) or one tile per CTA."""
+        """Multi-block pass bodies: persistent CTAs (default, where compiled
+        and the tiles fit: TMA-fed X and Y passes, register-pipelined Z pass)
+        or one tile per CTA everywhere."""
         call("a2a_dfft_set_blocks_kernel", self._h, int(bool(persistent)))
 
     @property

@@ -148,7 +148,6 @@ template <typename T, int N> struct PlanOf<T, N, KIND_TMAT2W> { using Plan = typ
     X(float,  768, KIND_PIPE,    8, 384, 1, 1)      \
     X(float,  768, KIND_DIRECT,  4, 128, 1, 1)      \
     X(float, 1024, KIND_DIRECT,  8, 512, 1, 1)      \
-    X(float, 1024, KIND_TMAT2S,  4, 128, 2, 1)      \
     X(float, 1024, KIND_DIRECT, 16, 512, 1, 2)      \
     X(float, 1024, KIND_RPIPE,   8, 512, 1, 1)      \
     X(float, 1024, KIND_TMA,     8, 512, 1, 1)      \

@@ -236,6 +236,10 @@ class FusedDistributedDfft:
 
         if self.blocks is None:
             raise RuntimeError("bind() first")
+        if self.G == 1:  # one process: the passes are ordered by its stream
+            for p in range(3):
+                self.dfft.execute_pass_blocks(self.blocks, p, inverse, 0, 1)
+            return
         torch.cuda.synchronize()
         tdist.barrier(group=self.group)  # every block holds its input
         for p in range(3):
