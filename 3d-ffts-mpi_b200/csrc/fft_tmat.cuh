@@ -236,8 +236,10 @@ __global__ void __launch_bounds__(THREADS, MINB) fft_tmat_kernel(const PassArgs<
 
 // KIND_TMAT2S: the 2-slot ring for batch-mode tiles of complex float (128
 // threads) whose first two stages exchange through warp shuffles instead of
-// shared memory.  Plans R0 x R1 x R2 with R0 R1 = 64: 512 = 8 x 8 x 8 (8-line
-// tiles) and 1024 = 4 x 16 x 16 (4-line tiles).
+// shared memory.  Plans R0 x R1 x R2 with R0 R1 = 64; registered for 512 =
+// 8 x 8 x 8 (8-line tiles).  (1024 = 4 x 16 x 16 would take 4-line tiles,
+// 32-byte rows; measured at 1024^3 it ran the X pass in 9.0 ms against 3.4 ms
+// for the wide-radix ring, so it is not registered.)
 //
 // Stage 0's radix-R0 butterfly j writes positions R0 j + r, and stage 1's
 // radix-R1 butterfly j' reads j' + (N / R1) r'': so with NG = N / 64 the R1
