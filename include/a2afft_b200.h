@@ -277,7 +277,8 @@ a2a_status a2a_dfft_execute_pass_blocks(a2a_dfft* dfft, void** blocks, int nbloc
 /* The kernel bodies a2a_dfft_execute_pass_blocks uses: 1 (default) one wave
  * of persistent CTAs per call, each working through its share of the part's
  * tiles -- the X and Y passes fed by TMA tensor-map copies of each brick
- * (one map per virtual rank, built from `blocks` and kept until they change;
+ * (one map per virtual rank, built from `blocks` and kept until they change,
+ * so calls of one dfft with different `blocks` must not overlap on the GPU;
  * plain loads, also from peer memory), the Z pass with the next tile's
  * gathers in flight in registers -- at lengths 256, 512, 1024 complex float
  * and 512, 1024 complex double where the tiles fit; elsewhere, or with 0, one
