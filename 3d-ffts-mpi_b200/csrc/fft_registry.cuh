@@ -130,13 +130,11 @@ template <typename T, int N> struct PlanOf<T, N, KIND_TMAT2W> { using Plan = typ
     X(float,  512, KIND_RPIPE,  16, 512, 1, 2)      \
     X(float,  512, KIND_RPIPE,   8, 256, 2, 1)      \
     X(float,  512, KIND_RPIPES,  8, 128, 2, 1)      \
+    X(float,  512, KIND_RPIPE,   8, 256, 3, 1)      \
     X(float,  512, KIND_DIRECT, 16, 512, 1, 2)      \
     X(float,  512, KIND_DIRECT,  8, 128, 4, 1)      \
     X(float,  512, KIND_RPIPE,  16, 512, 1, 1)      \
     X(float,  512, KIND_RPIPE,  16, 256, 1, 2)      \
-    X(float,  512, KIND_TMA,    16, 512, 1, 2)      \
-    X(float,  512, KIND_TMA,    16, 256, 1, 2)      \
-    X(float,  512, KIND_TMA,     8, 256, 2, 2)      \
     X(float,  512, KIND_DIRECT, 16, 256, 2, 2)      \
     X(float,  512, KIND_DIRECT, 16, 256, 2, 1)      \
     X(float,  512, KIND_DIRECT,  8, 128, 4, 2)      \
