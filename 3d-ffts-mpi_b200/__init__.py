@@ -516,10 +516,15 @@ class a2aBatch:
     def make_plans(self, d_scratch=None) -> None:
         call("a2a_batch_make_plans", self._h, None if d_scratch is None else self._ptrs(d_scratch))
 
-    def set_schedule(self, fused: bool = True, claim: int = 16, prefetch: bool = True) -> None:
+    def set_schedule(self, fused: bool = True, claim: int = 16, prefetch: bool = True,
+                     grouped: bool = False) -> None:
         """One launch per direction (``fused``) or one per pass; work items
-        a CTA takes per queue access; L2 prefetch of each CTA's next tile."""
-        call("a2a_batch_set_schedule", self._h, int(bool(fused)), int(claim), int(bool(prefetch)))
+        a CTA takes per queue access; L2 prefetch of each CTA's next tile.
+        ``grouped``: instead, the boxes of each shape as one tall grid per
+        pass through the single-grid pass kernels, the shapes on parallel
+        stream branches (``claim`` and ``prefetch`` then do not apply)."""
+        call("a2a_batch_set_schedule", self._h, 2 if grouped else int(bool(fused)), int(claim),
+             int(bool(prefetch)))
 
     def select_variant(self, length: int, batch_mode: bool, variant: int) -> None:
         call("a2a_batch_select_variant", self._h, int(length), int(bool(batch_mode)), int(variant))

@@ -342,6 +342,12 @@ cudaError_t launch_pass_t(const PassKernel& k, unsigned grid, const void* src, v
     return cudaLaunchKernel(k.fn, dim3(grid), dim3(k.threads), args, k.smem, st);
 }
 
+// Kernels whose CTAs stay resident and stride over the tiles (grid: one wave).
+bool persistent_kind(const PassKernel& k) {
+    return k.kind == a2a::KIND_PIPE || k.kind == a2a::KIND_TMA || k.kind == a2a::KIND_RPIPE ||
+           k.kind == a2a::KIND_RPIPES || is_tmat(k);
+}
+
 // Launch candidate `c` of a slot on buffer p (in place).
 cudaError_t launch_slot(const Dist& d, int slot, bool inv, int c, void* p, double scale, cudaStream_t st) {
     const a2a::PassSlot& ps = d.slot[slot][inv ? 1 : 0];
@@ -349,8 +355,7 @@ cudaError_t launch_slot(const Dist& d, int slot, bool inv, int c, void* p, doubl
     const SlotGeom g = slot_geom(d, slot);
     const uint64_t tiles = (uint64_t)g.NU * (g.NV / k.lines);
     uint64_t grid = tiles;
-    if (k.kind == a2a::KIND_PIPE || k.kind == a2a::KIND_TMA || k.kind == a2a::KIND_RPIPE ||
-        k.kind == a2a::KIND_RPIPES || is_tmat(k)) {
+    if (persistent_kind(k)) {
         const uint64_t resident = (uint64_t)std::max(ps.occ[c], 1) * d.sms;
         grid = std::min(tiles, resident);
     }
@@ -1719,6 +1724,30 @@ struct a2a_batch {
     cudaStream_t cap = nullptr;
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     std::vector<void*> bound;  // data pointers held in d_boxes
+
+    // Grouped schedule (fused == 2): the boxes of one shape form one tall
+    // grid per pass (line bases = box offset + the shape's own outer-line
+    // offsets, from the group's lowest box pointer), transformed by the
+    // single-grid pass kernels, one launch per (shape, pass); the shapes run
+    // on parallel branches (forked streams, a graph with one branch per shape
+    // when captured).
+    struct Group {
+        int dist = 0;                  // index into dists
+        std::vector<int> boxes;        // its boxes, in box order
+        int64_t elems = 0;             // elements of all its boxes
+        size_t tab[3] = {0, 0, 0};     // start of its per-pass line-base tables in d_gtab
+        int chosen[3] = {-1, -1, -1};  // candidate per pass in the distribution's slot lists
+        float tuned_ms[3][a2a::kMaxVariants] = {};
+        void* base = nullptr;          // lowest box pointer of the bound buffers
+    };
+    std::vector<Group> groups;         // largest first
+    bool grouped_possible = false;     // every (shape, pass) has a kernel the grouped schedule can run
+    bool grouped_ok = false;           // the bound buffers' offsets fit the 32-bit line-base tables
+    uint32_t* d_gtab = nullptr;
+    size_t gtab_entries = 0;
+    std::vector<cudaStream_t> gstreams;
+    cudaEvent_t gfork = nullptr;
+    std::vector<cudaEvent_t> gjoin;
 };
 
 namespace {
@@ -1743,6 +1772,97 @@ void batch_pass_geom(const a2a_batch* b, int i, int pass, int& n, int& NU, int& 
     if (pass == 0) { n = d.ng[2]; NU = d.ng[0]; NV = d.ng[1]; }
     else if (pass == 1) { n = d.ng[0]; NU = d.ng[1]; NV = d.ng[2]; }
     else { n = d.ng[1]; NU = d.ng[0]; NV = d.ng[2]; }
+}
+
+// Can the grouped schedule run candidate c of pass `pass` of shape d?  Both
+// directions must have it fitting the shape's geometry, and it must address
+// its lines through the offset tables (the tensor-map ring kernels describe
+// one buffer per map, so a tall grid of boxes is not one tensor).  The
+// geometry checks carry over from one box to the group: line bases only gain
+// box offsets, which are multiples of 16 bytes.
+bool group_eligible(const Dist& d, int pass, int c) {
+    for (int inv = 0; inv < 2; ++inv) {
+        const a2a::PassSlot& ps = d.slot[pass][inv];
+        if (c < 0 || c >= ps.ncand || !ps.fits[c] || is_tmat(ps.cand[c])) return false;
+    }
+    return true;
+}
+
+// One pass of one group: the chosen single-grid kernel over the group's tall
+// grid (K boxes x NU outer lines), in place from the group's base pointer.
+cudaError_t group_pass(const a2a_batch* b, const a2a_batch::Group& g, int pass, bool inv, cudaStream_t st) {
+    const Dist& d = b->dists[g.dist]->d;
+    const int c = g.chosen[pass];
+    const a2a::PassSlot& ps = d.slot[pass][inv ? 1 : 0];
+    const PassKernel& k = ps.cand[c];
+    const SlotGeom geo = slot_geom(d, pass);
+    const uint64_t NU = (uint64_t)geo.NU * g.boxes.size();
+    const uint64_t tiles = NU * (uint64_t)(geo.NV / k.lines);
+    uint64_t grid = tiles;
+    if (persistent_kind(k)) grid = std::min(tiles, (uint64_t)std::max(ps.occ[c], 1) * d.sms);
+    const int l = pass == 0 ? d.local[2] : pass == 1 ? d.local[0] : d.local[1];
+    const int split = split_ok(l, k);
+    const void* tw = ps.tw[c] ? ps.tw[c] : geo.tw;
+    const double scale = (inv && pass == 2) ? 1.0 / ((double)d.ng[0] * d.ng[1] * d.ng[2]) : 1.0;
+    const uint32_t* offU = b->d_gtab + g.tab[pass];
+    int* err = b->d_queue + b->queue_ints;
+    if (b->prec == A2A_C128)
+        return launch_pass_t<double>(k, unsigned(grid), g.base, g.base, geo.offA, offU, geo.offV, tw, (int)NU,
+                                     geo.NV, scale, split, err, st);
+    return launch_pass_t<float>(k, unsigned(grid), g.base, g.base, geo.offA, offU, geo.offV, tw, (int)NU, geo.NV,
+                                scale, split, err, st);
+}
+
+// One direction of the grouped schedule: fork the caller's stream into the
+// group streams, Z, X, Y of each group on its stream, join back.
+cudaError_t batch_group_launches(a2a_batch* b, bool inv, cudaStream_t st) {
+    cudaError_t e = cudaEventRecord(b->gfork, st);
+    for (size_t gi = 0; gi < b->groups.size() && e == cudaSuccess; ++gi) {
+        cudaStream_t s = b->gstreams[gi % b->gstreams.size()];
+        e = cudaStreamWaitEvent(s, b->gfork, 0);
+        for (int p = 0; p < 3 && e == cudaSuccess; ++p) e = group_pass(b, b->groups[gi], p, inv, s);
+        if (e == cudaSuccess) e = cudaEventRecord(b->gjoin[gi], s);
+    }
+    for (size_t gi = 0; gi < b->groups.size() && e == cudaSuccess; ++gi) e = cudaStreamWaitEvent(st, b->gjoin[gi], 0);
+    return e;
+}
+
+// Line-base tables of every group for the bound buffers: entry (k, u) of
+// pass p = (box k's pointer - group base) / element size + the shape's outer
+// offset u.  Sets grouped_ok (false when some group's boxes lie too far apart
+// for 32-bit element offsets; the grouped schedule then runs as the one-launch
+// schedule).  Returns whether any group's base pointer changed.
+bool batch_group_tables(a2a_batch* b, cudaStream_t st, cudaError_t* err) {
+    *err = cudaSuccess;
+    b->grouped_ok = false;
+    if (!b->grouped_possible) return false;
+    bool moved = false;
+    std::vector<uint32_t> h(b->gtab_entries);
+    const size_t eb = b->prec == A2A_C128 ? 16 : 8;
+    for (a2a_batch::Group& g : b->groups) {
+        const Dist& d = b->dists[g.dist]->d;
+        uintptr_t lo = UINTPTR_MAX;
+        for (int i : g.boxes) lo = std::min(lo, reinterpret_cast<uintptr_t>(b->bound[i]));
+        std::vector<uint64_t> boff;
+        for (int i : g.boxes) {
+            const uint64_t o = (reinterpret_cast<uintptr_t>(b->bound[i]) - lo) / eb;  // pointers are 16-byte aligned
+            if (o + d.nlocal * (uint64_t)d.P > (uint64_t(1) << 32)) return moved;
+            boff.push_back(o);
+        }
+        if (g.base != reinterpret_cast<void*>(lo)) moved = true;
+        g.base = reinterpret_cast<void*>(lo);
+        for (int p = 0; p < 3; ++p) {
+            const std::vector<uint32_t>& hU = *slot_geom(d, p).hU;
+            size_t pos = g.tab[p];
+            for (uint64_t o : boff)
+                for (uint32_t u : hU) h[pos++] = (uint32_t)(o + u);
+        }
+    }
+    // pageable source: staged before the call returns, ordered before the
+    // launches that follow on `st`
+    *err = cudaMemcpyAsync(b->d_gtab, h.data(), h.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st);
+    b->grouped_ok = *err == cudaSuccess;
+    return moved;
 }
 
 // Tiles per pass, the item list, launch shared memory and grid from the
@@ -1798,23 +1918,25 @@ a2a_status batch_layout(a2a_batch* b) {
 // Enqueues one direction: clear the queue counters, then the persistent
 // launch (or one launch per pass).
 cudaError_t batch_launches(a2a_batch* b, bool inv, cudaStream_t st) {
+    if (b->fused == 2 && b->grouped_ok) return batch_group_launches(b, inv, st);
     cudaError_t e = cudaMemsetAsync(b->d_queue, 0, b->queue_ints * sizeof(int), st);
     if (e != cudaSuccess) return e;
     const void* fn = a2a::batch_kernel(b->prec, inv);
+    const int fused = b->fused == 0 ? 0 : 1;  // the grouped schedule without usable tables: one launch
     a2a::BatchArgs a;
     a.boxes = b->d_boxes;
     a.items = b->d_items;
     a.claim = b->claim;
-    a.fused = b->fused;
+    a.fused = fused;
     a.wait_extra = b->wait_extra;
     a.prefetch = b->prefetch;
     a.abort = b->d_queue;
     a.done = b->d_queue + 4;
     a.err = b->d_queue + b->queue_ints;
-    const int launches = b->fused ? 1 : 3;
+    const int launches = fused ? 1 : 3;
     for (int k = 0; k < launches && e == cudaSuccess; ++k) {
-        a.item_lo = b->fused ? 0 : b->pass_start[k];
-        a.item_hi = b->fused ? b->pass_start[3] : b->pass_start[k + 1];
+        a.item_lo = fused ? 0 : b->pass_start[k];
+        a.item_hi = fused ? b->pass_start[3] : b->pass_start[k + 1];
         a.taken = b->d_queue + 1 + k;
         const int grid = std::max(1, std::min(a.item_hi - a.item_lo, b->grid));
         void* args[] = {&a};
@@ -1863,6 +1985,13 @@ a2a_status batch_bind(a2a_batch* b, void** data, cudaStream_t st) {
     A2A_CUDA(cudaMemcpyAsync(b->d_boxes, b->hbox.data(), b->hbox.size() * sizeof(a2a::BatchBox),
                              cudaMemcpyHostToDevice, st),
              "cudaMemcpyAsync(batch boxes)");
+    // the grouped schedule's launches carry the group base pointers: a
+    // captured graph of them is stale once a base moves
+    const bool was_ok = b->grouped_ok;
+    cudaError_t e = cudaSuccess;
+    const bool moved = batch_group_tables(b, st, &e);
+    A2A_CUDA(e, "cudaMemcpyAsync(batch group tables)");
+    if (b->fused == 2 && (moved || was_ok != b->grouped_ok)) batch_drop_graphs(b);
     return A2A_SUCCESS;
 }
 
@@ -1899,11 +2028,68 @@ void batch_free(a2a_batch* b) {
     if (b->d_boxes) cudaFree(b->d_boxes);
     if (b->d_items) cudaFree(b->d_items);
     if (b->d_queue) cudaFree(b->d_queue);
+    if (b->d_gtab) cudaFree(b->d_gtab);
+    for (cudaStream_t s : b->gstreams) cudaStreamDestroy(s);
+    if (b->gfork) cudaEventDestroy(b->gfork);
+    for (cudaEvent_t ev : b->gjoin) cudaEventDestroy(ev);
     for (a2a_distribution* h : b->dists) {
         release(h->d);
         delete h;
     }
     delete b;
+}
+
+// The grouped schedule's groups (one per box shape, largest first), their
+// table space, streams and events, and default kernels (each pass's
+// single-grid default where the grouped schedule can run it, else the first
+// candidate it can).
+a2a_status batch_groups_setup(a2a_batch* b) {
+    b->groups.clear();
+    for (int k = 0; k < (int)b->dists.size(); ++k) {
+        a2a_batch::Group g;
+        g.dist = k;
+        const Dist& d = b->dists[k]->d;
+        for (int i = 0; i < b->nboxes; ++i)
+            if (b->box_dist[i] == k) g.boxes.push_back(i);
+        g.elems = (int64_t)g.boxes.size() * (int64_t)(d.nlocal * d.P);
+        b->groups.push_back(g);
+    }
+    std::stable_sort(b->groups.begin(), b->groups.end(),
+                     [](const a2a_batch::Group& x, const a2a_batch::Group& y) { return x.elems > y.elems; });
+    b->grouped_possible = true;
+    size_t pos = 0;
+    for (a2a_batch::Group& g : b->groups) {
+        const Dist& d = b->dists[g.dist]->d;
+        for (int p = 0; p < 3; ++p) {
+            const SlotGeom geo = slot_geom(d, p);
+            g.tab[p] = pos;
+            pos += (size_t)geo.NU * g.boxes.size();
+            // a tall grid's tile count stays an int in the kernels
+            if ((uint64_t)geo.NU * g.boxes.size() * geo.NV >= (uint64_t(1) << 31)) b->grouped_possible = false;
+            const int def = d.slot[p][0].chosen;
+            int pick = group_eligible(d, p, def) ? def : -1;
+            for (int c = 0; c < d.slot[p][0].ncand && pick < 0; ++c)
+                if (group_eligible(d, p, c)) pick = c;
+            if (pick < 0) b->grouped_possible = false;
+            g.chosen[p] = pick;
+        }
+    }
+    b->gtab_entries = pos;
+    if (!b->grouped_possible) return A2A_SUCCESS;
+    A2A_CUDA(cudaMalloc(&b->d_gtab, std::max<size_t>(pos, 1) * sizeof(uint32_t)), "cudaMalloc(batch group tables)");
+    const size_t ns = std::min<size_t>(b->groups.size(), 8);
+    for (size_t i = 0; i < ns; ++i) {
+        cudaStream_t s = nullptr;
+        A2A_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate(batch group)");
+        b->gstreams.push_back(s);
+    }
+    A2A_CUDA(cudaEventCreateWithFlags(&b->gfork, cudaEventDisableTiming), "cudaEventCreate");
+    for (size_t i = 0; i < b->groups.size(); ++i) {
+        cudaEvent_t ev = nullptr;
+        A2A_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
+        b->gjoin.push_back(ev);
+    }
+    return A2A_SUCCESS;
 }
 
 }  // namespace
@@ -2046,7 +2232,7 @@ a2a_status a2a_batch_create(int nboxes, const int* shapes, int world_size, a2a_p
         batch_free(b);
         return cuda_fail(e, "batch set-up");
     }
-    if ((s = batch_layout(b)) != A2A_SUCCESS) {
+    if ((s = batch_groups_setup(b)) != A2A_SUCCESS || (s = batch_layout(b)) != A2A_SUCCESS) {
         batch_free(b);
         return s;
     }
@@ -2064,7 +2250,11 @@ a2a_status a2a_batch_box_elements(const a2a_batch* b, int box, int64_t* elements
 
 a2a_status a2a_batch_set_schedule(a2a_batch* b, int fused, int claim, int prefetch) {
     if (!b) return fail(A2A_ERROR_INVALID_VALUE, "batch is NULL");
-    if (fused != 0 && fused != 1) return fail(A2A_ERROR_INVALID_VALUE, "fused must be 0 or 1");
+    if (fused < 0 || fused > 2) return fail(A2A_ERROR_INVALID_VALUE, "fused must be 0, 1 or 2");
+    if (fused == 2 && !b->grouped_possible)
+        return fail(A2A_ERROR_UNSUPPORTED,
+                    "the grouped schedule needs, for every box shape and pass, a single-grid kernel that addresses "
+                    "its lines through the offset tables");
     if (claim < 1 || claim > 64) return fail(A2A_ERROR_INVALID_VALUE, "claim must be in [1, 64]");
     if (prefetch != 0 && prefetch != 1) return fail(A2A_ERROR_INVALID_VALUE, "prefetch must be 0 or 1");
     b->fused = fused;
@@ -2119,6 +2309,7 @@ a2a_status a2a_batch_make_plans(a2a_batch* b, void** d_scratch) {
     A2A_CUDA(cudaEventCreate(&e1), "cudaEventCreate");
     const bool graph = b->use_graph;
     b->use_graph = false;
+    b->fused = b->fused == 0 ? 0 : 1;  // the tile sweep times the persistent kernel
     // forward + inverse per trial (the inverse keeps the scratch values bounded)
     auto timed = [&](float* out) -> a2a_status {
         cudaError_t e = cudaSuccess;
@@ -2182,6 +2373,46 @@ a2a_status a2a_batch_make_plans(a2a_batch* b, void** d_scratch) {
     try_knob(&b->fused, 1 - b->fused);
     for (int c : {4, 8, 16, 32, 64}) try_knob(&b->claim, c);
     try_knob(&b->prefetch, 1 - b->prefetch);
+    // the grouped schedule: per (shape, pass) the fastest single-grid kernel
+    // it can run (forward + inverse pass on the group alone), then the
+    // whole grouped transform against the persistent schedule
+    if (s == A2A_SUCCESS && b->grouped_possible && b->grouped_ok) {
+        for (a2a_batch::Group& g : b->groups) {
+            const Dist& d = b->dists[g.dist]->d;
+            for (int p = 0; p < 3 && s == A2A_SUCCESS; ++p) {
+                int best = g.chosen[p];
+                float bt = 1e30f;
+                for (int c = 0; c < d.slot[p][0].ncand && s == A2A_SUCCESS; ++c) {
+                    if (!group_eligible(d, p, c)) continue;
+                    g.chosen[p] = c;
+                    cudaError_t e = cudaSuccess;
+                    float t = 1e30f;
+                    for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {
+                        e = cudaEventRecord(e0, st);
+                        if (e == cudaSuccess) e = group_pass(b, g, p, false, st);
+                        if (e == cudaSuccess) e = group_pass(b, g, p, true, st);
+                        if (e == cudaSuccess) e = cudaEventRecord(e1, st);
+                        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+                        float x = 0.f;
+                        if (e == cudaSuccess) e = cudaEventElapsedTime(&x, e0, e1);
+                        if (e == cudaSuccess && rep > 0) t = std::min(t, x);
+                    }
+                    if (e != cudaSuccess) {
+                        s = cuda_fail(e, "grouped autotune launch");
+                        break;
+                    }
+                    if ((s = batch_check_flag(b)) != A2A_SUCCESS) break;
+                    g.tuned_ms[p][c] = t;
+                    if (t < bt) {
+                        bt = t;
+                        best = c;
+                    }
+                }
+                g.chosen[p] = best;
+            }
+        }
+        try_knob(&b->fused, 2);
+    }
     b->use_graph = graph;
     batch_drop_graphs(b);
     cudaEventDestroy(e0);
@@ -2195,9 +2426,28 @@ a2a_status a2a_batch_plan_report(const a2a_batch* b, char* buf, size_t len) {
     char line[256];
     snprintf(line, sizeof line,
              "boxes=%d world_size=%d precision=%s schedule=%s claim=%d prefetch=%d grid=%d smem=%zu items=%d\n",
-             b->nboxes, b->P, b->prec == A2A_C128 ? "c128" : "c64", b->fused ? "one-launch" : "per-pass", b->claim,
-             b->prefetch, b->grid, b->smem, b->pass_start[3]);
+             b->nboxes, b->P, b->prec == A2A_C128 ? "c128" : "c64",
+             b->fused == 2 ? (b->grouped_ok ? "grouped" : "grouped(unusable offsets: one-launch)")
+             : b->fused ? "one-launch" : "per-pass",
+             b->claim, b->prefetch, b->grid, b->smem, b->pass_start[3]);
     r += line;
+    if (b->grouped_possible)
+        for (const a2a_batch::Group& g : b->groups) {
+            const Dist& d = b->dists[g.dist]->d;
+            snprintf(line, sizeof line, "  group %dx%dx%d boxes=%zu:", d.ng[0], d.ng[1], d.ng[2], g.boxes.size());
+            r += line;
+            const char* names[3] = {"Z", "X", "Y"};
+            for (int p = 0; p < 3; ++p) {
+                const int c = g.chosen[p];
+                const PassKernel& k = d.slot[p][0].cand[c];
+                snprintf(line, sizeof line, " %s %s lines=%d lpt=%d threads=%d (tuned ms %.4f)", names[p],
+                         k.kind == a2a::KIND_PIPE ? "pipe" : k.kind == a2a::KIND_TMA ? "tma"
+                         : k.kind == a2a::KIND_RPIPE ? "rpipe" : k.kind == a2a::KIND_RPIPES ? "rpipes" : "direct",
+                         k.lines, k.lpt, k.threads, g.tuned_ms[p][c]);
+                r += line;
+            }
+            r += "\n";
+        }
     for (int m = 0; m < 2; ++m)
         for (int li = 0; li < a2a::kBatchNumLengths; ++li) {
             if (!b->used[m][li]) continue;
@@ -2228,7 +2478,7 @@ a2a_status a2a_batch_check_device(a2a_batch* b) {
 
 a2a_status a2a_batch_launches_per_transform(const a2a_batch* b, int* out) {
     if (!b || !out) return fail(A2A_ERROR_INVALID_VALUE, "NULL argument");
-    *out = b->fused ? 1 : 3;
+    *out = (b->fused == 2 && b->grouped_ok) ? 3 * (int)b->groups.size() : b->fused ? 1 : 3;
     return A2A_SUCCESS;
 }
 

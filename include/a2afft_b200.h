@@ -357,7 +357,18 @@ a2a_status a2a_batch_make_plans(a2a_batch* batch, void** d_scratch);
 /* fused = 1: one launch per direction (later passes wait, device-side, for
  * the earlier pass of their box); 0: one launch per pass.  claim: most work
  * items a CTA takes per queue access (1..64; fewer as the queue drains).  prefetch = 1: each CTA asks L2 for
- * its next tile while it transforms the current one. */
+ * its next tile while it transforms the current one.
+ * fused = 2 (grouped): the boxes of each shape form one tall grid per pass
+ * (line bases: box offset from the shape's lowest box pointer + the shape's
+ * own line offsets) transformed by the single-grid pass kernels, one launch
+ * per (shape, pass), each shape's three passes on its own stream branch
+ * forked from and joined back to the caller's stream (parallel branches of
+ * the captured graph).  claim and prefetch do not apply.  Needs, per shape
+ * and pass, a kernel that addresses lines through the offset tables
+ * (A2A_ERROR_UNSUPPORTED otherwise), and every shape's boxes within 2^32
+ * elements of one another in the bound buffers; where they are not, calls
+ * run the fused = 1 schedule.  make_plans picks per (shape, pass) the kernel
+ * and then times this schedule against the others. */
 a2a_status a2a_batch_set_schedule(a2a_batch* batch, int fused, int claim, int prefetch);
 /* Tile choice for one length in line (batch_mode = 0, the Z pass) or batch
  * mode (the X and Y passes): 0 and 1 are two tile heights; 2 (batch mode,

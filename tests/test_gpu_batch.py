@@ -1,8 +1,9 @@
 """Batched form (``a2a_batch_*``: many boxes, one persistent launch per
-direction) against the FP64 oracle, against the single-grid plan
-(``a2a_dfft_*``) box by box, across its schedules, and its bounded-wait
-timeout path.  Tolerances as for the single-grid transform: relative L2
-error <= 1e-6 for complex64, <= 1e-12 for complex128."""
+direction, or the grouped schedule through the single-grid pass kernels)
+against the FP64 oracle, against the single-grid plan (``a2a_dfft_*``) box
+by box, across its schedules, and its bounded-wait timeout path.
+Tolerances as for the single-grid transform: relative L2 error <= 1e-6 for
+complex64, <= 1e-12 for complex128."""
 import numpy as np
 import pytest
 
@@ -98,6 +99,66 @@ def test_batch_schedules_agree_bitwise(pkg, oracle, cuda, fused, claim, prefetch
     assert torch.equal(flat, flat2)
 
 
+# repeated shapes, so that groups hold several boxes
+GROUPED = SMALL + [(32, 32, 32), (64, 64, 64), (32, 64, 128), (32, 64, 128), (192, 32, 64)]
+
+
+@pytest.mark.parametrize("prec,graph", [("c64", True), ("c64", False), ("c128", True)])
+def test_batch_grouped_schedule_vs_oracle(pkg, oracle, cuda, prec, graph):
+    """The grouped schedule: the boxes of each shape as one tall grid per
+    pass through the single-grid pass kernels, the shapes on parallel stream
+    branches (one graph branch per shape when captured)."""
+    import torch
+
+    P = 4
+    b = pkg.a2aBatch(GROUPED, P, prec)
+    b.set_schedule(grouped=True)
+    b.set_graph(graph)
+    flat, views, inputs = fill(pkg, oracle, cuda, b, prec, seed=31)
+    assert b.launches_per_transform == 1  # nothing bound yet: no group tables
+    s = torch.cuda.Stream()
+    b.forward(views, stream=s)
+    s.synchronize()
+    b.check_device()
+    assert b.launches_per_transform == 3 * len(set(GROUPED))
+    assert "schedule=grouped " in b.plan_report()
+    for i, (g, d) in enumerate(inputs):
+        ref = oracle.fft3_global(g, lines=oracle.fft_lines)
+        e = oracle.rel_l2(to_global(oracle, views[i], d, P), ref)
+        assert e <= TOL[prec], f"box {i} {b.shapes[i]} forward rel L2 {e:.3e}"
+    b.inverse(views, stream=s)
+    s.synchronize()
+    b.check_device()
+    for i, (g, d) in enumerate(inputs):
+        e = oracle.rel_l2(to_global(oracle, views[i], d, P), g)
+        assert e <= TOL[prec], f"box {i} {b.shapes[i]} round trip rel L2 {e:.3e}"
+
+
+def test_batch_grouped_matches_single_grid_and_rebinds(pkg, oracle, cuda):
+    """Grouped results equal each box's own single-grid plan; binding other
+    buffers (the groups' base pointers move) rebuilds the line-base tables
+    and the captured graph."""
+    import torch
+
+    P, prec = 4, "c64"
+    b = pkg.a2aBatch(GROUPED, P, prec)
+    b.set_schedule(grouped=True)
+    for seed in (41, 43):  # two different allocations in turn
+        flat, views, _ = fill(pkg, oracle, cuda, b, prec, seed=seed)
+        singles = [v.clone() for v in views]
+        b.forward(views)
+        for i, shp in enumerate(b.shapes):
+            dist = pkg.a2aDistribution(P, shp, 64, precision=prec)
+            f = pkg.a2adfft(dist)
+            f.make_plans()
+            f.forward(singles[i])
+            e = oracle.rel_l2(views[i].cpu().numpy(), singles[i].cpu().numpy())
+            assert e <= TOL[prec], f"seed {seed} box {i} {shp}: grouped vs single-grid rel diff {e:.3e}"
+            f.destroy()
+            dist.finalize()
+        torch.cuda.synchronize()
+
+
 def test_batch_line_pairs_bit_identical(pkg, oracle, cuda):
     """Variant 2 (batch mode, each thread moving two adjacent lines as one
     16-byte access) computes every line exactly as variant 0 does."""
@@ -169,16 +230,20 @@ def test_batch_wait_timeout_is_reported_and_recoverable(pkg, oracle, cuda):
         assert oracle.rel_l2(to_global(oracle, views[i], d, P), ref) <= TOL[prec]
 
 
-def test_batch_measured_workload_properties(pkg, oracle, cuda):
+@pytest.mark.parametrize("grouped", [False, True])
+def test_batch_measured_workload_properties(pkg, oracle, cuda, grouped):
     """The measured batch (96 cubes with edges drawn from 32..192, seed 3,
     plus two 128x256x512 boxes; 4 virtual ranks each, N(0,1) input):
-    exact DFT at sample points, Parseval and the round trip, per box."""
+    exact DFT at sample points, Parseval and the round trip, per box, in
+    the one-launch and the grouped schedule."""
     import torch
 
     P, prec = 4, "c64"
     shapes = pkg.batch_shapes()
     assert len(shapes) == 98
     b = pkg.a2aBatch(shapes, P, prec)
+    if grouped:
+        b.set_schedule(grouped=True)
     flat, views = b.empty(cuda)
     gen = torch.Generator(device=cuda)
     gen.manual_seed(3)
