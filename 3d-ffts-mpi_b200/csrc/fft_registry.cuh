@@ -188,7 +188,13 @@ template <typename T, int N> struct PlanOf<T, N, KIND_TMAT2W> { using Plan = typ
     X(float,  512, KIND_TMATI,   8, 128, 3, 2)      \
     X(float,  512, KIND_TMAT3,   8, 128, 2, 2)      \
     X(float, 1024, KIND_TMAT2,   4, 128, 2, 2)      \
-    X(float, 1024, KIND_TMATI,   4, 128, 3, 2)
+    X(float, 1024, KIND_TMATI,   4, 128, 3, 2)      \
+    X(float,   96, KIND_RPIPE,  32, 128, 3, 1)      \
+    X(float,   96, KIND_RPIPE,  16, 128, 4, 1)      \
+    X(float,  128, KIND_RPIPE,  16, 128, 4, 1)      \
+    X(float,  128, KIND_RPIPE,  32, 256, 2, 1)      \
+    X(float,  192, KIND_RPIPE,  16, 256, 2, 1)      \
+    X(float,  192, KIND_RPIPE,   8, 128, 4, 1)
 
 #define A2A_VARIANTS_F64(X)                         \
     X(double,    4, KIND_DIRECT,  4,  32, 1, 1)     \

@@ -81,6 +81,9 @@ def parse_args():
                          "split over the GPUs and whose passes gather across them (peer loads/stores)")
     ap.add_argument("--batch-cubes", type=int, default=96, help="batch workload: number of drawn cubes")
     ap.add_argument("--batch-big", type=int, default=2, help="batch workload: number of 128x256x512 boxes")
+    ap.add_argument("--batch-schedule", choices=["one-launch", "per-pass", "grouped"], default=None,
+                    help="batch workload with --no-tune: this schedule instead of the default one-launch "
+                         "(profiling runs)")
     ap.add_argument("--no-tune", action="store_true", help="batch workload: default plan, no make_plans timing "
                     "(profiling runs)")
     ap.add_argument("--precision", choices=["c64", "c128"], default="c64", help="cube workload element type")
@@ -409,7 +412,8 @@ def run_batch(args, rank, world, local_rank):
         scratch.normal_()
         b.make_plans(sviews)  # tile heights per length, schedule, claim, prefetch
         del scratch, sviews
-    plan_report = b.plan_report()
+    elif args.batch_schedule:
+        b.set_schedule(fused=args.batch_schedule != "per-pass", grouped=args.batch_schedule == "grouped")
     flat, views = b.empty(dev)
     gen = torch.Generator(device=dev).manual_seed(BATCH_SEED)
     flat.copy_(torch.complex(torch.randn(flat.numel(), generator=gen, device=dev),
@@ -424,6 +428,7 @@ def run_batch(args, rank, world, local_rank):
         b.inverse(views, stream=stream)
     stream.synchronize()
     b.check_device()
+    plan_report = b.plan_report()  # after the first call bound the buffers (the grouped tables need them)
 
     rel_err = rt_err = None
     if (world == 1 or rank == 0) and not args.no_check:
