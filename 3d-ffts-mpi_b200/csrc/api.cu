@@ -20,6 +20,7 @@
 #include "batch.cuh"
 #include "fft_mb.cuh"
 #include "fft_tc.cuh"
+#include "fft_tc2.cuh"
 #include "internal.h"
 
 using a2a::Dist;
@@ -39,15 +40,18 @@ struct a2a_dfft {
     // of their radix plans per axis, split radix-16 operands per direction
     PassKernel tc[3][2];  // the kernel in use per pass and direction
     // candidates per pass, direction: 0 = one tile per CTA, 1 = persistent
-    // CTAs fed by the TMA ring (where the plan and geometry allow it)
-    PassKernel tcv[3][2][2];
-    bool tcv_fits[3][2] = {};
-    int tcv_occ[3][2] = {};
-    float tcv_ms[3][2] = {};
+    // CTAs fed by the TMA ring (where the plan and geometry allow it), 2 =
+    // the two-stage form (512 = 16 x 32), also fed by the TMA ring
+    PassKernel tcv[3][2][3];
+    bool tcv_fits[3][3] = {};
+    int tcv_occ[3][3] = {};
+    float tcv_ms[3][3] = {};
     int tc_chosen[3] = {0, 0, 0};
     void* d_tc = nullptr;
     const void* tc_tw[3] = {nullptr, nullptr, nullptr};
     const void* tc_b[2] = {nullptr, nullptr};
+    const void* tc2_tw = nullptr;              // W512^(b k1), [b][k1]
+    const void* tc2_b[2] = {nullptr, nullptr};  // two-stage operands per direction
     // multi-block pass body: persistent register-pipelined where compiled
     bool mb_persistent = true;
     // batch-mode multi-block passes: per-rank tensor maps (device memory),
@@ -629,7 +633,8 @@ cudaError_t run_tc_pass(const a2a_dfft* f, int pass, bool inv, void* p, cudaStre
     const double scale = (inv && pass == 2) ? 1.0 / ((double)d.ng[0] * d.ng[1] * d.ng[2]) : 1.0;
     const void* maps = nullptr;
     unsigned grid = unsigned((uint64_t)g.NU * (g.NV / k.lines));
-    if (k.kind == a2a::KIND_TCR) {  // tensor maps of this pass for buffer p, one wave of persistent CTAs
+    const bool two = k.kind == a2a::KIND_TC2;
+    if (k.kind == a2a::KIND_TCR || two) {  // tensor maps of this pass for buffer p, one wave of persistent CTAs
         a2a::TmatEntry& ce = d.tmat[pass];
         if (ce.ptr != p || ce.lines != k.lines) {
             ce.ptr = nullptr;
@@ -638,7 +643,7 @@ cudaError_t run_tc_pass(const a2a_dfft* f, int pass, bool inv, void* p, cudaStre
             ce.lines = k.lines;
         }
         maps = &ce.maps;
-        grid = (unsigned)std::min<uint64_t>(grid, (uint64_t)std::max(f->tcv_occ[pass][1], 1) * d.sms);
+        grid = (unsigned)std::min<uint64_t>(grid, (uint64_t)std::max(f->tcv_occ[pass][two ? 2 : 1], 1) * d.sms);
     }
     a2a::PassArgs<float> a;
     a.src = static_cast<const float2*>(p);
@@ -646,13 +651,13 @@ cudaError_t run_tc_pass(const a2a_dfft* f, int pass, bool inv, void* p, cudaStre
     a.offA = g.offA;
     a.offU = g.offU;
     a.offV = g.offV;
-    a.tw = static_cast<const float2*>(f->tc_tw[axis]);
+    a.tw = static_cast<const float2*>(two ? f->tc2_tw : f->tc_tw[axis]);
     a.NU = g.NU;
     a.NV = g.NV;
     a.scale = float(scale);
     a.split = 0;
     a.err = d.d_err;
-    a.tcb = f->tc_b[inv ? 1 : 0];
+    a.tcb = two ? f->tc2_b[inv ? 1 : 0] : f->tc_b[inv ? 1 : 0];
     void* args[] = {&a, const_cast<void*>(maps)};
     return cudaLaunchKernel(k.fn, dim3(grid), dim3(k.threads), args, k.smem, st);
 }
@@ -755,6 +760,46 @@ void tc_operand_image(bool inverse, int fmt, std::vector<uint16_t>& img) {
         }
 }
 
+// The two-stage form's operand of one direction: the radix-16 image above,
+// then the radix-32 real DFT matrix (K x N = 64 x 64; K = [re b<16 | im b<16 |
+// re b>=16 | im b>=16], N the same over the outputs k2), split like the
+// radix-16 one, K-major without swizzle: element (n, k) at (k/8)*1024 +
+// (n/8)*128 + (n%8)*16 + (k%8)*2 of its part.
+void tc2_operand_image(bool inverse, int fmt, std::vector<uint16_t>& img) {
+    std::vector<uint16_t> b16;
+    tc_operand_image(inverse, fmt, b16);
+    const int parts = a2a::tc_parts(fmt);
+    img.assign(a2a::tc2_b_bytes(fmt) / 2, 0);
+    std::copy(b16.begin(), b16.end(), img.begin());
+    const size_t base = (size_t)parts * a2a::kTcMatB;  // bytes
+    const long double pi = acosl(-1.0L);
+    for (int k = 0; k < 64; ++k)
+        for (int n = 0; n < 64; ++n) {
+            const int kb = k / 16, nb = n / 16;
+            const int r = k % 16 + 16 * (kb / 2), c = n % 16 + 16 * (nb / 2);
+            const long double ang = 2.0L * pi * (long double)((r * c) % 32) / 32.0L;
+            const double C = (double)cosl(ang);
+            const double S = (inverse ? 1.0 : -1.0) * (double)sinl(ang);
+            double v;
+            if (kb % 2 == 0) v = nb % 2 == 0 ? C : S;
+            else v = nb % 2 == 0 ? -S : C;
+            const size_t off = (size_t)(k / 8) * a2a::kTc2ChunkB1 + (n / 8) * 128 + (n % 8) * 16 + (k % 8) * 2;
+            for (int q = 0; q < parts; ++q) {
+                uint16_t h;
+                if (fmt == a2a::TC_FP16) {
+                    const __half hh = __float2half_rn((float)v);
+                    h = __half_as_ushort(hh);
+                    v -= (double)__half2float(hh);
+                } else {
+                    const __nv_bfloat16 hh = __float2bfloat16_rn((float)v);
+                    h = __bfloat16_as_ushort(hh);
+                    v -= (double)__bfloat162float(hh);
+                }
+                img[(base + q * a2a::kTc2MatB1 + off) / 2] = h;
+            }
+        }
+}
+
 a2a_status setup_tc(a2a_dfft* f, a2a_method m) {
     const Dist& d = f->dist->d;
     if (d.prec != A2A_C64) return fail(A2A_ERROR_NOT_IMPLEMENTED, "the split tensor-core methods take A2A_C64 data");
@@ -780,9 +825,19 @@ a2a_status setup_tc(a2a_dfft* f, a2a_method m) {
             ring = g.NV % f->tcv[p][0][1].lines == 0 &&
                    build_tmat(d, p, f->tcv[p][0][1].lines, reinterpret_cast<const void*>(uintptr_t(1) << 20), &probe);
         }
+        // the two-stage form (512), on the same ring geometry with 8-line tiles
+        bool two = true;
+        for (int inv = 0; inv < 2; ++inv)
+            two = two && a2a::find_tc2_kernel(g.n, g.mode, inv, fmt, &f->tcv[p][inv][2]);
+        if (two) {
+            a2a::TmatMaps probe;
+            two = g.NV % f->tcv[p][0][2].lines == 0 &&
+                  build_tmat(d, p, f->tcv[p][0][2].lines, reinterpret_cast<const void*>(uintptr_t(1) << 20), &probe);
+        }
         f->tcv_fits[p][0] = true;
         f->tcv_fits[p][1] = ring;
-        for (int c = 0; c < 2; ++c) {
+        f->tcv_fits[p][2] = two;
+        for (int c = 0; c < 3; ++c) {
             f->tcv_ms[p][c] = 0.f;
             if (!f->tcv_fits[p][c]) continue;
             for (int inv = 0; inv < 2; ++inv) {
@@ -792,7 +847,7 @@ a2a_status setup_tc(a2a_dfft* f, a2a_method m) {
                 // the ring form's tiles arrive by TMA, not through L1: give
                 // the SM's unified memory to shared memory, so that two rings
                 // fit per SM
-                if (c == 1)
+                if (c >= 1)
                     A2A_CUDA(cudaFuncSetAttribute(f->tcv[p][inv][c].fn, cudaFuncAttributePreferredSharedMemoryCarveout,
                                                   100),
                              "cudaFuncSetAttribute");
@@ -817,7 +872,7 @@ a2a_status setup_tc(a2a_dfft* f, a2a_method m) {
             const int by_smem = (int)((size_t)smem_sm / smem_cta);
             const int by_regs = regs_sm / (regs_warp * (kk.threads / 32));
             const int by_thr = thr_sm / kk.threads;
-            const int need = (kk.threads / a2a::kTcRows) * a2a::tc_block_cols(fmt);
+            const int need = c == 2 ? a2a::tc2_cols(fmt) : (kk.threads / a2a::kTcRows) * a2a::tc_block_cols(fmt);
             int cols = 32;
             while (cols < need) cols *= 2;
             f->tcv_occ[p][c] = std::min(std::min(by_smem, by_regs), std::min(by_thr, 512 / cols));
@@ -845,10 +900,26 @@ a2a_status setup_tc(a2a_dfft* f, a2a_method m) {
     std::vector<uint16_t> b0, b1;
     tc_operand_image(false, fmt, b0);
     tc_operand_image(true, fmt, b1);
+    // the two-stage form: W512^(b k1) (forward sign, [b][k1]) and its operands
+    std::vector<float> tw2;
+    {
+        const long double pi = acosl(-1.0L);
+        for (int b = 0; b < 32; ++b)
+            for (int k1 = 0; k1 < 16; ++k1) {
+                const long double ang = 2.0L * pi * (long double)((b * k1) % 512) / 512.0L;
+                tw2.push_back((float)cosl(ang));
+                tw2.push_back((float)-sinl(ang));
+            }
+    }
+    std::vector<uint16_t> c0, c1;
+    tc2_operand_image(false, fmt, c0);
+    tc2_operand_image(true, fmt, c1);
+    const size_t tw2_bytes = ((tw2.size() * sizeof(float)) + 255) & ~size_t(255);
+    const size_t cb = (size_t)a2a::tc2_b_bytes(fmt);
     if (f->d_tc) cudaFree(f->d_tc);
     f->d_tc = nullptr;
     const size_t bb = (size_t)a2a::tc_b_bytes(fmt);
-    A2A_CUDA(cudaMalloc(&f->d_tc, tw_bytes + 2 * bb), "cudaMalloc(tensor-core tables)");
+    A2A_CUDA(cudaMalloc(&f->d_tc, tw_bytes + 2 * bb + tw2_bytes + 2 * cb), "cudaMalloc(tensor-core tables)");
     char* base = static_cast<char*>(f->d_tc);
     if (!tw.empty())
         A2A_CUDA(cudaMemcpy(base, tw.data(), tw.size() * sizeof(float), cudaMemcpyHostToDevice), "cudaMemcpy");
@@ -857,6 +928,13 @@ a2a_status setup_tc(a2a_dfft* f, a2a_method m) {
     for (int axis = 0; axis < 3; ++axis) f->tc_tw[axis] = base + twpos[axis] * sizeof(float2);
     f->tc_b[0] = base + tw_bytes;
     f->tc_b[1] = base + tw_bytes + bb;
+    char* base2 = base + tw_bytes + 2 * bb;  // 256-byte aligned (tw_bytes a 256-byte, bb a 2 KB multiple)
+    A2A_CUDA(cudaMemcpy(base2, tw2.data(), tw2.size() * sizeof(float), cudaMemcpyHostToDevice), "cudaMemcpy");
+    A2A_CUDA(cudaMemcpy(base2 + tw2_bytes, c0.data(), cb, cudaMemcpyHostToDevice), "cudaMemcpy");
+    A2A_CUDA(cudaMemcpy(base2 + tw2_bytes + cb, c1.data(), cb, cudaMemcpyHostToDevice), "cudaMemcpy");
+    f->tc2_tw = base2;
+    f->tc2_b[0] = base2 + tw2_bytes;
+    f->tc2_b[1] = base2 + tw2_bytes + cb;
     return A2A_SUCCESS;
 }
 
@@ -1183,7 +1261,7 @@ a2a_status a2a_dfft_make_plans(a2a_dfft* f, void** d_scratch) {
         for (int p = 0; p < 3 && e == cudaSuccess; ++p) {
             int best = f->tc_chosen[p];
             float best_ms = 1e30f;
-            for (int c = 0; c < 2 && e == cudaSuccess; ++c) {
+            for (int c = 0; c < 3 && e == cudaSuccess; ++c) {
                 if (!f->tcv_fits[p][c]) continue;
                 for (int inv = 0; inv < 2; ++inv) f->tc[p][inv] = f->tcv[p][inv][c];
                 e = transform();  // warm-up
@@ -1224,7 +1302,7 @@ a2a_status a2a_dfft_check_device(const a2a_dfft* f) {
 a2a_status a2a_dfft_variant_count(const a2a_dfft* f, int pass, int* count) {
     if (!f || !count) return fail(A2A_ERROR_INVALID_VALUE, "NULL argument");
     if (pass < 0 || pass > 2) return fail(A2A_ERROR_INVALID_VALUE, "pass must be 0 (Z), 1 (X) or 2 (Y)");
-    *count = f->method == A2A_METHOD_PLAIN ? f->dist->d.slot[pass][0].ncand : 2;
+    *count = f->method == A2A_METHOD_PLAIN ? f->dist->d.slot[pass][0].ncand : 3;
     return A2A_SUCCESS;
 }
 
@@ -1232,9 +1310,9 @@ a2a_status a2a_dfft_select_variant(a2a_dfft* f, int pass, int variant) {
     if (!f) return fail(A2A_ERROR_INVALID_VALUE, "dfft is NULL");
     if (pass < 0 || pass > 2) return fail(A2A_ERROR_INVALID_VALUE, "pass must be 0 (Z), 1 (X) or 2 (Y)");
     Dist& d = f->dist->d;
-    if (f->method != A2A_METHOD_PLAIN) {  // 0: one tile per CTA, 1: the persistent ring form
+    if (f->method != A2A_METHOD_PLAIN) {  // 0: one tile per CTA, 1: the persistent ring form, 2: two-stage
         if (!f->tcv[pass][0][0].fn) return fail(A2A_ERROR_NO_PLANS, "the tensor-core kernels are not set up");
-        if (variant < 0 || variant > 1) return fail(A2A_ERROR_INVALID_VALUE, "variant %d outside [0, 2)", variant);
+        if (variant < 0 || variant > 2) return fail(A2A_ERROR_INVALID_VALUE, "variant %d outside [0, 3)", variant);
         if (!f->tcv_fits[pass][variant])
             return fail(A2A_ERROR_UNSUPPORTED, "tensor-core variant %d does not fit this pass", variant);
         f->tc_chosen[pass] = variant;
@@ -1283,7 +1361,7 @@ a2a_status a2a_dfft_plan_report(const a2a_dfft* f, char* buf, size_t len) {
     }
     if (f->method != A2A_METHOD_PLAIN)
         for (int p = 0; p < 3; ++p)
-            for (int c = 0; c < 2; ++c) {
+            for (int c = 0; c < 3; ++c) {
                 if (!f->tcv_fits[p][c]) continue;
                 const PassKernel& k = f->tcv[p][0][c];
                 char line[256];
@@ -1291,7 +1369,7 @@ a2a_status a2a_dfft_plan_report(const a2a_dfft* f, char* buf, size_t len) {
                          "%s pass n=%d tensor-core %s %s lines=%d threads=%d smem=%zu occ=%d radix=%d,%d,%d "
                          "tuned_ms=%.4f%s\n",
                          names[p], k.n, f->method == A2A_METHOD_SPLIT_FP16 ? "split-fp16" : "split-bf16",
-                         c ? "ring" : "tile", k.lines, k.threads, k.smem, f->tcv_occ[p][c], k.radix[0], k.radix[1],
+                         c == 2 ? "two-stage" : c ? "ring" : "tile", k.lines, k.threads, k.smem, f->tcv_occ[p][c], k.radix[0], k.radix[1],
                          k.radix[2], f->tcv_ms[p][c], c == f->tc_chosen[p] ? " <- in use" : "");
                 out += line;
             }

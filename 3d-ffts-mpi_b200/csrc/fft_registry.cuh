@@ -329,5 +329,9 @@ constexpr int kMaxVariants = 32;
 bool find_tc_kernel(int n, int mode, bool inverse, int fmt, PassKernel* out);
 // the persistent TMA-ring form of it, where the plan has one (not 256)
 bool find_tc_ring_kernel(int n, int mode, bool inverse, int fmt, PassKernel* out);
+// the two-stage tensor-core form (radix-16 GEMM, twiddle, radix-32 GEMM; 512
+// only), fed by the TMA ring; its operand is tc2_b_bytes(fmt) bytes per
+// direction and its twiddle table W512^(b k1) laid out [b][k1]
+bool find_tc2_kernel(int n, int mode, bool inverse, int fmt, PassKernel* out);
 
 }  // namespace a2a

@@ -2,6 +2,7 @@
 // lookup.  Lengths whose plan ends in radix-16 stages: every stage after the
 // first is a tensor-core GEMM.
 #include "fft_tc.cuh"
+#include "fft_tc2.cuh"
 #include "internal.h"
 
 namespace a2a {
@@ -77,6 +78,35 @@ bool find_tc_ring_kernel(int n, int mode, bool inverse, int fmt, PassKernel* out
         case 1024: *out = tc_pick<1024, true>(mode, inverse, fmt); return true;
         default: return false;
     }
+}
+
+template <int MODE, bool INV, int FMT> PassKernel make_tc2_kernel() {
+    PassKernel k;
+    k.fn = reinterpret_cast<const void*>(&fft_tc2_ring_kernel<MODE, INV, FMT>);
+    k.kind = KIND_TC2;
+    k.smem = tc2_smem_bytes(FMT);
+    k.n = kTc2N;
+    k.threads = kTc2Threads;
+    k.lines = kTc2Lines;
+    k.min_blocks = 2;
+    k.lpt = 1;
+    k.nstages = 2;
+    k.radix[0] = 16;
+    k.radix[1] = 32;
+    k.twtotal = kTc2Tw;
+    return k;
+}
+
+bool find_tc2_kernel(int n, int mode, bool inverse, int fmt, PassKernel* out) {
+    if (n != kTc2N) return false;
+#define A2A_TC2(M_, F_) *out = inverse ? make_tc2_kernel<M_, true, F_>() : make_tc2_kernel<M_, false, F_>()
+    if (mode == MODE_LINE) {
+        if (fmt == TC_FP16) A2A_TC2(MODE_LINE, TC_FP16); else A2A_TC2(MODE_LINE, TC_BF16);
+    } else {
+        if (fmt == TC_FP16) A2A_TC2(MODE_BATCH, TC_FP16); else A2A_TC2(MODE_BATCH, TC_BF16);
+    }
+#undef A2A_TC2
+    return true;
 }
 
 }  // namespace a2a

@@ -54,11 +54,12 @@ def test_split_with_tones(pkg, oracle, cuda, method):
 
 @pytest.mark.parametrize("method", ["split_fp16", "split_bf16"])
 @pytest.mark.parametrize("P,shape", [(4, 64), (16, 128), (16, (512, 64, 64)), (4, (64, 64, 512)),
-                                     (4, (64, 1024, 64)), (4, (64, 64, 1024))])
-def test_split_both_kernel_forms(pkg, oracle, cuda, P, shape, method):
-    """Each tensor-core kernel form -- one tile per CTA, and the persistent
-    form fed by the TMA ring -- on every pass gives the FP64 oracle's
-    transform (relative L2 <= 1e-6)."""
+                                     (4, (64, 512, 64)), (4, (64, 1024, 64)), (4, (64, 64, 1024))])
+def test_split_every_kernel_form(pkg, oracle, cuda, P, shape, method):
+    """Each tensor-core kernel form -- one tile per CTA, the persistent form
+    fed by the TMA ring, and the two-stage form (512 = 16 x 32: radix-16
+    GEMM, twiddle, radix-32 GEMM, TMA ring) -- on every pass gives the FP64
+    oracle's transform (relative L2 <= 1e-6)."""
     import torch
 
     shape = (shape,) * 3 if isinstance(shape, int) else tuple(shape)
@@ -69,14 +70,16 @@ def test_split_both_kernel_forms(pkg, oracle, cuda, P, shape, method):
     ref = oracle.fft3_fp64(g)
     f = pkg.a2adfft(dist, method=method)
     f.make_plans()
-    assert f.variant_count(0) == 2
+    assert f.variant_count(0) == 3
     tested = 0
-    for form in (0, 1):
+    applied = [0, 0, 0]
+    for form in (0, 1, 2):
         for p in range(3):
             try:
                 f.select_variant(p, form)
+                applied[form] += 1
             except pkg.A2AError:
-                assert form == 1  # the ring form does not fit every geometry
+                assert form >= 1  # the ring and two-stage forms do not fit every pass
                 f.select_variant(p, 0)
         x = x0.clone()
         f.forward(x)
@@ -85,7 +88,9 @@ def test_split_both_kernel_forms(pkg, oracle, cuda, P, shape, method):
         f.inverse(x)
         assert oracle.rel_l2(x.cpu().numpy(), x0.cpu().numpy()) <= 2 * TOL[method], f"form {form} round trip"
         tested += 1
-    assert tested == 2
+    assert tested == 3
+    assert applied[0] == 3
+    assert applied[2] == sum(n == 512 for n in shape), applied  # the two-stage form: every 512 pass
 
 
 def test_split_rejects_double_and_unsupported_lengths(pkg, cuda):
