@@ -55,7 +55,7 @@ __host__ __device__ constexpr size_t tc2_smem_bytes(int fmt) {
     bytes += sizeof(uint32_t) * (size_t)kTc2N;
     bytes += sizeof(size_t) * (size_t)kTc2Lines;
     bytes += sizeof(float) * (size_t)kTc2Threads;                     // stage-1 row maxima (fp16)
-    bytes += sizeof(unsigned long long) * 3 + 16;                     // ring barriers, MMA barrier, tmem address
+    bytes += sizeof(unsigned long long) * 3 + 16;                     // ring barriers, MMA barrier, tmem address, wait flag
     return bytes;
 }
 
@@ -191,6 +191,7 @@ __global__ void __launch_bounds__(kTc2Threads, 2)
     unsigned long long* rbar = reinterpret_cast<unsigned long long*>(pmax + THREADS);
     unsigned long long* mbar = rbar + NSTG;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 1);
+    int* wflag = reinterpret_cast<int*>(tmem_slot + 1);
 
     const int tid = threadIdx.x;
     const int warp = tid / 32;
@@ -245,26 +246,38 @@ __global__ void __launch_bounds__(kTc2Threads, 2)
 
     bool ok = true;
     int i = 0;
-    // a bounded wait on the MMA barrier that every thread joins; on expiry:
-    // flag, and look once more for completion before tensor memory may be freed
+    // the MMA completion: thread 0 waits (bounded) and tells the CTA through
+    // shared memory (0: done; 1: done after the first wait gave up; 2: never
+    // seen done -- the tensor memory must then stay allocated); a failed wait
+    // raises the error flag and ends the pass
     auto mma_wait = [&]() -> bool {
-        const bool w = mbar_wait_bounded(mbar, phase);
-        if (__syncthreads_or(!w)) {
-            if ((tid % 32) == 0) atomicExch(a.err, 1);
-            drained = __syncthreads_and(mbar_wait_bounded(mbar, phase)) != 0;
+        if (tid == 0) *wflag = mbar_wait_bounded(mbar, phase) ? 0 : mbar_wait_bounded(mbar, phase) ? 1 : 2;
+        __syncthreads();
+        const int f = *wflag;
+        if (f) {
+            if (tid == 0) atomicExch(a.err, 1);
+            drained = f == 1;
             return false;
         }
         phase ^= 1u;
         tc_fence_after();
         return true;
     };
+    // line bases of this CTA's next tile (threads 0..B-1), loaded one tile ahead
+    auto line_base = [&](int t) -> size_t {
+        const int u = t / tilesV;
+        const int v0 = (t - u * tilesV) * B;
+        return (size_t)__ldg(a.offU + u) + __ldg(a.offV + v0 + tid);
+    };
+    size_t nbase = 0;
+    if (tid < B && mine > 0) nbase = line_base(blockIdx.x);
     for (; i < mine; ++i) {
         const int t = blockIdx.x + i * gridDim.x;
         const int s = i % NSTG;
-        const int u = t / tilesV;
-        const int v0 = (t - u * tilesV) * B;
-        const size_t ubase = __ldg(a.offU + u);
-        if (tid < B) base_s[tid] = ubase + __ldg(a.offV + v0 + tid);
+        if (tid < B) {
+            base_s[tid] = nbase;
+            if (i + 1 < mine) nbase = line_base(t + gridDim.x);
+        }
         if (__syncthreads_or(!mbar_wait_bounded(rbar + s, (uint32_t)((i / NSTG) & 1)))) {
             if (tid == 0) atomicExch(a.err, 1);
             ok = false;
