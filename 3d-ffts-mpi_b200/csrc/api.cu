@@ -50,8 +50,9 @@ struct a2a_dfft {
     void* d_tc = nullptr;
     const void* tc_tw[3] = {nullptr, nullptr, nullptr};
     const void* tc_b[2] = {nullptr, nullptr};
-    const void* tc2_tw = nullptr;              // W512^(b k1), [b][k1]
-    const void* tc2_b[2] = {nullptr, nullptr};  // two-stage operands per direction
+    // two-stage form per pass: twiddles W_n^(b k1) ([b][k1]) and operands per direction
+    const void* tc2_tw[3] = {nullptr, nullptr, nullptr};
+    const void* tc2_b[3][2] = {};
     // multi-block pass body: persistent register-pipelined where compiled
     bool mb_persistent = true;
     // batch-mode multi-block passes: per-rank tensor maps (device memory),
@@ -651,13 +652,13 @@ cudaError_t run_tc_pass(const a2a_dfft* f, int pass, bool inv, void* p, cudaStre
     a.offA = g.offA;
     a.offU = g.offU;
     a.offV = g.offV;
-    a.tw = static_cast<const float2*>(two ? f->tc2_tw : f->tc_tw[axis]);
+    a.tw = static_cast<const float2*>(two ? f->tc2_tw[pass] : f->tc_tw[axis]);
     a.NU = g.NU;
     a.NV = g.NV;
     a.scale = float(scale);
     a.split = 0;
     a.err = d.d_err;
-    a.tcb = two ? f->tc2_b[inv ? 1 : 0] : f->tc_b[inv ? 1 : 0];
+    a.tcb = two ? f->tc2_b[pass][inv ? 1 : 0] : f->tc_b[inv ? 1 : 0];
     void* args[] = {&a, const_cast<void*>(maps)};
     return cudaLaunchKernel(k.fn, dim3(grid), dim3(k.threads), args, k.smem, st);
 }
@@ -760,18 +761,26 @@ void tc_operand_image(bool inverse, int fmt, std::vector<uint16_t>& img) {
         }
 }
 
-// The two-stage form's operand of one direction: the radix-16 image above,
-// then the radix-32 real DFT matrix (K x N = 64 x 64; K = [re b<16 | im b<16 |
-// re b>=16 | im b>=16], N the same over the outputs k2), split like the
-// radix-16 one, K-major without swizzle: element (n, k) at (k/8)*1024 +
-// (n/8)*128 + (n%8)*16 + (k%8)*2 of its part.
-void tc2_operand_image(bool inverse, int fmt, std::vector<uint16_t>& img) {
-    std::vector<uint16_t> b16;
-    tc_operand_image(inverse, fmt, b16);
+size_t tc2_b_bytes_n(int n, int fmt) {
+    return n == 512 ? (size_t)a2a::tc2_b_bytes<512>(fmt) : (size_t)a2a::tc2_b_bytes<1024>(fmt);
+}
+
+// The two-stage form's operand of one direction for length n: at 512 the
+// radix-16 image above, then the radix-32 real DFT matrix; at 1024 the
+// radix-32 matrix alone (both stages use it).  The radix-32 matrix: K x N =
+// 64 x 64, K = [re b<16 | im b<16 | re b>=16 | im b>=16], N the same over the
+// outputs k2, split like the radix-16 one, K-major without swizzle: element
+// (n, k) at (k/8)*1024 + (n/8)*128 + (n%8)*16 + (k%8)*2 of its part.
+void tc2_operand_image(int len, bool inverse, int fmt, std::vector<uint16_t>& img) {
     const int parts = a2a::tc_parts(fmt);
-    img.assign(a2a::tc2_b_bytes(fmt) / 2, 0);
-    std::copy(b16.begin(), b16.end(), img.begin());
-    const size_t base = (size_t)parts * a2a::kTcMatB;  // bytes
+    img.assign(tc2_b_bytes_n(len, fmt) / 2, 0);
+    size_t base = 0;  // bytes
+    if (len == 512) {
+        std::vector<uint16_t> b16;
+        tc_operand_image(inverse, fmt, b16);
+        std::copy(b16.begin(), b16.end(), img.begin());
+        base = (size_t)parts * a2a::kTcMatB;
+    }
     const long double pi = acosl(-1.0L);
     for (int k = 0; k < 64; ++k)
         for (int n = 0; n < 64; ++n) {
@@ -900,26 +909,39 @@ a2a_status setup_tc(a2a_dfft* f, a2a_method m) {
     std::vector<uint16_t> b0, b1;
     tc_operand_image(false, fmt, b0);
     tc_operand_image(true, fmt, b1);
-    // the two-stage form: W512^(b k1) (forward sign, [b][k1]) and its operands
-    std::vector<float> tw2;
-    {
+    // the two-stage form, per pass where it fits: W_n^(b k1) (forward sign,
+    // [b < 32][k1 < n / 32]) and its operands per direction
+    std::vector<char> two;  // host image of the segments, each 256-byte aligned
+    size_t seg[3][3] = {};  // per pass: twiddle, forward and inverse operand offsets
+    for (int p = 0; p < 3; ++p) {
+        if (!f->tcv_fits[p][2]) continue;
+        const int n = f->tcv[p][0][2].n;
+        std::vector<float> t;
         const long double pi = acosl(-1.0L);
         for (int b = 0; b < 32; ++b)
-            for (int k1 = 0; k1 < 16; ++k1) {
-                const long double ang = 2.0L * pi * (long double)((b * k1) % 512) / 512.0L;
-                tw2.push_back((float)cosl(ang));
-                tw2.push_back((float)-sinl(ang));
+            for (int k1 = 0; k1 < n / 32; ++k1) {
+                const long double ang = 2.0L * pi * (long double)((b * k1) % n) / (long double)n;
+                t.push_back((float)cosl(ang));
+                t.push_back((float)-sinl(ang));
             }
+        auto append = [&](const void* src, size_t bytes) {
+            const size_t at = (two.size() + 255) & ~size_t(255);
+            two.resize(at + bytes);
+            std::memcpy(two.data() + at, src, bytes);
+            return at;
+        };
+        seg[p][0] = append(t.data(), t.size() * sizeof(float));
+        for (int inv = 0; inv < 2; ++inv) {
+            std::vector<uint16_t> img;
+            tc2_operand_image(n, inv != 0, fmt, img);
+            seg[p][1 + inv] = append(img.data(), img.size() * sizeof(uint16_t));
+        }
     }
-    std::vector<uint16_t> c0, c1;
-    tc2_operand_image(false, fmt, c0);
-    tc2_operand_image(true, fmt, c1);
-    const size_t tw2_bytes = ((tw2.size() * sizeof(float)) + 255) & ~size_t(255);
-    const size_t cb = (size_t)a2a::tc2_b_bytes(fmt);
+    const size_t two_bytes = (two.size() + 255) & ~size_t(255);
     if (f->d_tc) cudaFree(f->d_tc);
     f->d_tc = nullptr;
     const size_t bb = (size_t)a2a::tc_b_bytes(fmt);
-    A2A_CUDA(cudaMalloc(&f->d_tc, tw_bytes + 2 * bb + tw2_bytes + 2 * cb), "cudaMalloc(tensor-core tables)");
+    A2A_CUDA(cudaMalloc(&f->d_tc, tw_bytes + 2 * bb + two_bytes), "cudaMalloc(tensor-core tables)");
     char* base = static_cast<char*>(f->d_tc);
     if (!tw.empty())
         A2A_CUDA(cudaMemcpy(base, tw.data(), tw.size() * sizeof(float), cudaMemcpyHostToDevice), "cudaMemcpy");
@@ -929,12 +951,12 @@ a2a_status setup_tc(a2a_dfft* f, a2a_method m) {
     f->tc_b[0] = base + tw_bytes;
     f->tc_b[1] = base + tw_bytes + bb;
     char* base2 = base + tw_bytes + 2 * bb;  // 256-byte aligned (tw_bytes a 256-byte, bb a 2 KB multiple)
-    A2A_CUDA(cudaMemcpy(base2, tw2.data(), tw2.size() * sizeof(float), cudaMemcpyHostToDevice), "cudaMemcpy");
-    A2A_CUDA(cudaMemcpy(base2 + tw2_bytes, c0.data(), cb, cudaMemcpyHostToDevice), "cudaMemcpy");
-    A2A_CUDA(cudaMemcpy(base2 + tw2_bytes + cb, c1.data(), cb, cudaMemcpyHostToDevice), "cudaMemcpy");
-    f->tc2_tw = base2;
-    f->tc2_b[0] = base2 + tw2_bytes;
-    f->tc2_b[1] = base2 + tw2_bytes + cb;
+    if (!two.empty())
+        A2A_CUDA(cudaMemcpy(base2, two.data(), two.size(), cudaMemcpyHostToDevice), "cudaMemcpy");
+    for (int p = 0; p < 3; ++p) {
+        f->tc2_tw[p] = f->tcv_fits[p][2] ? base2 + seg[p][0] : nullptr;
+        for (int inv = 0; inv < 2; ++inv) f->tc2_b[p][inv] = f->tcv_fits[p][2] ? base2 + seg[p][1 + inv] : nullptr;
+    }
     return A2A_SUCCESS;
 }
 

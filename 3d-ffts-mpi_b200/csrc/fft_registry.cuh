@@ -329,9 +329,10 @@ constexpr int kMaxVariants = 32;
 bool find_tc_kernel(int n, int mode, bool inverse, int fmt, PassKernel* out);
 // the persistent TMA-ring form of it, where the plan has one (not 256)
 bool find_tc_ring_kernel(int n, int mode, bool inverse, int fmt, PassKernel* out);
-// the two-stage tensor-core form (radix-16 GEMM, twiddle, radix-32 GEMM; 512
-// only), fed by the TMA ring; its operand is tc2_b_bytes(fmt) bytes per
-// direction and its twiddle table W512^(b k1) laid out [b][k1]
+// the two-stage tensor-core form (512 = 16 x 32, 1024 = 32 x 32: radix-R0
+// GEMM, twiddle, radix-32 GEMM), fed by the TMA ring; its operand is
+// tc2_b_bytes<n>(fmt) bytes per direction and its twiddle table W_n^(b k1)
+// laid out [b < 32][k1 < n / 32]
 bool find_tc2_kernel(int n, int mode, bool inverse, int fmt, PassKernel* out);
 
 }  // namespace a2a

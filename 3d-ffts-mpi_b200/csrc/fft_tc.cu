@@ -80,33 +80,40 @@ bool find_tc_ring_kernel(int n, int mode, bool inverse, int fmt, PassKernel* out
     }
 }
 
-template <int MODE, bool INV, int FMT> PassKernel make_tc2_kernel() {
+template <int N, int MODE, bool INV, int FMT> PassKernel make_tc2_kernel() {
+    using G = Tc2Geom<N>;
     PassKernel k;
-    k.fn = reinterpret_cast<const void*>(&fft_tc2_ring_kernel<MODE, INV, FMT>);
+    k.fn = reinterpret_cast<const void*>(&fft_tc2_ring_kernel<N, MODE, INV, FMT>);
     k.kind = KIND_TC2;
-    k.smem = tc2_smem_bytes(FMT);
-    k.n = kTc2N;
+    k.smem = tc2_smem_bytes<N>(FMT);
+    k.n = N;
     k.threads = kTc2Threads;
-    k.lines = kTc2Lines;
+    k.lines = G::B;
     k.min_blocks = 2;
     k.lpt = 1;
     k.nstages = 2;
-    k.radix[0] = 16;
+    k.radix[0] = G::R0;
     k.radix[1] = 32;
-    k.twtotal = kTc2Tw;
+    k.twtotal = G::TW;
     return k;
 }
 
-bool find_tc2_kernel(int n, int mode, bool inverse, int fmt, PassKernel* out) {
-    if (n != kTc2N) return false;
-#define A2A_TC2(M_, F_) *out = inverse ? make_tc2_kernel<M_, true, F_>() : make_tc2_kernel<M_, false, F_>()
+template <int N> PassKernel tc2_pick(int mode, bool inverse, int fmt) {
+#define A2A_TC2(M_, F_) return inverse ? make_tc2_kernel<N, M_, true, F_>() : make_tc2_kernel<N, M_, false, F_>()
     if (mode == MODE_LINE) {
         if (fmt == TC_FP16) A2A_TC2(MODE_LINE, TC_FP16); else A2A_TC2(MODE_LINE, TC_BF16);
     } else {
         if (fmt == TC_FP16) A2A_TC2(MODE_BATCH, TC_FP16); else A2A_TC2(MODE_BATCH, TC_BF16);
     }
 #undef A2A_TC2
-    return true;
+}
+
+bool find_tc2_kernel(int n, int mode, bool inverse, int fmt, PassKernel* out) {
+    switch (n) {
+        case 512: *out = tc2_pick<512>(mode, inverse, fmt); return true;
+        case 1024: *out = tc2_pick<1024>(mode, inverse, fmt); return true;
+        default: return false;
+    }
 }
 
 }  // namespace a2a

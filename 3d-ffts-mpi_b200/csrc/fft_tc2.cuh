@@ -1,72 +1,89 @@
-// Two-stage split-precision tensor-core pass for N = 512 = 16 x 32.
+// Two-stage split-precision tensor-core pass, N = R0 x 32: 512 = 16 x 32 and
+// 1024 = 32 x 32.
 //
-// With n = 32 a + b and k = k1 + 16 k2 (a, k1 < 16; b, k2 < 32):
-//   X[k1 + 16 k2] = sum_b W32^(b k2) W512^(b k1) sum_a x[32 a + b] W16^(a k1)
-// Stage 0: for each b, the radix-16 DFT over a of the stride-32 subsequence
-// (no twiddles): one 32 x 32 real GEMM row per (line, b), as the radix-16
-// stage of fft_tc.cuh.  Its outputs go to tile position 16 b + k1.
-// Stage 1: for each k1, the inputs tile[k1 + 16 b] times W512^(b k1), then
-// the radix-32 DFT over b: one 64 x 64 real GEMM row per (line, k1), with
-// K = [re b<16 | im b<16 | re b>=16 | im b>=16] and the outputs in the same
-// order over k2.  A 128-row stage-1 block has two threads per row (warps w
-// and w + 4 reach the same tensor-memory lanes): thread half h writes the
-// inputs b in [16h, 16h + 16) (its 16 columns of each part) and reads the
-// outputs k2 in [16h, 16h + 16).
+// With n = 32 a + b and k = k1 + R0 k2 (a, k1 < R0; b, k2 < 32):
+//   X[k1 + R0 k2] = sum_b W32^(b k2) W_N^(b k1) sum_a x[32 a + b] W_R0^(a k1)
+// Stage 0: for each b, the radix-R0 DFT over a of the stride-32 subsequence
+// (no twiddles), one real GEMM row per (line, b); its outputs go to tile
+// position R0 b + k1.  Stage 1: for each k1, the inputs tile[k1 + R0 b] times
+// W_N^(b k1), then the radix-32 DFT over b, one 64 x 64 real GEMM row per
+// (line, k1), with K = [re b<16 | im b<16 | re b>=16 | im b>=16] and the
+// outputs in the same order over k2.  A radix-16 row (32 x 32, as in
+// fft_tc.cuh) has one thread; a radix-32 row has two: warps w and w + 4 reach
+// the same tensor-memory lanes, so thread half h writes the inputs of its half
+// of K (its 16 columns of each part) and reads its half of N.  Every thread
+// thus splits 16 complex values per stage.
 //
-// So a pass has two GEMM stages, one twiddle multiply and one shared-memory
-// exchange per element (the three-stage 2 x 16 x 16 form has two of each
-// plus a CUDA-core radix-2 stage).  Operands are split as in fft_tc.cuh
-// (fp16: two parts, rows scaled by a power of two; bf16: three parts); a
-// stage-1 row's scale is agreed between its two threads through shared
-// memory.  Tiles of 8 lines arrive by the single-GPU TMA ring of fft_tmat.cuh
-// (2 slots, transformed in place, no multicast); the slot of a tile is
-// refilled as soon as its stage-1 operands are in tensor memory.
+// A pass has two GEMM stages, one twiddle multiply and one shared-memory
+// exchange per element.  Operands are split as in fft_tc.cuh (fp16: two parts,
+// rows scaled by a power of two; bf16: three parts); a radix-32 row's scale is
+// agreed between its two threads through shared memory.  Tiles (8 lines at
+// 512, 4 at 1024: 32 KB) arrive by the single-GPU TMA ring of fft_tmat.cuh (2
+// slots, transformed in place, no multicast); a tile's slot is refilled as
+// soon as its stage-1 operands are in tensor memory.
 #pragma once
 
 #include "fft_tc.cuh"
 
 namespace a2a {
 
-constexpr int kTc2N = 512;
-constexpr int kTc2Lines = 8;
 constexpr int kTc2Threads = 256;
 // the radix-32 operand: K-major N x K, N = K = 64 (16-bit values): a K chunk
 // of 8 values over all 64 rows is 1 KB, one part 8 KB
 constexpr int kTc2ChunkB1 = 64 / 8 * 128;
 constexpr int kTc2MatB1 = 8 * kTc2ChunkB1;
-// both operands of one direction: the radix-16 parts, then the radix-32 parts
-__host__ __device__ constexpr int tc2_b_bytes(int fmt) { return tc_parts(fmt) * (kTcMatB + kTc2MatB1); }
-// tensor-memory columns: stage 0 two blocks of (16 per part + 32), stage 1
-// one block of (32 per part + 64) -- the same count, reused
+
+template <int N> struct Tc2Geom {
+    static_assert(N == 512 || N == 1024, "two-stage lengths: 512 = 16 x 32 and 1024 = 32 x 32");
+    static constexpr int R0 = N / 32;                  // first radix (16 or 32); the second is 32
+    static constexpr int NB1 = N / 32;                 // stage-1 rows per line (= R0)
+    static constexpr int B = N == 512 ? 8 : 4;         // lines per tile (32 KB)
+    static constexpr int ROWS0 = B * 32;               // stage-0 rows: 256 or 128
+    static constexpr int TPR0 = kTc2Threads / ROWS0;   // threads per stage-0 row: 1 or 2
+    static constexpr int SH = R0 == 16 ? 4 : 5;        // log2 R0
+    static constexpr int RMASK = 128 / (B * 8) - 1;    // batch-mode tile rows per 128 bytes, minus 1
+    static constexpr int TW = 32 * NB1;                // twiddles W_N^(b k1), [b][k1]
+    static_assert(B * NB1 == 128, "one 128-row stage-1 block, two threads per row");
+};
+
+// both operands of one direction: the radix-16 parts (512 only), then the
+// radix-32 parts (1024: one operand serves both stages)
+template <int N> __host__ __device__ constexpr int tc2_b_bytes(int fmt) {
+    return tc_parts(fmt) * ((N == 512 ? kTcMatB : 0) + kTc2MatB1);
+}
+// tensor-memory columns: stage 0 (two blocks of 16 per part + 32, or one of 32
+// per part + 64) and stage 1 (one block of 32 per part + 64) take the same
+// count, reused
 __host__ __device__ constexpr int tc2_cols(int fmt) { return 32 * tc_parts(fmt) + 64; }
 __host__ __device__ constexpr uint32_t tc2_tcols(int fmt) { return tc2_cols(fmt) <= 128 ? 128u : 256u; }
-// twiddles W512^(b k1) (forward sign), [b][k1]
-constexpr int kTc2Tw = 32 * 16;
 
 __host__ __device__ constexpr uint32_t umma_idesc_f16_n(int fmt, int n) {
     return (1u << 4) | ((uint32_t)fmt << 7) | ((uint32_t)fmt << 10) | (((uint32_t)n >> 3) << 17) | ((128u >> 4) << 24);
 }
 
-__host__ __device__ constexpr size_t tc2_smem_bytes(int fmt) {
-    size_t bytes = kTmatAlign;                                        // room to align the ring
-    bytes += 2 * (size_t)tmat_slot_bytes<float, kTc2Lines, kTc2N>();  // two slots
-    bytes += (size_t)tc2_b_bytes(fmt);
-    bytes += sizeof(float2) * (size_t)kTc2Tw;
-    bytes += sizeof(uint32_t) * (size_t)kTc2N;
-    bytes += sizeof(size_t) * (size_t)kTc2Lines;
-    bytes += sizeof(float) * (size_t)kTc2Threads;                     // stage-1 row maxima (fp16)
-    bytes += sizeof(unsigned long long) * 3 + 16;                     // ring barriers, MMA barrier, tmem address, wait flag
+template <int N> __host__ __device__ constexpr size_t tc2_smem_bytes(int fmt) {
+    using G = Tc2Geom<N>;
+    size_t bytes = kTmatAlign;                                   // room to align the ring
+    bytes += 2 * (size_t)tmat_slot_bytes<float, G::B, N>();      // two slots
+    bytes += (size_t)tc2_b_bytes<N>(fmt);
+    bytes += sizeof(float2) * (size_t)G::TW;
+    bytes += sizeof(uint32_t) * (size_t)N;
+    bytes += sizeof(size_t) * (size_t)G::B;
+    bytes += sizeof(float) * (size_t)kTc2Threads;                // radix-32 row maxima (fp16)
+    bytes += sizeof(unsigned long long) * 3 + 16;                // ring barriers, MMA barrier, tmem address, wait flag
     return bytes;
 }
 
-// Tile positions (in place in the ring slot) of the stage-0 outputs: batch
-// mode rows of 8 lines, row n stored at n ^ ((n >> 4) & 1) (the two rows a
-// half-warp writes, 16 apart, land in different bank halves); line mode
-// [b][n] with n's low four bits XOR-ed with bits 4-7 (a half-warp writes
-// positions 16 apart).  Stage 1's reads stay conflict-free under both.
-template <int MODE> __device__ __forceinline__ int tc2_pos(int b, int n) {
-    if constexpr (MODE == MODE_BATCH) return (n ^ ((n >> 4) & 1)) * kTc2Lines + b;
-    else return b * kTc2N + (n ^ ((n >> 4) & 15));
+// Tile positions (in place in the ring slot) of the stage-0 outputs.  Batch
+// mode: rows of B lines, row n stored at n ^ ((n >> log2 R0) & RMASK), so the
+// rows R0 apart that a half-warp writes land in different bank groups; line
+// mode: [b][n] with n's low four bits XOR-ed with (n >> log2 R0), so the
+// positions R0 apart that a half-warp writes fall in distinct banks.  Stage 1's
+// reads stay conflict-free under both.
+template <int N, int MODE> __device__ __forceinline__ int tc2_pos(int b, int n) {
+    using G = Tc2Geom<N>;
+    if constexpr (MODE == MODE_BATCH) return (n ^ ((n >> G::SH) & G::RMASK)) * G::B + b;
+    else return b * N + (n ^ ((n >> G::SH) & 15));
 }
 
 // fp16 row scale: 2^-e and 2^e with e the exponent of mx (as frexp gives it).
@@ -96,49 +113,30 @@ template <int FMT> __device__ __forceinline__ void tc2_split16(const float2 (&x)
     }
 }
 
-// Thread 0: the MMAs of one stage, then the commit.  Stage 0: two 128-row
-// blocks (columns 0 and BC0), K = 32, N = 32, operand b0; stage 1: one block,
-// K = 64 (four K = 16 steps per term), N = 64, operand b1.  Terms smallest
-// first, as in fft_tc.cuh.
-template <int FMT, int STAGE>
-__device__ __forceinline__ void tc2_issue(uint32_t tmem, uint32_t b_addr, unsigned long long* bar) {
+// Thread 0: the MMAs of one GEMM stage, then the commit.  Radix 16: two
+// 128-row blocks (columns 0 and 16 NP + 32), K = 32 (two K = 16 steps per
+// term), N = 32; radix 32: one block, K = 64 (four steps per term), N = 64.
+// `op` is the stage's split operand in shared memory.  Terms smallest first,
+// as in fft_tc.cuh.
+template <int FMT, int R>
+__device__ __forceinline__ void tc2_issue(uint32_t tmem, uint32_t op, unsigned long long* bar) {
     constexpr int NP = tc_parts(FMT);
+    constexpr int NBLK = R == 16 ? 2 : 1;
+    constexpr int AC = R;                // A columns per part: 2R values, two per column
+    constexpr int BC = NP * AC + 2 * R;  // block columns (A parts, then the accumulator)
+    constexpr int KSTEPS = R / 8;        // K = 16 steps per term
+    constexpr int CHUNK = R == 16 ? kTcChunkB : kTc2ChunkB1;  // bytes of one 8-value K chunk of the operand
+    constexpr int PART = R == 16 ? kTcMatB : kTc2MatB1;
+    const uint32_t idesc = umma_idesc_f16_n(FMT, 2 * R);
     tc_fence_after();
-    if constexpr (STAGE == 0) {
-        constexpr int BC0 = 16 * NP + 32;
-        const uint32_t idesc = umma_idesc_f16_n(FMT, 32);
-        auto bre = [&](int q) { return umma_smem_desc(b_addr + q * kTcMatB, kTcChunkB, 128); };
-        auto bim = [&](int q) { return umma_smem_desc(b_addr + q * kTcMatB + 2 * kTcChunkB, kTcChunkB, 128); };
 #pragma unroll
-        for (int blk = 0; blk < 2; ++blk) {
-            const uint32_t ab = tmem + blk * BC0;
-            const uint32_t dacc = ab + 16 * NP;
-            auto term = [&](int pa, int qb, uint32_t acc) {
-                tc_mma_ts(dacc, ab + 16 * pa, bre(qb), idesc, acc);
-                tc_mma_ts(dacc, ab + 16 * pa + 8, bim(qb), idesc, 1);
-            };
-            if constexpr (NP == 2) {
-                term(0, 1, 0);
-                term(1, 0, 1);
-                term(0, 0, 1);
-            } else {
-                term(0, 2, 0);
-                term(1, 1, 1);
-                term(2, 0, 1);
-                term(0, 1, 1);
-                term(1, 0, 1);
-                term(0, 0, 1);
-            }
-        }
-    } else {
-        const uint32_t idesc = umma_idesc_f16_n(FMT, 64);
-        const uint32_t b1 = b_addr + NP * kTcMatB;
-        const uint32_t dacc = tmem + 32 * NP;
+    for (int blk = 0; blk < NBLK; ++blk) {
+        const uint32_t ab = tmem + blk * BC;
+        const uint32_t dacc = ab + NP * AC;
         auto term = [&](int pa, int qb, uint32_t acc) {
 #pragma unroll
-            for (int c = 0; c < 4; ++c)
-                tc_mma_ts(dacc, tmem + 32 * pa + 8 * c,
-                          umma_smem_desc(b1 + qb * kTc2MatB1 + c * 2 * kTc2ChunkB1, kTc2ChunkB1, 128), idesc,
+            for (int c = 0; c < KSTEPS; ++c)
+                tc_mma_ts(dacc, ab + AC * pa + 8 * c, umma_smem_desc(op + qb * PART + c * 2 * CHUNK, CHUNK, 128), idesc,
                           c == 0 ? acc : 1u);
         };
         if constexpr (NP == 2) {
@@ -157,35 +155,38 @@ __device__ __forceinline__ void tc2_issue(uint32_t tmem, uint32_t b_addr, unsign
     tc_commit(bar);
 }
 
-// The persistent kernel: each CTA allocates its tensor memory and loads both
+// The persistent kernel: each CTA allocates its tensor memory and loads the
 // split operands, the twiddles and the offsets once, then works through tiles
-// blockIdx.x, blockIdx.x + gridDim.x, ... of 8 lines, each arriving as whole
+// blockIdx.x, blockIdx.x + gridDim.x, ... of B lines, each arriving as whole
 // tensor-map copies in a 2-slot ring.  Every wait is bounded; on expiry the
 // device error flag is raised, the rest of the pass is skipped, the CTA waits
 // (bounded) for its copies in flight and frees its tensor memory only if the
 // MMAs it committed were seen to finish.
-template <int MODE, bool INV, int FMT>
+template <int N, int MODE, bool INV, int FMT>
 __global__ void __launch_bounds__(kTc2Threads, 2)
     fft_tc2_ring_kernel(const PassArgs<float> a, const __grid_constant__ TmatMaps m) {
-    constexpr int N = kTc2N;
-    constexpr int B = kTc2Lines;
+    using G = Tc2Geom<N>;
+    constexpr int R0 = G::R0;
+    constexpr int NB1 = G::NB1;
+    constexpr int B = G::B;
+    constexpr int TPR0 = G::TPR0;
     constexpr int THREADS = kTc2Threads;
     constexpr int NP = tc_parts(FMT);
-    constexpr int BC0 = 16 * NP + 32;  // stage-0 block columns (A parts, then the accumulator)
-    constexpr int ACC0 = 16 * NP;
-    constexpr int ACC1 = 32 * NP;      // stage-1 accumulator (64 columns)
+    constexpr int BC0 = NP * R0 + 2 * R0;  // stage-0 block columns (A parts, then the accumulator)
+    constexpr int ACC0 = NP * R0;          // stage-0 accumulator, within its block
+    constexpr int ACC1 = 32 * NP;          // stage-1 accumulator (64 columns)
     constexpr uint32_t TCOLS = tc2_tcols(FMT);
     constexpr uint32_t SLOT = tmat_slot_bytes<float, B, N>();
     constexpr int NSTG = 2;
     static_assert(B * N * sizeof(float2) <= SLOT, "a tile fits its slot");
-    static_assert(2 * BC0 <= (int)TCOLS && ACC1 + 64 <= (int)TCOLS, "tensor-memory columns");
+    static_assert((TPR0 == 1 ? 2 : 1) * BC0 <= (int)TCOLS && ACC1 + 64 <= (int)TCOLS, "tensor-memory columns");
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const uint32_t s0 = smem_u32(smem_raw);
     unsigned char* ring = smem_raw + (((s0 + kTmatAlign - 1) & ~(kTmatAlign - 1)) - s0);
     unsigned char* bmat = ring + NSTG * SLOT;
-    float2* tw = reinterpret_cast<float2*>(bmat + tc2_b_bytes(FMT));
-    uint32_t* offA_s = reinterpret_cast<uint32_t*>(tw + kTc2Tw);
+    float2* tw = reinterpret_cast<float2*>(bmat + tc2_b_bytes<N>(FMT));
+    uint32_t* offA_s = reinterpret_cast<uint32_t*>(tw + G::TW);
     size_t* base_s = reinterpret_cast<size_t*>(offA_s + N);
     float* pmax = reinterpret_cast<float*>(base_s + B);
     unsigned long long* rbar = reinterpret_cast<unsigned long long*>(pmax + THREADS);
@@ -213,30 +214,37 @@ __global__ void __launch_bounds__(kTc2Threads, 2)
     {
         const uint4* src = reinterpret_cast<const uint4*>(a.tcb);
         uint4* dst = reinterpret_cast<uint4*>(bmat);
-        for (int i = tid; i < tc2_b_bytes(FMT) / 16; i += THREADS) dst[i] = src[i];
+        for (int i = tid; i < tc2_b_bytes<N>(FMT) / 16; i += THREADS) dst[i] = src[i];
     }
-    for (int i = tid; i < kTc2Tw; i += THREADS) tw[i] = a.tw[i];
+    for (int i = tid; i < G::TW; i += THREADS) tw[i] = a.tw[i];
     for (int i = tid; i < N; i += THREADS) offA_s[i] = a.offA[i];
     fence_proxy_async_smem();  // operands visible to the tensor cores
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
-    const uint32_t b_addr = smem_u32(bmat);
+    const uint32_t op0 = smem_u32(bmat);                                // stage-0 operand (radix R0)
+    const uint32_t op1 = op0 + (N == 512 ? NP * kTcMatB : 0);          // stage-1 operand (radix 32)
     uint32_t phase = 0;
     bool drained = true;
 
-    // stage 0: one radix-16 row per thread (block warp / 4, lane tid % 128)
-    int b0, j0;
-    if constexpr (MODE == MODE_BATCH) { b0 = tid % B; j0 = tid / B; }
-    else { j0 = tid % 32; b0 = tid / 32; }
-    const uint32_t row0 = ((uint32_t)((warp % 4) * 32) << 16) + (uint32_t)((warp / 4) * BC0);
-    // stage 1: row tid % 128 of the one block, half h = tid / 128
+    // stage 0: radix 16 -- one row per thread (block warp / 4); radix 32 --
+    // row tid % 128 of one block, half h0 = tid / 128
+    int b0, j0, h0;
+    uint32_t row0;
+    {
+        const int r = TPR0 == 1 ? tid : tid % 128;
+        h0 = TPR0 == 1 ? 0 : tid / 128;
+        if constexpr (MODE == MODE_BATCH) { b0 = r % B; j0 = r / B; }
+        else { j0 = r % 32; b0 = r / 32; }
+        row0 = ((uint32_t)((warp % 4) * 32) << 16) + (TPR0 == 1 ? (uint32_t)((warp / 4) * BC0) : 0u);
+    }
+    // stage 1: row tid % 128 of one block, half h = tid / 128
     const int h = tid / 128;
     const int rr = tid % 128;
     int b1, j1;
     if constexpr (MODE == MODE_BATCH) { b1 = rr % B; j1 = rr / B; }
-    else { j1 = rr % 16; b1 = rr / 16; }
+    else { j1 = rr % NB1; b1 = rr / NB1; }
     const uint32_t row1 = (uint32_t)((warp % 4) * 32) << 16;
 
     int issued = 0;  // thread 0: tiles of this CTA whose copies were issued
@@ -285,13 +293,13 @@ __global__ void __launch_bounds__(kTc2Threads, 2)
         }
         float2* slot = reinterpret_cast<float2*>(ring + s * SLOT);
 
-        // ---- stage 0: radix-16 DFTs of x[j0 + 32 r] ----
+        // ---- stage 0: radix-R0 DFTs of x[j0 + 32 a] (this thread's 16 a) ----
         float2 x[16];
 #pragma unroll
-        for (int r = 0; r < 16; ++r) {
-            const int n = j0 + 32 * r;
+        for (int q = 0; q < 16; ++q) {
+            const int n = j0 + 32 * (16 * h0 + q);
             if constexpr (MODE == MODE_BATCH) {
-                x[r] = slot[n * B + b0];
+                x[q] = slot[n * B + b0];
             } else {  // [z chunk][b][z within the chunk]
                 int q2, zl;
                 if (m.chunk_shift >= 0) {
@@ -301,26 +309,36 @@ __global__ void __launch_bounds__(kTc2Threads, 2)
                     q2 = n / m.chunk;
                     zl = n - q2 * m.chunk;
                 }
-                x[r] = slot[(q2 * B + b0) * m.chunk + zl];
+                x[q] = slot[(q2 * B + b0) * m.chunk + zl];
             }
         }
         float down = 1.f, up = 1.f;
         if constexpr (FMT == TC_FP16) {
             float mx = 0.f;
 #pragma unroll
-            for (int r = 0; r < 16; ++r) mx = fmaxf(mx, fmaxf(fabsf(x[r].x), fabsf(x[r].y)));
+            for (int q = 0; q < 16; ++q) mx = fmaxf(mx, fmaxf(fabsf(x[q].x), fabsf(x[q].y)));
+            if constexpr (TPR0 == 2) {  // the row's other half
+                pmax[tid] = mx;
+                __syncthreads();
+                mx = fmaxf(mx, pmax[tid ^ 128]);
+            }
             tc2_scale(mx, down, up);
         }
         {
             uint32_t w[16 * NP];
             tc2_split16<FMT>(x, down, w);
-            tc_st32(tmem + row0, reinterpret_cast<const uint32_t(&)[32]>(w));
-            if constexpr (NP == 3) tc_st16(tmem + row0 + 32, w + 32);
+            if constexpr (TPR0 == 1) {
+                tc_st32(tmem + row0, reinterpret_cast<const uint32_t(&)[32]>(w));
+                if constexpr (NP == 3) tc_st16(tmem + row0 + 32, w + 32);
+            } else {
+#pragma unroll
+                for (int q = 0; q < NP; ++q) tc_st16(tmem + row0 + 32 * q + 16 * h0, w + 16 * q);
+            }
             tc_wait_st();
         }
         tc_fence_before();
         __syncthreads();  // all A rows stored; every read of the slot done
-        if (tid == 0) tc2_issue<FMT, 0>(tmem, b_addr, mbar);
+        if (tid == 0) tc2_issue<FMT, R0>(tmem, op0, mbar);
         if (!mma_wait()) {
             ok = false;
             ++i;  // tile i's copy has landed
@@ -328,18 +346,19 @@ __global__ void __launch_bounds__(kTc2Threads, 2)
         }
         {
             float y[32];
-            tc_ld32(tmem + row0 + ACC0, y);
+            tc_ld32(tmem + row0 + ACC0 + 32 * h0, y);
 #pragma unroll
-            for (int k = 0; k < 16; ++k) slot[tc2_pos<MODE>(b0, 16 * j0 + k)] = make_float2(y[k] * up, y[16 + k] * up);
+            for (int q = 0; q < 16; ++q)
+                slot[tc2_pos<N, MODE>(b0, R0 * j0 + 16 * h0 + q)] = make_float2(y[q] * up, y[16 + q] * up);
         }
         tc_fence_before();
         __syncthreads();  // stage-0 outputs in the tile; accumulators read
 
-        // ---- stage 1: twiddles, then radix-32 DFTs over b of tile[j1 + 16 b] ----
+        // ---- stage 1: twiddles, then radix-32 DFTs over b of tile[j1 + NB1 b] ----
 #pragma unroll
         for (int q = 0; q < 16; ++q) {
             const int bb = 16 * h + q;
-            x[q] = cmulw<INV>(slot[tc2_pos<MODE>(b1, j1 + 16 * bb)], tw[bb * 16 + j1]);  // W^0 = 1 exactly
+            x[q] = cmulw<INV>(slot[tc2_pos<N, MODE>(b1, j1 + NB1 * bb)], tw[bb * NB1 + j1]);  // W^0 = 1 exactly
         }
         if constexpr (FMT == TC_FP16) {
             float mx = 0.f;
@@ -359,7 +378,7 @@ __global__ void __launch_bounds__(kTc2Threads, 2)
         tc_fence_before();
         __syncthreads();  // all A rows stored; every read of the tile done
         if (tid == 0) {
-            tc2_issue<FMT, 1>(tmem, b_addr, mbar);
+            tc2_issue<FMT, 32>(tmem, op1, mbar);
             if (issued < mine) {  // the slot is free: refill it with the tile NSTG ahead
                 fence_proxy_async_smem();
                 tmat_issue<float, B, N>(m, blockIdx.x + issued * gridDim.x, tilesV, ring + s * SLOT, rbar + s);
@@ -377,8 +396,7 @@ __global__ void __launch_bounds__(kTc2Threads, 2)
             float2* line = a.dst + base_s[b1];
 #pragma unroll
             for (int q = 0; q < 16; ++q)
-                st_stream(line + offA_s[j1 + 16 * (16 * h + q)],
-                          scl(make_float2(y[q] * up, y[16 + q] * up), a.scale));
+                st_stream(line + offA_s[j1 + NB1 * (16 * h + q)], scl(make_float2(y[q] * up, y[16 + q] * up), a.scale));
         }
         tc_fence_before();
         __syncthreads();  // accumulators read before the next tile's MMAs; line bases free

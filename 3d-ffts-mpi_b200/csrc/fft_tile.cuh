@@ -462,7 +462,7 @@ enum PassKind : int {
     KIND_TCR = 9,     // tensor-core stages, persistent CTAs fed by the in-place 2-slot TMA ring
     KIND_TMAT2S = 10, // the 2-slot ring, batch tiles, first exchange by warp shuffles (R0 R1 = 64 plans)
     KIND_RPIPES = 11, // register-pipelined line-mode tiles, first exchange by warp shuffles (512)
-    KIND_TC2 = 12     // two tensor-core stages (512 = 16 x 32: radix-16 GEMM, twiddle, radix-32 GEMM), TMA ring
+    KIND_TC2 = 12     // two tensor-core stages (512 = 16 x 32, 1024 = 32 x 32: GEMM, twiddle, radix-32 GEMM), TMA ring
 };
 
 constexpr int kTmaBuffers = 2;
