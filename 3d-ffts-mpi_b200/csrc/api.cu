@@ -41,11 +41,12 @@ struct a2a_dfft {
     PassKernel tc[3][2];  // the kernel in use per pass and direction
     // candidates per pass, direction: 0 = one tile per CTA, 1 = persistent
     // CTAs fed by the TMA ring (where the plan and geometry allow it), 2 =
-    // the two-stage form (512 = 16 x 32), also fed by the TMA ring
-    PassKernel tcv[3][2][3];
-    bool tcv_fits[3][3] = {};
-    int tcv_occ[3][3] = {};
-    float tcv_ms[3][3] = {};
+    // the two-stage form (512 = 16 x 32, 1024 = 32 x 32), also fed by the TMA
+    // ring, 3 = the two-stage form with 8-line tiles of 1024
+    PassKernel tcv[3][2][4];
+    bool tcv_fits[3][4] = {};
+    int tcv_occ[3][4] = {};
+    float tcv_ms[3][4] = {};
     int tc_chosen[3] = {0, 0, 0};
     void* d_tc = nullptr;
     const void* tc_tw[3] = {nullptr, nullptr, nullptr};
@@ -644,7 +645,10 @@ cudaError_t run_tc_pass(const a2a_dfft* f, int pass, bool inv, void* p, cudaStre
             ce.lines = k.lines;
         }
         maps = &ce.maps;
-        grid = (unsigned)std::min<uint64_t>(grid, (uint64_t)std::max(f->tcv_occ[pass][two ? 2 : 1], 1) * d.sms);
+        int occ = 1;  // resident CTAs per SM of this candidate
+        for (int c = 1; c < 4; ++c)
+            if (f->tcv_fits[pass][c] && f->tcv[pass][inv ? 1 : 0][c].fn == k.fn) occ = f->tcv_occ[pass][c];
+        grid = (unsigned)std::min<uint64_t>(grid, (uint64_t)std::max(occ, 1) * d.sms);
     }
     a2a::PassArgs<float> a;
     a.src = static_cast<const float2*>(p);
@@ -834,19 +838,24 @@ a2a_status setup_tc(a2a_dfft* f, a2a_method m) {
             ring = g.NV % f->tcv[p][0][1].lines == 0 &&
                    build_tmat(d, p, f->tcv[p][0][1].lines, reinterpret_cast<const void*>(uintptr_t(1) << 20), &probe);
         }
-        // the two-stage form (512), on the same ring geometry with 8-line tiles
-        bool two = true;
-        for (int inv = 0; inv < 2; ++inv)
-            two = two && a2a::find_tc2_kernel(g.n, g.mode, inv, fmt, &f->tcv[p][inv][2]);
-        if (two) {
-            a2a::TmatMaps probe;
-            two = g.NV % f->tcv[p][0][2].lines == 0 &&
-                  build_tmat(d, p, f->tcv[p][0][2].lines, reinterpret_cast<const void*>(uintptr_t(1) << 20), &probe);
+        // the two-stage form (512, 1024; and 1024 with 8-line tiles), on the
+        // same ring geometry
+        bool two[2] = {true, true};
+        for (int w = 0; w < 2; ++w) {
+            for (int inv = 0; inv < 2; ++inv)
+                two[w] = two[w] && a2a::find_tc2_kernel(g.n, g.mode, inv, fmt, w == 1, &f->tcv[p][inv][2 + w]);
+            if (two[w]) {
+                a2a::TmatMaps probe;
+                two[w] = g.NV % f->tcv[p][0][2 + w].lines == 0 &&
+                         build_tmat(d, p, f->tcv[p][0][2 + w].lines, reinterpret_cast<const void*>(uintptr_t(1) << 20),
+                                    &probe);
+            }
         }
         f->tcv_fits[p][0] = true;
         f->tcv_fits[p][1] = ring;
-        f->tcv_fits[p][2] = two;
-        for (int c = 0; c < 3; ++c) {
+        f->tcv_fits[p][2] = two[0];
+        f->tcv_fits[p][3] = two[1];
+        for (int c = 0; c < 4; ++c) {
             f->tcv_ms[p][c] = 0.f;
             if (!f->tcv_fits[p][c]) continue;
             for (int inv = 0; inv < 2; ++inv) {
@@ -881,7 +890,8 @@ a2a_status setup_tc(a2a_dfft* f, a2a_method m) {
             const int by_smem = (int)((size_t)smem_sm / smem_cta);
             const int by_regs = regs_sm / (regs_warp * (kk.threads / 32));
             const int by_thr = thr_sm / kk.threads;
-            const int need = c == 2 ? a2a::tc2_cols(fmt) : (kk.threads / a2a::kTcRows) * a2a::tc_block_cols(fmt);
+            const int need = c >= 2 ? (kk.threads / 256) * a2a::tc2_cols(fmt)
+                                    : (kk.threads / a2a::kTcRows) * a2a::tc_block_cols(fmt);
             int cols = 32;
             while (cols < need) cols *= 2;
             f->tcv_occ[p][c] = std::min(std::min(by_smem, by_regs), std::min(by_thr, 512 / cols));
@@ -911,11 +921,12 @@ a2a_status setup_tc(a2a_dfft* f, a2a_method m) {
     tc_operand_image(true, fmt, b1);
     // the two-stage form, per pass where it fits: W_n^(b k1) (forward sign,
     // [b < 32][k1 < n / 32]) and its operands per direction
+    auto g_len = [&](int p) { return slot_geom(d, p).n; };
     std::vector<char> two;  // host image of the segments, each 256-byte aligned
     size_t seg[3][3] = {};  // per pass: twiddle, forward and inverse operand offsets
     for (int p = 0; p < 3; ++p) {
-        if (!f->tcv_fits[p][2]) continue;
-        const int n = f->tcv[p][0][2].n;
+        if (!f->tcv_fits[p][2] && !f->tcv_fits[p][3]) continue;
+        const int n = g_len(p);
         std::vector<float> t;
         const long double pi = acosl(-1.0L);
         for (int b = 0; b < 32; ++b)
@@ -954,8 +965,9 @@ a2a_status setup_tc(a2a_dfft* f, a2a_method m) {
     if (!two.empty())
         A2A_CUDA(cudaMemcpy(base2, two.data(), two.size(), cudaMemcpyHostToDevice), "cudaMemcpy");
     for (int p = 0; p < 3; ++p) {
-        f->tc2_tw[p] = f->tcv_fits[p][2] ? base2 + seg[p][0] : nullptr;
-        for (int inv = 0; inv < 2; ++inv) f->tc2_b[p][inv] = f->tcv_fits[p][2] ? base2 + seg[p][1 + inv] : nullptr;
+        const bool any = f->tcv_fits[p][2] || f->tcv_fits[p][3];
+        f->tc2_tw[p] = any ? base2 + seg[p][0] : nullptr;
+        for (int inv = 0; inv < 2; ++inv) f->tc2_b[p][inv] = any ? base2 + seg[p][1 + inv] : nullptr;
     }
     return A2A_SUCCESS;
 }
@@ -1283,7 +1295,7 @@ a2a_status a2a_dfft_make_plans(a2a_dfft* f, void** d_scratch) {
         for (int p = 0; p < 3 && e == cudaSuccess; ++p) {
             int best = f->tc_chosen[p];
             float best_ms = 1e30f;
-            for (int c = 0; c < 3 && e == cudaSuccess; ++c) {
+            for (int c = 0; c < 4 && e == cudaSuccess; ++c) {
                 if (!f->tcv_fits[p][c]) continue;
                 for (int inv = 0; inv < 2; ++inv) f->tc[p][inv] = f->tcv[p][inv][c];
                 e = transform();  // warm-up
@@ -1324,7 +1336,7 @@ a2a_status a2a_dfft_check_device(const a2a_dfft* f) {
 a2a_status a2a_dfft_variant_count(const a2a_dfft* f, int pass, int* count) {
     if (!f || !count) return fail(A2A_ERROR_INVALID_VALUE, "NULL argument");
     if (pass < 0 || pass > 2) return fail(A2A_ERROR_INVALID_VALUE, "pass must be 0 (Z), 1 (X) or 2 (Y)");
-    *count = f->method == A2A_METHOD_PLAIN ? f->dist->d.slot[pass][0].ncand : 3;
+    *count = f->method == A2A_METHOD_PLAIN ? f->dist->d.slot[pass][0].ncand : 4;
     return A2A_SUCCESS;
 }
 
@@ -1332,9 +1344,9 @@ a2a_status a2a_dfft_select_variant(a2a_dfft* f, int pass, int variant) {
     if (!f) return fail(A2A_ERROR_INVALID_VALUE, "dfft is NULL");
     if (pass < 0 || pass > 2) return fail(A2A_ERROR_INVALID_VALUE, "pass must be 0 (Z), 1 (X) or 2 (Y)");
     Dist& d = f->dist->d;
-    if (f->method != A2A_METHOD_PLAIN) {  // 0: one tile per CTA, 1: the persistent ring form, 2: two-stage
+    if (f->method != A2A_METHOD_PLAIN) {  // 0: one tile per CTA, 1: ring form, 2: two-stage, 3: two-stage 8-line
         if (!f->tcv[pass][0][0].fn) return fail(A2A_ERROR_NO_PLANS, "the tensor-core kernels are not set up");
-        if (variant < 0 || variant > 2) return fail(A2A_ERROR_INVALID_VALUE, "variant %d outside [0, 3)", variant);
+        if (variant < 0 || variant > 3) return fail(A2A_ERROR_INVALID_VALUE, "variant %d outside [0, 4)", variant);
         if (!f->tcv_fits[pass][variant])
             return fail(A2A_ERROR_UNSUPPORTED, "tensor-core variant %d does not fit this pass", variant);
         f->tc_chosen[pass] = variant;
@@ -1383,7 +1395,7 @@ a2a_status a2a_dfft_plan_report(const a2a_dfft* f, char* buf, size_t len) {
     }
     if (f->method != A2A_METHOD_PLAIN)
         for (int p = 0; p < 3; ++p)
-            for (int c = 0; c < 3; ++c) {
+            for (int c = 0; c < 4; ++c) {
                 if (!f->tcv_fits[p][c]) continue;
                 const PassKernel& k = f->tcv[p][0][c];
                 char line[256];
@@ -1391,7 +1403,7 @@ a2a_status a2a_dfft_plan_report(const a2a_dfft* f, char* buf, size_t len) {
                          "%s pass n=%d tensor-core %s %s lines=%d threads=%d smem=%zu occ=%d radix=%d,%d,%d "
                          "tuned_ms=%.4f%s\n",
                          names[p], k.n, f->method == A2A_METHOD_SPLIT_FP16 ? "split-fp16" : "split-bf16",
-                         c == 2 ? "two-stage" : c ? "ring" : "tile", k.lines, k.threads, k.smem, f->tcv_occ[p][c], k.radix[0], k.radix[1],
+                         c >= 2 ? "two-stage" : c ? "ring" : "tile", k.lines, k.threads, k.smem, f->tcv_occ[p][c], k.radix[0], k.radix[1],
                          k.radix[2], f->tcv_ms[p][c], c == f->tc_chosen[p] ? " <- in use" : "");
                 out += line;
             }

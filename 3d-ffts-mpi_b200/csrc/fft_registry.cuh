@@ -332,7 +332,8 @@ bool find_tc_ring_kernel(int n, int mode, bool inverse, int fmt, PassKernel* out
 // the two-stage tensor-core form (512 = 16 x 32, 1024 = 32 x 32: radix-R0
 // GEMM, twiddle, radix-32 GEMM), fed by the TMA ring; its operand is
 // tc2_b_bytes<n>(fmt) bytes per direction and its twiddle table W_n^(b k1)
-// laid out [b < 32][k1 < n / 32]
-bool find_tc2_kernel(int n, int mode, bool inverse, int fmt, PassKernel* out);
+// laid out [b < 32][k1 < n / 32].  wide: the 8-line, 512-thread tiles of
+// 1024 (else 8 lines at 512, 4 at 1024)
+bool find_tc2_kernel(int n, int mode, bool inverse, int fmt, bool wide, PassKernel* out);
 
 }  // namespace a2a

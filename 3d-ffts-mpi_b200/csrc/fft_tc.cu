@@ -80,16 +80,16 @@ bool find_tc_ring_kernel(int n, int mode, bool inverse, int fmt, PassKernel* out
     }
 }
 
-template <int N, int MODE, bool INV, int FMT> PassKernel make_tc2_kernel() {
-    using G = Tc2Geom<N>;
+template <int N, int BL, int MODE, bool INV, int FMT> PassKernel make_tc2_kernel() {
+    using G = Tc2Geom<N, BL>;
     PassKernel k;
-    k.fn = reinterpret_cast<const void*>(&fft_tc2_ring_kernel<N, MODE, INV, FMT>);
+    k.fn = reinterpret_cast<const void*>(&fft_tc2_ring_kernel<N, BL, MODE, INV, FMT>);
     k.kind = KIND_TC2;
-    k.smem = tc2_smem_bytes<N>(FMT);
+    k.smem = tc2_smem_bytes<N, BL>(FMT);
     k.n = N;
-    k.threads = kTc2Threads;
+    k.threads = G::THREADS;
     k.lines = G::B;
-    k.min_blocks = 2;
+    k.min_blocks = G::THREADS == 512 ? 1 : 2;
     k.lpt = 1;
     k.nstages = 2;
     k.radix[0] = G::R0;
@@ -98,8 +98,9 @@ template <int N, int MODE, bool INV, int FMT> PassKernel make_tc2_kernel() {
     return k;
 }
 
-template <int N> PassKernel tc2_pick(int mode, bool inverse, int fmt) {
-#define A2A_TC2(M_, F_) return inverse ? make_tc2_kernel<N, M_, true, F_>() : make_tc2_kernel<N, M_, false, F_>()
+template <int N, int BL> PassKernel tc2_pick(int mode, bool inverse, int fmt) {
+#define A2A_TC2(M_, F_) \
+    return inverse ? make_tc2_kernel<N, BL, M_, true, F_>() : make_tc2_kernel<N, BL, M_, false, F_>()
     if (mode == MODE_LINE) {
         if (fmt == TC_FP16) A2A_TC2(MODE_LINE, TC_FP16); else A2A_TC2(MODE_LINE, TC_BF16);
     } else {
@@ -108,12 +109,10 @@ template <int N> PassKernel tc2_pick(int mode, bool inverse, int fmt) {
 #undef A2A_TC2
 }
 
-bool find_tc2_kernel(int n, int mode, bool inverse, int fmt, PassKernel* out) {
-    switch (n) {
-        case 512: *out = tc2_pick<512>(mode, inverse, fmt); return true;
-        case 1024: *out = tc2_pick<1024>(mode, inverse, fmt); return true;
-        default: return false;
-    }
+bool find_tc2_kernel(int n, int mode, bool inverse, int fmt, bool wide, PassKernel* out) {
+    if (n == 512 && !wide) { *out = tc2_pick<512, 8>(mode, inverse, fmt); return true; }
+    if (n == 1024) { *out = wide ? tc2_pick<1024, 8>(mode, inverse, fmt) : tc2_pick<1024, 4>(mode, inverse, fmt); return true; }
+    return false;
 }
 
 }  // namespace a2a

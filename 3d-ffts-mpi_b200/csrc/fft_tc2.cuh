@@ -27,23 +27,30 @@
 
 namespace a2a {
 
-constexpr int kTc2Threads = 256;
 // the radix-32 operand: K-major N x K, N = K = 64 (16-bit values): a K chunk
 // of 8 values over all 64 rows is 1 KB, one part 8 KB
 constexpr int kTc2ChunkB1 = 64 / 8 * 128;
 constexpr int kTc2MatB1 = 8 * kTc2ChunkB1;
 
-template <int N> struct Tc2Geom {
-    static_assert(N == 512 || N == 1024, "two-stage lengths: 512 = 16 x 32 and 1024 = 32 x 32");
+// Geometry of one instance: N = 512 with 8-line tiles, N = 1024 with 4- or
+// 8-line tiles.  A radix-16 row has one thread, a radix-32 row two; rows are
+// grouped in 128-row blocks of tensor memory.
+template <int N, int BL> struct Tc2Geom {
+    static_assert((N == 512 && BL == 8) || (N == 1024 && (BL == 4 || BL == 8)),
+                  "two-stage instances: 512 = 16 x 32 (8 lines), 1024 = 32 x 32 (4 or 8 lines)");
     static constexpr int R0 = N / 32;                  // first radix (16 or 32); the second is 32
     static constexpr int NB1 = N / 32;                 // stage-1 rows per line (= R0)
-    static constexpr int B = N == 512 ? 8 : 4;         // lines per tile (32 KB)
-    static constexpr int ROWS0 = B * 32;               // stage-0 rows: 256 or 128
-    static constexpr int TPR0 = kTc2Threads / ROWS0;   // threads per stage-0 row: 1 or 2
+    static constexpr int B = BL;                       // lines per tile
+    static constexpr int ROWS0 = B * 32;               // stage-0 rows
+    static constexpr int ROWS1 = B * NB1;              // stage-1 rows
+    static constexpr int TPR0 = R0 == 16 ? 1 : 2;      // threads per stage-0 row
+    static constexpr int THREADS = ROWS1 * 2;          // two threads per radix-32 row
+    static constexpr int NBLK0 = ROWS0 / 128;          // 128-row blocks per stage
+    static constexpr int NBLK1 = ROWS1 / 128;
     static constexpr int SH = R0 == 16 ? 4 : 5;        // log2 R0
     static constexpr int RMASK = 128 / (B * 8) - 1;    // batch-mode tile rows per 128 bytes, minus 1
     static constexpr int TW = 32 * NB1;                // twiddles W_N^(b k1), [b][k1]
-    static_assert(B * NB1 == 128, "one 128-row stage-1 block, two threads per row");
+    static_assert(ROWS0 * TPR0 == THREADS, "every thread has one stage-0 row (part)");
 };
 
 // both operands of one direction: the radix-16 parts (512 only), then the
@@ -54,22 +61,25 @@ template <int N> __host__ __device__ constexpr int tc2_b_bytes(int fmt) {
 // tensor-memory columns: stage 0 (two blocks of 16 per part + 32, or one of 32
 // per part + 64) and stage 1 (one block of 32 per part + 64) take the same
 // count, reused
+// (per 128-row block of a stage)
 __host__ __device__ constexpr int tc2_cols(int fmt) { return 32 * tc_parts(fmt) + 64; }
-__host__ __device__ constexpr uint32_t tc2_tcols(int fmt) { return tc2_cols(fmt) <= 128 ? 128u : 256u; }
+template <int NBLK> __host__ __device__ constexpr uint32_t tc2_tcols(int fmt) {
+    return NBLK * tc2_cols(fmt) <= 128 ? 128u : NBLK * tc2_cols(fmt) <= 256 ? 256u : 512u;
+}
 
 __host__ __device__ constexpr uint32_t umma_idesc_f16_n(int fmt, int n) {
     return (1u << 4) | ((uint32_t)fmt << 7) | ((uint32_t)fmt << 10) | (((uint32_t)n >> 3) << 17) | ((128u >> 4) << 24);
 }
 
-template <int N> __host__ __device__ constexpr size_t tc2_smem_bytes(int fmt) {
-    using G = Tc2Geom<N>;
+template <int N, int BL> __host__ __device__ constexpr size_t tc2_smem_bytes(int fmt) {
+    using G = Tc2Geom<N, BL>;
     size_t bytes = kTmatAlign;                                   // room to align the ring
     bytes += 2 * (size_t)tmat_slot_bytes<float, G::B, N>();      // two slots
     bytes += (size_t)tc2_b_bytes<N>(fmt);
     bytes += sizeof(float2) * (size_t)G::TW;
     bytes += sizeof(uint32_t) * (size_t)N;
     bytes += sizeof(size_t) * (size_t)G::B;
-    bytes += sizeof(float) * (size_t)kTc2Threads;                // radix-32 row maxima (fp16)
+    bytes += sizeof(float) * (size_t)G::THREADS;                 // radix-32 row maxima (fp16)
     bytes += sizeof(unsigned long long) * 3 + 16;                // ring barriers, MMA barrier, tmem address, wait flag
     return bytes;
 }
@@ -80,8 +90,8 @@ template <int N> __host__ __device__ constexpr size_t tc2_smem_bytes(int fmt) {
 // mode: [b][n] with n's low four bits XOR-ed with (n >> log2 R0), so the
 // positions R0 apart that a half-warp writes fall in distinct banks.  Stage 1's
 // reads stay conflict-free under both.
-template <int N, int MODE> __device__ __forceinline__ int tc2_pos(int b, int n) {
-    using G = Tc2Geom<N>;
+template <int N, int BL, int MODE> __device__ __forceinline__ int tc2_pos(int b, int n) {
+    using G = Tc2Geom<N, BL>;
     if constexpr (MODE == MODE_BATCH) return (n ^ ((n >> G::SH) & G::RMASK)) * G::B + b;
     else return b * N + (n ^ ((n >> G::SH) & 15));
 }
@@ -113,15 +123,15 @@ template <int FMT> __device__ __forceinline__ void tc2_split16(const float2 (&x)
     }
 }
 
-// Thread 0: the MMAs of one GEMM stage, then the commit.  Radix 16: two
-// 128-row blocks (columns 0 and 16 NP + 32), K = 32 (two K = 16 steps per
-// term), N = 32; radix 32: one block, K = 64 (four steps per term), N = 64.
+// Thread 0: the MMAs of one GEMM stage over its NBLK 128-row blocks, then the
+// commit.  Radix 16: blocks of 16 NP + 32 columns, K = 32 (two K = 16 steps
+// per term), N = 32; radix 32: blocks of 32 NP + 64 columns, K = 64 (four
+// steps per term), N = 64.
 // `op` is the stage's split operand in shared memory.  Terms smallest first,
 // as in fft_tc.cuh.
-template <int FMT, int R>
+template <int FMT, int R, int NBLK>
 __device__ __forceinline__ void tc2_issue(uint32_t tmem, uint32_t op, unsigned long long* bar) {
     constexpr int NP = tc_parts(FMT);
-    constexpr int NBLK = R == 16 ? 2 : 1;
     constexpr int AC = R;                // A columns per part: 2R values, two per column
     constexpr int BC = NP * AC + 2 * R;  // block columns (A parts, then the accumulator)
     constexpr int KSTEPS = R / 8;        // K = 16 steps per term
@@ -162,30 +172,31 @@ __device__ __forceinline__ void tc2_issue(uint32_t tmem, uint32_t op, unsigned l
 // device error flag is raised, the rest of the pass is skipped, the CTA waits
 // (bounded) for its copies in flight and frees its tensor memory only if the
 // MMAs it committed were seen to finish.
-template <int N, int MODE, bool INV, int FMT>
-__global__ void __launch_bounds__(kTc2Threads, 2)
+template <int N, int BL, int MODE, bool INV, int FMT>
+__global__ void __launch_bounds__(Tc2Geom<N, BL>::THREADS, Tc2Geom<N, BL>::THREADS == 512 ? 1 : 2)
     fft_tc2_ring_kernel(const PassArgs<float> a, const __grid_constant__ TmatMaps m) {
-    using G = Tc2Geom<N>;
+    using G = Tc2Geom<N, BL>;
     constexpr int R0 = G::R0;
     constexpr int NB1 = G::NB1;
     constexpr int B = G::B;
     constexpr int TPR0 = G::TPR0;
-    constexpr int THREADS = kTc2Threads;
+    constexpr int THREADS = G::THREADS;
     constexpr int NP = tc_parts(FMT);
     constexpr int BC0 = NP * R0 + 2 * R0;  // stage-0 block columns (A parts, then the accumulator)
     constexpr int ACC0 = NP * R0;          // stage-0 accumulator, within its block
-    constexpr int ACC1 = 32 * NP;          // stage-1 accumulator (64 columns)
-    constexpr uint32_t TCOLS = tc2_tcols(FMT);
-    constexpr uint32_t SLOT = tmat_slot_bytes<float, B, N>();
+    constexpr int BC1 = 32 * NP + 64;      // stage-1 block columns
+    constexpr int ACC1 = 32 * NP;          // stage-1 accumulator (64 columns), within its block
+    constexpr uint32_t TCOLS = tc2_tcols<G::NBLK1>(FMT);
+    constexpr uint32_t SLOT = tmat_slot_bytes<float, B, N>();  // B lines x N complex
     constexpr int NSTG = 2;
     static_assert(B * N * sizeof(float2) <= SLOT, "a tile fits its slot");
-    static_assert((TPR0 == 1 ? 2 : 1) * BC0 <= (int)TCOLS && ACC1 + 64 <= (int)TCOLS, "tensor-memory columns");
+    static_assert(G::NBLK0 * BC0 <= (int)TCOLS && G::NBLK1 * BC1 <= (int)TCOLS, "tensor-memory columns");
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const uint32_t s0 = smem_u32(smem_raw);
     unsigned char* ring = smem_raw + (((s0 + kTmatAlign - 1) & ~(kTmatAlign - 1)) - s0);
     unsigned char* bmat = ring + NSTG * SLOT;
-    float2* tw = reinterpret_cast<float2*>(bmat + tc2_b_bytes<N>(FMT));
+    float2* tw = reinterpret_cast<float2*>(bmat + tc2_b_bytes<N>(FMT));  // (operands of N, any tile height)
     uint32_t* offA_s = reinterpret_cast<uint32_t*>(tw + G::TW);
     size_t* base_s = reinterpret_cast<size_t*>(offA_s + N);
     float* pmax = reinterpret_cast<float*>(base_s + B);
@@ -228,24 +239,26 @@ __global__ void __launch_bounds__(kTc2Threads, 2)
     uint32_t phase = 0;
     bool drained = true;
 
-    // stage 0: radix 16 -- one row per thread (block warp / 4); radix 32 --
-    // row tid % 128 of one block, half h0 = tid / 128
+    // stage 0: radix 16 -- row tid (block tid / 128), one thread per row;
+    // radix 32 -- row (tid / 256) * 128 + tid % 128, half h0 = (tid / 128) % 2.
+    // The lane of a row is tid % 128, which warp tid / 32 reaches.
     int b0, j0, h0;
     uint32_t row0;
     {
-        const int r = TPR0 == 1 ? tid : tid % 128;
-        h0 = TPR0 == 1 ? 0 : tid / 128;
+        const int blk = TPR0 == 1 ? tid / 128 : tid / 256;
+        const int r = blk * 128 + tid % 128;
+        h0 = TPR0 == 1 ? 0 : (tid / 128) % 2;
         if constexpr (MODE == MODE_BATCH) { b0 = r % B; j0 = r / B; }
         else { j0 = r % 32; b0 = r / 32; }
-        row0 = ((uint32_t)((warp % 4) * 32) << 16) + (TPR0 == 1 ? (uint32_t)((warp / 4) * BC0) : 0u);
+        row0 = ((uint32_t)((warp % 4) * 32) << 16) + (uint32_t)(blk * BC0);
     }
-    // stage 1: row tid % 128 of one block, half h = tid / 128
-    const int h = tid / 128;
-    const int rr = tid % 128;
+    // stage 1: row (tid / 256) * 128 + tid % 128, half h = (tid / 128) % 2
+    const int h = (tid / 128) % 2;
+    const int rr = (tid / 256) * 128 + tid % 128;
     int b1, j1;
     if constexpr (MODE == MODE_BATCH) { b1 = rr % B; j1 = rr / B; }
     else { j1 = rr % NB1; b1 = rr / NB1; }
-    const uint32_t row1 = (uint32_t)((warp % 4) * 32) << 16;
+    const uint32_t row1 = ((uint32_t)((warp % 4) * 32) << 16) + (uint32_t)((tid / 256) * BC1);
 
     int issued = 0;  // thread 0: tiles of this CTA whose copies were issued
     if (tid == 0)
@@ -338,7 +351,7 @@ __global__ void __launch_bounds__(kTc2Threads, 2)
         }
         tc_fence_before();
         __syncthreads();  // all A rows stored; every read of the slot done
-        if (tid == 0) tc2_issue<FMT, R0>(tmem, op0, mbar);
+        if (tid == 0) tc2_issue<FMT, R0, G::NBLK0>(tmem, op0, mbar);
         if (!mma_wait()) {
             ok = false;
             ++i;  // tile i's copy has landed
@@ -349,7 +362,7 @@ __global__ void __launch_bounds__(kTc2Threads, 2)
             tc_ld32(tmem + row0 + ACC0 + 32 * h0, y);
 #pragma unroll
             for (int q = 0; q < 16; ++q)
-                slot[tc2_pos<N, MODE>(b0, R0 * j0 + 16 * h0 + q)] = make_float2(y[q] * up, y[16 + q] * up);
+                slot[tc2_pos<N, BL, MODE>(b0, R0 * j0 + 16 * h0 + q)] = make_float2(y[q] * up, y[16 + q] * up);
         }
         tc_fence_before();
         __syncthreads();  // stage-0 outputs in the tile; accumulators read
@@ -358,7 +371,7 @@ __global__ void __launch_bounds__(kTc2Threads, 2)
 #pragma unroll
         for (int q = 0; q < 16; ++q) {
             const int bb = 16 * h + q;
-            x[q] = cmulw<INV>(slot[tc2_pos<N, MODE>(b1, j1 + NB1 * bb)], tw[bb * NB1 + j1]);  // W^0 = 1 exactly
+            x[q] = cmulw<INV>(slot[tc2_pos<N, BL, MODE>(b1, j1 + NB1 * bb)], tw[bb * NB1 + j1]);  // W^0 = 1 exactly
         }
         if constexpr (FMT == TC_FP16) {
             float mx = 0.f;
@@ -378,7 +391,7 @@ __global__ void __launch_bounds__(kTc2Threads, 2)
         tc_fence_before();
         __syncthreads();  // all A rows stored; every read of the tile done
         if (tid == 0) {
-            tc2_issue<FMT, 32>(tmem, op1, mbar);
+            tc2_issue<FMT, 32, G::NBLK1>(tmem, op1, mbar);
             if (issued < mine) {  // the slot is free: refill it with the tile NSTG ahead
                 fence_proxy_async_smem();
                 tmat_issue<float, B, N>(m, blockIdx.x + issued * gridDim.x, tilesV, ring + s * SLOT, rbar + s);
