@@ -922,7 +922,7 @@ a2a_status setup_tc(a2a_dfft* f, a2a_method m) {
     // the two-stage form, per pass where it fits: W_n^(b k1) (forward sign,
     // [b < 32][k1 < n / 32]) and its operands per direction
     auto g_len = [&](int p) { return slot_geom(d, p).n; };
-    std::vector<char> two;  // host image of the segments, each 256-byte aligned
+    std::vector<char> img2;  // host image of the segments, each 256-byte aligned
     size_t seg[3][3] = {};  // per pass: twiddle, forward and inverse operand offsets
     for (int p = 0; p < 3; ++p) {
         if (!f->tcv_fits[p][2] && !f->tcv_fits[p][3]) continue;
@@ -936,9 +936,9 @@ a2a_status setup_tc(a2a_dfft* f, a2a_method m) {
                 t.push_back((float)-sinl(ang));
             }
         auto append = [&](const void* src, size_t bytes) {
-            const size_t at = (two.size() + 255) & ~size_t(255);
-            two.resize(at + bytes);
-            std::memcpy(two.data() + at, src, bytes);
+            const size_t at = (img2.size() + 255) & ~size_t(255);
+            img2.resize(at + bytes);
+            std::memcpy(img2.data() + at, src, bytes);
             return at;
         };
         seg[p][0] = append(t.data(), t.size() * sizeof(float));
@@ -948,11 +948,11 @@ a2a_status setup_tc(a2a_dfft* f, a2a_method m) {
             seg[p][1 + inv] = append(img.data(), img.size() * sizeof(uint16_t));
         }
     }
-    const size_t two_bytes = (two.size() + 255) & ~size_t(255);
+    const size_t img2_bytes = (img2.size() + 255) & ~size_t(255);
     if (f->d_tc) cudaFree(f->d_tc);
     f->d_tc = nullptr;
     const size_t bb = (size_t)a2a::tc_b_bytes(fmt);
-    A2A_CUDA(cudaMalloc(&f->d_tc, tw_bytes + 2 * bb + two_bytes), "cudaMalloc(tensor-core tables)");
+    A2A_CUDA(cudaMalloc(&f->d_tc, tw_bytes + 2 * bb + img2_bytes), "cudaMalloc(tensor-core tables)");
     char* base = static_cast<char*>(f->d_tc);
     if (!tw.empty())
         A2A_CUDA(cudaMemcpy(base, tw.data(), tw.size() * sizeof(float), cudaMemcpyHostToDevice), "cudaMemcpy");
@@ -962,8 +962,8 @@ a2a_status setup_tc(a2a_dfft* f, a2a_method m) {
     f->tc_b[0] = base + tw_bytes;
     f->tc_b[1] = base + tw_bytes + bb;
     char* base2 = base + tw_bytes + 2 * bb;  // 256-byte aligned (tw_bytes a 256-byte, bb a 2 KB multiple)
-    if (!two.empty())
-        A2A_CUDA(cudaMemcpy(base2, two.data(), two.size(), cudaMemcpyHostToDevice), "cudaMemcpy");
+    if (!img2.empty())
+        A2A_CUDA(cudaMemcpy(base2, img2.data(), img2.size(), cudaMemcpyHostToDevice), "cudaMemcpy");
     for (int p = 0; p < 3; ++p) {
         const bool any = f->tcv_fits[p][2] || f->tcv_fits[p][3];
         f->tc2_tw[p] = any ? base2 + seg[p][0] : nullptr;
