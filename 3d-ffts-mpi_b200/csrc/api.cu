@@ -42,11 +42,12 @@ struct a2a_dfft {
     // candidates per pass, direction: 0 = one tile per CTA, 1 = persistent
     // CTAs fed by the TMA ring (where the plan and geometry allow it), 2 =
     // the two-stage form (512 = 16 x 32, 1024 = 32 x 32), also fed by the TMA
-    // ring, 3 = the two-stage form with 8-line tiles of 1024
-    PassKernel tcv[3][2][4];
-    bool tcv_fits[3][4] = {};
-    int tcv_occ[3][4] = {};
-    float tcv_ms[3][4] = {};
+    // ring, 3 = the two-stage form with 8-line tiles of 1024, 4 = the
+    // software-pipelined two-stage form (fp16)
+    PassKernel tcv[3][2][5];
+    bool tcv_fits[3][5] = {};
+    int tcv_occ[3][5] = {};
+    float tcv_ms[3][5] = {};
     int tc_chosen[3] = {0, 0, 0};
     void* d_tc = nullptr;
     const void* tc_tw[3] = {nullptr, nullptr, nullptr};
@@ -646,7 +647,7 @@ cudaError_t run_tc_pass(const a2a_dfft* f, int pass, bool inv, void* p, cudaStre
         }
         maps = &ce.maps;
         int occ = 1;  // resident CTAs per SM of this candidate
-        for (int c = 1; c < 4; ++c)
+        for (int c = 1; c < 5; ++c)
             if (f->tcv_fits[pass][c] && f->tcv[pass][inv ? 1 : 0][c].fn == k.fn) occ = f->tcv_occ[pass][c];
         grid = (unsigned)std::min<uint64_t>(grid, (uint64_t)std::max(occ, 1) * d.sms);
     }
@@ -855,7 +856,16 @@ a2a_status setup_tc(a2a_dfft* f, a2a_method m) {
         f->tcv_fits[p][1] = ring;
         f->tcv_fits[p][2] = two[0];
         f->tcv_fits[p][3] = two[1];
-        for (int c = 0; c < 4; ++c) {
+        // the pipelined two-stage form (fp16)
+        bool pipe = true;
+        for (int inv = 0; inv < 2; ++inv) pipe = pipe && a2a::find_tc2p_kernel(g.n, g.mode, inv, fmt, &f->tcv[p][inv][4]);
+        if (pipe) {
+            a2a::TmatMaps probe;
+            pipe = g.NV % f->tcv[p][0][4].lines == 0 &&
+                   build_tmat(d, p, f->tcv[p][0][4].lines, reinterpret_cast<const void*>(uintptr_t(1) << 20), &probe);
+        }
+        f->tcv_fits[p][4] = pipe;
+        for (int c = 0; c < 5; ++c) {
             f->tcv_ms[p][c] = 0.f;
             if (!f->tcv_fits[p][c]) continue;
             for (int inv = 0; inv < 2; ++inv) {
@@ -890,8 +900,9 @@ a2a_status setup_tc(a2a_dfft* f, a2a_method m) {
             const int by_smem = (int)((size_t)smem_sm / smem_cta);
             const int by_regs = regs_sm / (regs_warp * (kk.threads / 32));
             const int by_thr = thr_sm / kk.threads;
-            const int need = c >= 2 ? (kk.threads / 256) * a2a::tc2_cols(fmt)
-                                    : (kk.threads / a2a::kTcRows) * a2a::tc_block_cols(fmt);
+            const int need = c == 4   ? 2 * a2a::tc2_cols(fmt)  // two regions
+                             : c >= 2 ? (kk.threads / 256) * a2a::tc2_cols(fmt)
+                                      : (kk.threads / a2a::kTcRows) * a2a::tc_block_cols(fmt);
             int cols = 32;
             while (cols < need) cols *= 2;
             f->tcv_occ[p][c] = std::min(std::min(by_smem, by_regs), std::min(by_thr, 512 / cols));
@@ -925,7 +936,7 @@ a2a_status setup_tc(a2a_dfft* f, a2a_method m) {
     std::vector<char> img2;  // host image of the segments, each 256-byte aligned
     size_t seg[3][3] = {};  // per pass: twiddle, forward and inverse operand offsets
     for (int p = 0; p < 3; ++p) {
-        if (!f->tcv_fits[p][2] && !f->tcv_fits[p][3]) continue;
+        if (!f->tcv_fits[p][2] && !f->tcv_fits[p][3] && !f->tcv_fits[p][4]) continue;
         const int n = g_len(p);
         std::vector<float> t;
         const long double pi = acosl(-1.0L);
@@ -965,7 +976,7 @@ a2a_status setup_tc(a2a_dfft* f, a2a_method m) {
     if (!img2.empty())
         A2A_CUDA(cudaMemcpy(base2, img2.data(), img2.size(), cudaMemcpyHostToDevice), "cudaMemcpy");
     for (int p = 0; p < 3; ++p) {
-        const bool any = f->tcv_fits[p][2] || f->tcv_fits[p][3];
+        const bool any = f->tcv_fits[p][2] || f->tcv_fits[p][3] || f->tcv_fits[p][4];
         f->tc2_tw[p] = any ? base2 + seg[p][0] : nullptr;
         for (int inv = 0; inv < 2; ++inv) f->tc2_b[p][inv] = any ? base2 + seg[p][1 + inv] : nullptr;
     }
@@ -1295,7 +1306,7 @@ a2a_status a2a_dfft_make_plans(a2a_dfft* f, void** d_scratch) {
         for (int p = 0; p < 3 && e == cudaSuccess; ++p) {
             int best = f->tc_chosen[p];
             float best_ms = 1e30f;
-            for (int c = 0; c < 4 && e == cudaSuccess; ++c) {
+            for (int c = 0; c < 5 && e == cudaSuccess; ++c) {
                 if (!f->tcv_fits[p][c]) continue;
                 for (int inv = 0; inv < 2; ++inv) f->tc[p][inv] = f->tcv[p][inv][c];
                 e = transform();  // warm-up
@@ -1336,7 +1347,7 @@ a2a_status a2a_dfft_check_device(const a2a_dfft* f) {
 a2a_status a2a_dfft_variant_count(const a2a_dfft* f, int pass, int* count) {
     if (!f || !count) return fail(A2A_ERROR_INVALID_VALUE, "NULL argument");
     if (pass < 0 || pass > 2) return fail(A2A_ERROR_INVALID_VALUE, "pass must be 0 (Z), 1 (X) or 2 (Y)");
-    *count = f->method == A2A_METHOD_PLAIN ? f->dist->d.slot[pass][0].ncand : 4;
+    *count = f->method == A2A_METHOD_PLAIN ? f->dist->d.slot[pass][0].ncand : 5;
     return A2A_SUCCESS;
 }
 
@@ -1344,9 +1355,9 @@ a2a_status a2a_dfft_select_variant(a2a_dfft* f, int pass, int variant) {
     if (!f) return fail(A2A_ERROR_INVALID_VALUE, "dfft is NULL");
     if (pass < 0 || pass > 2) return fail(A2A_ERROR_INVALID_VALUE, "pass must be 0 (Z), 1 (X) or 2 (Y)");
     Dist& d = f->dist->d;
-    if (f->method != A2A_METHOD_PLAIN) {  // 0: one tile per CTA, 1: ring form, 2: two-stage, 3: two-stage 8-line
+    if (f->method != A2A_METHOD_PLAIN) {  // 0: tile, 1: ring, 2: two-stage, 3: two-stage 8-line, 4: pipelined
         if (!f->tcv[pass][0][0].fn) return fail(A2A_ERROR_NO_PLANS, "the tensor-core kernels are not set up");
-        if (variant < 0 || variant > 3) return fail(A2A_ERROR_INVALID_VALUE, "variant %d outside [0, 4)", variant);
+        if (variant < 0 || variant > 4) return fail(A2A_ERROR_INVALID_VALUE, "variant %d outside [0, 5)", variant);
         if (!f->tcv_fits[pass][variant])
             return fail(A2A_ERROR_UNSUPPORTED, "tensor-core variant %d does not fit this pass", variant);
         f->tc_chosen[pass] = variant;
@@ -1395,7 +1406,7 @@ a2a_status a2a_dfft_plan_report(const a2a_dfft* f, char* buf, size_t len) {
     }
     if (f->method != A2A_METHOD_PLAIN)
         for (int p = 0; p < 3; ++p)
-            for (int c = 0; c < 4; ++c) {
+            for (int c = 0; c < 5; ++c) {
                 if (!f->tcv_fits[p][c]) continue;
                 const PassKernel& k = f->tcv[p][0][c];
                 char line[256];
@@ -1403,7 +1414,7 @@ a2a_status a2a_dfft_plan_report(const a2a_dfft* f, char* buf, size_t len) {
                          "%s pass n=%d tensor-core %s %s lines=%d threads=%d smem=%zu occ=%d radix=%d,%d,%d "
                          "tuned_ms=%.4f%s\n",
                          names[p], k.n, f->method == A2A_METHOD_SPLIT_FP16 ? "split-fp16" : "split-bf16",
-                         c >= 2 ? "two-stage" : c ? "ring" : "tile", k.lines, k.threads, k.smem, f->tcv_occ[p][c], k.radix[0], k.radix[1],
+                         c == 4 ? "two-stage-pipelined" : c >= 2 ? "two-stage" : c ? "ring" : "tile", k.lines, k.threads, k.smem, f->tcv_occ[p][c], k.radix[0], k.radix[1],
                          k.radix[2], f->tcv_ms[p][c], c == f->tc_chosen[p] ? " <- in use" : "");
                 out += line;
             }

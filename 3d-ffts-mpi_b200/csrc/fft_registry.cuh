@@ -335,5 +335,8 @@ bool find_tc_ring_kernel(int n, int mode, bool inverse, int fmt, PassKernel* out
 // laid out [b < 32][k1 < n / 32].  wide: the 8-line, 512-thread tiles of
 // 1024 (else 8 lines at 512, 4 at 1024)
 bool find_tc2_kernel(int n, int mode, bool inverse, int fmt, bool wide, PassKernel* out);
+// its software-pipelined form (fp16; 512 with 8-line, 1024 with 4-line tiles):
+// the same tables
+bool find_tc2p_kernel(int n, int mode, bool inverse, int fmt, PassKernel* out);
 
 }  // namespace a2a

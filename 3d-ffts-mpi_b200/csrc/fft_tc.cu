@@ -109,6 +109,36 @@ template <int N, int BL> PassKernel tc2_pick(int mode, bool inverse, int fmt) {
 #undef A2A_TC2
 }
 
+template <int N, int BL> PassKernel tc2p_pick(int mode, bool inverse) {
+    using G = Tc2Geom<N, BL>;
+    PassKernel k;
+    if (mode == MODE_LINE)
+        k.fn = inverse ? reinterpret_cast<const void*>(&fft_tc2p_ring_kernel<N, BL, MODE_LINE, true>)
+                       : reinterpret_cast<const void*>(&fft_tc2p_ring_kernel<N, BL, MODE_LINE, false>);
+    else
+        k.fn = inverse ? reinterpret_cast<const void*>(&fft_tc2p_ring_kernel<N, BL, MODE_BATCH, true>)
+                       : reinterpret_cast<const void*>(&fft_tc2p_ring_kernel<N, BL, MODE_BATCH, false>);
+    k.kind = KIND_TC2;
+    k.smem = tc2p_smem_bytes<N, BL>();
+    k.n = N;
+    k.threads = G::THREADS;
+    k.lines = G::B;
+    k.min_blocks = 2;
+    k.lpt = 1;
+    k.nstages = 2;
+    k.radix[0] = G::R0;
+    k.radix[1] = 32;
+    k.twtotal = G::TW;
+    return k;
+}
+
+bool find_tc2p_kernel(int n, int mode, bool inverse, int fmt, PassKernel* out) {
+    if (fmt != TC_FP16) return false;
+    if (n == 512) { *out = tc2p_pick<512, 8>(mode, inverse); return true; }
+    if (n == 1024) { *out = tc2p_pick<1024, 4>(mode, inverse); return true; }
+    return false;
+}
+
 bool find_tc2_kernel(int n, int mode, bool inverse, int fmt, bool wide, PassKernel* out) {
     if (n == 512 && !wide) { *out = tc2_pick<512, 8>(mode, inverse, fmt); return true; }
     if (n == 1024) { *out = wide ? tc2_pick<1024, 8>(mode, inverse, fmt) : tc2_pick<1024, 4>(mode, inverse, fmt); return true; }

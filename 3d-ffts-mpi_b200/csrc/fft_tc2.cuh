@@ -165,6 +165,103 @@ __device__ __forceinline__ void tc2_issue(uint32_t tmem, uint32_t op, unsigned l
     tc_commit(bar);
 }
 
+// ---- the stage steps of one thread (shared by the kernels below) ----
+
+// Stage-0 inputs x[j0 + 32 a] of line b0 from the TMA slot, for this thread's
+// 16 values of a (a = 16 h0 + q).
+template <int N, int BL, int MODE>
+__device__ __forceinline__ void tc2_s0_load(const float2* slot, const TmatMaps& m, int b0, int j0, int h0,
+                                            float2 (&x)[16]) {
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+        const int n = j0 + 32 * (16 * h0 + q);
+        if constexpr (MODE == MODE_BATCH) {
+            x[q] = slot[n * BL + b0];
+        } else {  // [z chunk][b][z within the chunk]
+            int q2, zl;
+            if (m.chunk_shift >= 0) {
+                q2 = n >> m.chunk_shift;
+                zl = n & (m.chunk - 1);
+            } else {
+                q2 = n / m.chunk;
+                zl = n - q2 * m.chunk;
+            }
+            x[q] = slot[(q2 * BL + b0) * m.chunk + zl];
+        }
+    }
+}
+
+// fp16 row scale of x (bf16: 1).  PAIR: the row's other half is thread tid ^
+// 128; the two agree through pmax (a CTA barrier, so every thread calls this).
+template <int FMT, bool PAIR>
+__device__ __forceinline__ void tc2_row_scale(const float2 (&x)[16], float* pmax, int tid, float& down, float& up) {
+    down = up = 1.f;
+    if constexpr (FMT == TC_FP16) {
+        float mx = 0.f;
+#pragma unroll
+        for (int q = 0; q < 16; ++q) mx = fmaxf(mx, fmaxf(fabsf(x[q].x), fabsf(x[q].y)));
+        if constexpr (PAIR) {
+            pmax[tid] = mx;
+            __syncthreads();
+            mx = fmaxf(mx, pmax[tid ^ 128]);
+        }
+        tc2_scale(mx, down, up);
+    }
+}
+
+// The split A operand of this thread's row (part) into tensor memory at
+// `row` (lane and block column): radix 16 -- the whole row, parts 16 columns
+// apart; radix 32 -- half h of the row, parts 32 columns apart.
+template <int FMT, int R>
+__device__ __forceinline__ void tc2_store_a(uint32_t row, int h, const float2 (&x)[16], float down) {
+    constexpr int NP = tc_parts(FMT);
+    uint32_t w[16 * NP];
+    tc2_split16<FMT>(x, down, w);
+    if constexpr (R == 16) {
+        tc_st32(row, reinterpret_cast<const uint32_t(&)[32]>(w));
+        if constexpr (NP == 3) tc_st16(row + 32, w + 32);
+    } else {
+#pragma unroll
+        for (int q = 0; q < NP; ++q) tc_st16(row + 32 * q + 16 * h, w + 16 * q);
+    }
+    tc_wait_st();
+}
+
+// Stage-0 outputs of this thread (accumulator columns at `acc`) into the
+// tile: position R0 j0 + 16 h0 + q.
+template <int N, int BL, int MODE>
+__device__ __forceinline__ void tc2_s0_out(uint32_t acc, float2* slot, int b0, int j0, int h0, float up) {
+    constexpr int R0 = Tc2Geom<N, BL>::R0;
+    float y[32];
+    tc_ld32(acc, y);
+#pragma unroll
+    for (int q = 0; q < 16; ++q) slot[tc2_pos<N, BL, MODE>(b0, R0 * j0 + 16 * h0 + q)] = make_float2(y[q] * up, y[16 + q] * up);
+}
+
+// Stage-1 inputs tile[j1 + NB1 b] times W_N^(b j1), for b = 16 h + q.
+template <int N, int BL, int MODE, bool INV>
+__device__ __forceinline__ void tc2_s1_load(const float2* slot, const float2* tw, int b1, int j1, int h,
+                                            float2 (&x)[16]) {
+    constexpr int NB1 = Tc2Geom<N, BL>::NB1;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+        const int bb = 16 * h + q;
+        x[q] = cmulw<INV>(slot[tc2_pos<N, BL, MODE>(b1, j1 + NB1 * bb)], tw[bb * NB1 + j1]);  // W^0 = 1 exactly
+    }
+}
+
+// Stage-1 outputs X[j1 + NB1 k2], k2 = 16 h + q, to the line in global memory.
+template <int N, int BL>
+__device__ __forceinline__ void tc2_s1_out(uint32_t acc, float2* line, const uint32_t* offA_s, int j1, int h, float up,
+                                           float scale) {
+    constexpr int NB1 = Tc2Geom<N, BL>::NB1;
+    float y[32];
+    tc_ld32(acc, y);
+#pragma unroll
+    for (int q = 0; q < 16; ++q)
+        st_stream(line + offA_s[j1 + NB1 * (16 * h + q)], scl(make_float2(y[q] * up, y[16 + q] * up), scale));
+}
+
 // The persistent kernel: each CTA allocates its tensor memory and loads the
 // split operands, the twiddles and the offsets once, then works through tiles
 // blockIdx.x, blockIdx.x + gridDim.x, ... of B lines, each arriving as whole
@@ -308,47 +405,10 @@ __global__ void __launch_bounds__(Tc2Geom<N, BL>::THREADS, Tc2Geom<N, BL>::THREA
 
         // ---- stage 0: radix-R0 DFTs of x[j0 + 32 a] (this thread's 16 a) ----
         float2 x[16];
-#pragma unroll
-        for (int q = 0; q < 16; ++q) {
-            const int n = j0 + 32 * (16 * h0 + q);
-            if constexpr (MODE == MODE_BATCH) {
-                x[q] = slot[n * B + b0];
-            } else {  // [z chunk][b][z within the chunk]
-                int q2, zl;
-                if (m.chunk_shift >= 0) {
-                    q2 = n >> m.chunk_shift;
-                    zl = n & (m.chunk - 1);
-                } else {
-                    q2 = n / m.chunk;
-                    zl = n - q2 * m.chunk;
-                }
-                x[q] = slot[(q2 * B + b0) * m.chunk + zl];
-            }
-        }
-        float down = 1.f, up = 1.f;
-        if constexpr (FMT == TC_FP16) {
-            float mx = 0.f;
-#pragma unroll
-            for (int q = 0; q < 16; ++q) mx = fmaxf(mx, fmaxf(fabsf(x[q].x), fabsf(x[q].y)));
-            if constexpr (TPR0 == 2) {  // the row's other half
-                pmax[tid] = mx;
-                __syncthreads();
-                mx = fmaxf(mx, pmax[tid ^ 128]);
-            }
-            tc2_scale(mx, down, up);
-        }
-        {
-            uint32_t w[16 * NP];
-            tc2_split16<FMT>(x, down, w);
-            if constexpr (TPR0 == 1) {
-                tc_st32(tmem + row0, reinterpret_cast<const uint32_t(&)[32]>(w));
-                if constexpr (NP == 3) tc_st16(tmem + row0 + 32, w + 32);
-            } else {
-#pragma unroll
-                for (int q = 0; q < NP; ++q) tc_st16(tmem + row0 + 32 * q + 16 * h0, w + 16 * q);
-            }
-            tc_wait_st();
-        }
+        float down, up;
+        tc2_s0_load<N, BL, MODE>(slot, m, b0, j0, h0, x);
+        tc2_row_scale<FMT, TPR0 == 2>(x, pmax, tid, down, up);
+        tc2_store_a<FMT, R0>(tmem + row0, h0, x, down);
         tc_fence_before();
         __syncthreads();  // all A rows stored; every read of the slot done
         if (tid == 0) tc2_issue<FMT, R0, G::NBLK0>(tmem, op0, mbar);
@@ -357,37 +417,14 @@ __global__ void __launch_bounds__(Tc2Geom<N, BL>::THREADS, Tc2Geom<N, BL>::THREA
             ++i;  // tile i's copy has landed
             break;
         }
-        {
-            float y[32];
-            tc_ld32(tmem + row0 + ACC0 + 32 * h0, y);
-#pragma unroll
-            for (int q = 0; q < 16; ++q)
-                slot[tc2_pos<N, BL, MODE>(b0, R0 * j0 + 16 * h0 + q)] = make_float2(y[q] * up, y[16 + q] * up);
-        }
+        tc2_s0_out<N, BL, MODE>(tmem + row0 + ACC0 + 32 * h0, slot, b0, j0, h0, up);
         tc_fence_before();
         __syncthreads();  // stage-0 outputs in the tile; accumulators read
 
         // ---- stage 1: twiddles, then radix-32 DFTs over b of tile[j1 + NB1 b] ----
-#pragma unroll
-        for (int q = 0; q < 16; ++q) {
-            const int bb = 16 * h + q;
-            x[q] = cmulw<INV>(slot[tc2_pos<N, BL, MODE>(b1, j1 + NB1 * bb)], tw[bb * NB1 + j1]);  // W^0 = 1 exactly
-        }
-        if constexpr (FMT == TC_FP16) {
-            float mx = 0.f;
-#pragma unroll
-            for (int q = 0; q < 16; ++q) mx = fmaxf(mx, fmaxf(fabsf(x[q].x), fabsf(x[q].y)));
-            pmax[tid] = mx;
-            __syncthreads();
-            tc2_scale(fmaxf(mx, pmax[tid ^ 128]), down, up);
-        }
-        {
-            uint32_t w[16 * NP];
-            tc2_split16<FMT>(x, down, w);
-#pragma unroll
-            for (int q = 0; q < NP; ++q) tc_st16(tmem + row1 + 32 * q + 16 * h, w + 16 * q);
-            tc_wait_st();
-        }
+        tc2_s1_load<N, BL, MODE, INV>(slot, tw, b1, j1, h, x);
+        tc2_row_scale<FMT, true>(x, pmax, tid, down, up);
+        tc2_store_a<FMT, 32>(tmem + row1, h, x, down);
         tc_fence_before();
         __syncthreads();  // all A rows stored; every read of the tile done
         if (tid == 0) {
@@ -403,19 +440,231 @@ __global__ void __launch_bounds__(Tc2Geom<N, BL>::THREADS, Tc2Geom<N, BL>::THREA
             ++i;
             break;
         }
-        {
-            float y[32];
-            tc_ld32(tmem + row1 + ACC1 + 32 * h, y);
-            float2* line = a.dst + base_s[b1];
-#pragma unroll
-            for (int q = 0; q < 16; ++q)
-                st_stream(line + offA_s[j1 + NB1 * (16 * h + q)], scl(make_float2(y[q] * up, y[16 + q] * up), a.scale));
-        }
+        tc2_s1_out<N, BL>(tmem + row1 + ACC1 + 32 * h, a.dst + base_s[b1], offA_s, j1, h, up, a.scale);
         tc_fence_before();
         __syncthreads();  // accumulators read before the next tile's MMAs; line bases free
     }
     if (!ok && tid == 0)  // wait (bounded) for this CTA's copies still in flight before leaving
         for (int j = i; j < issued; ++j) mbar_wait_bounded(rbar + j % NSTG, (uint32_t)((j / NSTG) & 1));
+    __syncthreads();
+    if (!drained) return;  // MMAs never seen to finish: the columns stay allocated
+    tc_fence_after();
+    if (tid < 32)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TCOLS) : "memory");
+}
+
+// Software-pipelined form (fp16; the 256-thread instances: 512 with 8-line and
+// 1024 with 4-line tiles).  Two tensor-memory regions of 128 columns, tile i
+// in region i % 2; stage 0 and stage 1 commit to their own mbarriers.  While
+// tile i's stage-1 MMAs run, the CTA prepares and issues tile i + 1's stage 0
+// (its slot has landed); tile i's stage-1 results are then read back and
+// stored while tile i + 1's stage-0 MMAs run.  Line bases are double-buffered.
+// Thread 0 keeps the most recent commit not yet waited for: a CTA that gives up
+// a wait frees its tensor memory only after that commit is seen complete.
+template <int N, int BL> __host__ __device__ constexpr size_t tc2p_smem_bytes() {
+    return tc2_smem_bytes<N, BL>(TC_FP16) + sizeof(size_t) * BL + sizeof(unsigned long long);
+}
+
+template <int N, int BL, int MODE, bool INV>
+__global__ void __launch_bounds__(256, 2)
+    fft_tc2p_ring_kernel(const PassArgs<float> a, const __grid_constant__ TmatMaps m) {
+    using G = Tc2Geom<N, BL>;
+    constexpr int FMT = TC_FP16;
+    constexpr int R0 = G::R0;
+    constexpr int B = G::B;
+    constexpr int TPR0 = G::TPR0;
+    constexpr int THREADS = 256;
+    static_assert(G::THREADS == THREADS, "the pipelined form has the 256-thread geometries");
+    constexpr int NP = tc_parts(FMT);
+    constexpr int BC0 = NP * R0 + 2 * R0;
+    constexpr int ACC0 = NP * R0;
+    constexpr int ACC1 = 32 * NP;
+    constexpr uint32_t REG = 128;  // columns per region
+    constexpr uint32_t TCOLS = 2 * REG;
+    static_assert(G::NBLK0 * BC0 <= (int)REG && G::NBLK1 * (32 * NP + 64) <= (int)REG, "a tile fits its region");
+    constexpr uint32_t SLOT = tmat_slot_bytes<float, B, N>();
+    constexpr int NSTG = 2;
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const uint32_t s0 = smem_u32(smem_raw);
+    unsigned char* ring = smem_raw + (((s0 + kTmatAlign - 1) & ~(kTmatAlign - 1)) - s0);
+    unsigned char* bmat = ring + NSTG * SLOT;
+    float2* tw = reinterpret_cast<float2*>(bmat + tc2_b_bytes<N>(FMT));
+    uint32_t* offA_s = reinterpret_cast<uint32_t*>(tw + G::TW);
+    size_t* base_s = reinterpret_cast<size_t*>(offA_s + N);  // [2][B]
+    float* pmax = reinterpret_cast<float*>(base_s + 2 * B);
+    unsigned long long* rbar = reinterpret_cast<unsigned long long*>(pmax + THREADS);
+    unsigned long long* mb0 = rbar + NSTG;  // stage-0 commits
+    unsigned long long* mb1 = mb0 + 1;      // stage-1 commits
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mb1 + 1);
+    int* wflag = reinterpret_cast<int*>(tmem_slot + 1);
+
+    const int tid = threadIdx.x;
+    const int warp = tid / 32;
+    const int tilesV = a.NV / B;
+    const int ntiles = a.NU * tilesV;
+    const int mine = (int)blockIdx.x < ntiles ? (ntiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x : 0;
+
+    if (tid < 32) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TCOLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int i = 0; i < NSTG; ++i) mbar_init(rbar + i, 1);
+        mbar_init(mb0, 1);
+        mbar_init(mb1, 1);
+        fence_mbar_init();
+    }
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(a.tcb);
+        uint4* dst = reinterpret_cast<uint4*>(bmat);
+        for (int i = tid; i < tc2_b_bytes<N>(FMT) / 16; i += THREADS) dst[i] = src[i];
+    }
+    for (int i = tid; i < G::TW; i += THREADS) tw[i] = a.tw[i];
+    for (int i = tid; i < N; i += THREADS) offA_s[i] = a.offA[i];
+    fence_proxy_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t op0 = smem_u32(bmat);
+    const uint32_t op1 = op0 + (N == 512 ? NP * kTcMatB : 0);
+
+    // rows as in fft_tc2_ring_kernel (256 threads: one stage-1 block)
+    int b0, j0, h0;
+    uint32_t row0;
+    {
+        const int blk = TPR0 == 1 ? tid / 128 : 0;
+        const int r = blk * 128 + tid % 128;
+        h0 = TPR0 == 1 ? 0 : tid / 128;
+        if constexpr (MODE == MODE_BATCH) { b0 = r % B; j0 = r / B; }
+        else { j0 = r % 32; b0 = r / 32; }
+        row0 = ((uint32_t)((warp % 4) * 32) << 16) + (uint32_t)(blk * BC0);
+    }
+    const int h = tid / 128;
+    const int rr = tid % 128;
+    int b1, j1;
+    if constexpr (MODE == MODE_BATCH) { b1 = rr % B; j1 = rr / B; }
+    else { j1 = rr % G::NB1; b1 = rr / G::NB1; }
+    const uint32_t row1 = (uint32_t)((warp % 4) * 32) << 16;
+
+    uint32_t ph0 = 0, ph1 = 0;
+    unsigned long long* pend = nullptr;  // thread 0: the latest commit not yet waited for
+    uint32_t pend_ph = 0;
+    bool drained = true;
+    // an MMA completion: thread 0 waits (bounded) and tells the CTA; on expiry
+    // the error flag is raised and `drained` says whether the latest commit
+    // was then seen complete
+    auto mma_wait = [&](unsigned long long* bar, uint32_t& ph) -> bool {
+        if (tid == 0) {
+            int f = 0;
+            if (!mbar_wait_bounded(bar, ph)) f = (pend && !mbar_wait_bounded(pend, pend_ph)) ? 2 : 1;
+            else if (pend == bar && pend_ph == ph) pend = nullptr;
+            *wflag = f;
+        }
+        __syncthreads();
+        const int f = *wflag;
+        if (f) {
+            if (tid == 0) atomicExch(a.err, 1);
+            drained = f == 1;
+            return false;
+        }
+        ph ^= 1u;
+        tc_fence_after();
+        return true;
+    };
+    auto line_base = [&](int t) -> size_t {
+        const int u = t / tilesV;
+        const int v0 = (t - u * tilesV) * B;
+        return (size_t)__ldg(a.offU + u) + __ldg(a.offV + v0 + tid);
+    };
+
+    int issued = 0;  // thread 0: tiles of this CTA whose copies were issued
+    if (tid == 0)
+        for (; issued < NSTG && issued < mine; ++issued)
+            tmat_issue<float, B, N>(m, blockIdx.x + issued * gridDim.x, tilesV, ring + issued * SLOT, rbar + issued);
+    size_t nbase = 0;
+    if (tid < B && mine > 0) nbase = line_base(blockIdx.x);
+    int consumed = 0;  // tiles whose copies were waited for
+    float up0 = 1.f;   // stage-0 unscale of the tile whose stage 0 is in flight
+    float2 x[16];
+    float down;
+    // stage 0 of this CTA's tile k into region k % 2: line bases, slot, operands, MMAs
+    auto stage0 = [&](int k) -> bool {
+        if (tid < B) {
+            base_s[(k & 1) * B + tid] = nbase;
+            if (k + 1 < mine) nbase = line_base(blockIdx.x + (k + 1) * gridDim.x);
+        }
+        if (__syncthreads_or(!mbar_wait_bounded(rbar + k % NSTG, (uint32_t)((k / NSTG) & 1)))) {
+            if (tid == 0) atomicExch(a.err, 1);
+            return false;
+        }
+        ++consumed;
+        const float2* slot = reinterpret_cast<const float2*>(ring + (k % NSTG) * SLOT);
+        tc2_s0_load<N, B, MODE>(slot, m, b0, j0, h0, x);
+        tc2_row_scale<FMT, TPR0 == 2>(x, pmax, tid, down, up0);
+        tc2_store_a<FMT, R0>(tmem + (uint32_t)(k & 1) * REG + row0, h0, x, down);
+        tc_fence_before();
+        __syncthreads();  // all A rows stored; every read of the slot done
+        if (tid == 0) {
+            tc2_issue<FMT, R0, G::NBLK0>(tmem + (uint32_t)(k & 1) * REG, op0, mb0);
+            pend = mb0;
+            pend_ph = ph0;
+        }
+        return true;
+    };
+
+    bool ok = mine > 0 ? stage0(0) : true;
+    for (int i = 0; ok && i < mine; ++i) {
+        const uint32_t reg = (uint32_t)(i & 1) * REG;
+        float2* slot = reinterpret_cast<float2*>(ring + (i % NSTG) * SLOT);
+        if (!mma_wait(mb0, ph0)) {  // tile i's stage 0
+            ok = false;
+            break;
+        }
+        tc2_s0_out<N, B, MODE>(tmem + reg + row0 + ACC0 + 32 * h0, slot, b0, j0, h0, up0);
+        tc_fence_before();
+        __syncthreads();  // stage-0 outputs in the tile; accumulators read
+        float up1;
+        tc2_s1_load<N, B, MODE, INV>(slot, tw, b1, j1, h, x);
+        tc2_row_scale<FMT, true>(x, pmax, tid, down, up1);
+        tc2_store_a<FMT, 32>(tmem + reg + row1, h, x, down);
+        tc_fence_before();
+        __syncthreads();  // all A rows stored; every read of the tile done
+        if (tid == 0) {
+            tc2_issue<FMT, 32, G::NBLK1>(tmem + reg, op1, mb1);
+            pend = mb1;
+            pend_ph = ph1;
+            if (issued < mine) {  // the slot is free: refill it with the tile NSTG ahead
+                fence_proxy_async_smem();
+                tmat_issue<float, B, N>(m, blockIdx.x + issued * gridDim.x, tilesV, ring + (i % NSTG) * SLOT,
+                                        rbar + (i % NSTG));
+                ++issued;
+            }
+        }
+        if (i + 1 < mine && !stage0(i + 1)) {  // under tile i's stage-1 MMAs
+            ok = false;
+            break;
+        }
+        if (!mma_wait(mb1, ph1)) {  // tile i's stage 1
+            ok = false;
+            break;
+        }
+        tc2_s1_out<N, B>(tmem + reg + row1 + ACC1 + 32 * h, a.dst + base_s[(i & 1) * B + b1], offA_s, j1, h, up1,
+                         a.scale);
+        tc_fence_before();
+        __syncthreads();  // accumulators read before the region is reused; line bases free
+    }
+    if (!ok) {  // copies and MMAs still in flight, each waited for (bounded)
+        if (tid == 0) {
+            for (int j = consumed; j < issued; ++j) mbar_wait_bounded(rbar + j % NSTG, (uint32_t)((j / NSTG) & 1));
+            *wflag = (pend && !mbar_wait_bounded(pend, pend_ph)) ? 2 : 0;
+        }
+        __syncthreads();
+        if (*wflag == 2) drained = false;
+    }
     __syncthreads();
     if (!drained) return;  // MMAs never seen to finish: the columns stay allocated
     tc_fence_after();

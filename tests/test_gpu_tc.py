@@ -59,8 +59,9 @@ def test_split_every_kernel_form(pkg, oracle, cuda, P, shape, method):
     """Each tensor-core kernel form -- one tile per CTA, the persistent form
     fed by the TMA ring, and the two-stage form (512 = 16 x 32 and 1024 =
     32 x 32: a radix-16 or radix-32 GEMM, one twiddle, a radix-32 GEMM, TMA
-    ring; at 1024 with 4- or 8-line tiles) -- on every pass gives the FP64
-    oracle's transform (relative L2 <= 1e-6)."""
+    ring; at 1024 with 4- or 8-line tiles; in fp16 also software-pipelined
+    over two tensor-memory regions) -- on every pass gives the FP64 oracle's
+    transform (relative L2 <= 1e-6)."""
     import torch
 
     shape = (shape,) * 3 if isinstance(shape, int) else tuple(shape)
@@ -71,10 +72,10 @@ def test_split_every_kernel_form(pkg, oracle, cuda, P, shape, method):
     ref = oracle.fft3_fp64(g)
     f = pkg.a2adfft(dist, method=method)
     f.make_plans()
-    assert f.variant_count(0) == 4
+    assert f.variant_count(0) == 5
     tested = 0
-    applied = [set(), set(), set(), set()]
-    for form in (0, 1, 2, 3):
+    applied = [set(), set(), set(), set(), set()]
+    for form in (0, 1, 2, 3, 4):
         for p in range(3):
             try:
                 f.select_variant(p, form)
@@ -89,13 +90,15 @@ def test_split_every_kernel_form(pkg, oracle, cuda, P, shape, method):
         f.inverse(x)
         assert oracle.rel_l2(x.cpu().numpy(), x0.cpu().numpy()) <= 2 * TOL[method], f"form {form} round trip"
         tested += 1
-    assert tested == 4
+    assert tested == 5
     assert applied[0] == {0, 1, 2}
     # the two-stage form (512 and 1024) runs on the ring form's tile geometry:
     # it fits exactly the passes of those lengths where the ring form fits
     lengths = (shape[2], shape[0], shape[1])  # Z, X, Y
     assert applied[2] == {p for p in applied[1] if lengths[p] in (512, 1024)}, applied
     assert applied[3] <= {p for p in range(3) if lengths[p] == 1024}, applied  # 8-line tiles of 1024
+    # the software-pipelined two-stage form: fp16, on the two-stage form's passes
+    assert applied[4] == (applied[2] if method == "split_fp16" else set()), applied
 
 
 def test_split_rejects_double_and_unsupported_lengths(pkg, cuda):
