@@ -223,11 +223,12 @@ a2a_status a2a_dfft_check_device(const a2a_dfft* dfft);
 /* Launch variants compiled for a pass (0 = Z, 1 = X, 2 = Y), and a manual
  * choice among them (overrides the default or the make_plans timing; fails
  * with A2A_ERROR_UNSUPPORTED for a variant that does not fit the pass).  With
- * a split tensor-core method there are four: 0 = one tile per CTA, 1 =
+ * a split tensor-core method there are five: 0 = one tile per CTA, 1 =
  * persistent CTAs fed by a TMA ring (the default where it fits), 2 = the
  * two-stage form (lengths 512 and 1024: a radix-16 or radix-32 GEMM, one
  * twiddle, a radix-32 GEMM; TMA ring), 3 = the two-stage form with 8-line
- * tiles (1024).  No reference counterpart. */
+ * tiles (1024), 4 = the two-stage form software-pipelined over two
+ * tensor-memory regions (fp16).  No reference counterpart. */
 a2a_status a2a_dfft_variant_count(const a2a_dfft* dfft, int pass, int* count);
 a2a_status a2a_dfft_select_variant(a2a_dfft* dfft, int pass, int variant);
 
