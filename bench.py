@@ -34,9 +34,12 @@ workload, every step, and prints its line with "impl": "reference".
 ``--workload batch`` measures the batched form instead: 96 complex64 cubes with
 edges drawn from 32 48 64 96 128 192 (seed 3) plus two 128x256x512 boxes, each
 on 4 virtual ranks (dims [2,2,1]), N(0,1) input (seed 3); one step = one
-batched forward + inverse (one persistent launch per direction, replayed from a
-CUDA graph).  Its CPU baseline runs the same step sequence on the host (oracle
-port) once per distinct shape, scaled by the shape counts.
+batched forward + inverse, replayed from a CUDA graph in the schedule the
+batch's make_plans picks (one persistent launch per direction, one per pass, or
+the grouped schedule: each shape's boxes as one grid through the single-grid
+pass kernels, shapes on parallel graph branches).  Its CPU baseline runs the
+same step sequence on the host (oracle port) once per distinct shape, scaled by
+the shape counts.
 """
 from __future__ import annotations
 
