@@ -251,15 +251,17 @@ __device__ __forceinline__ void tc2_s1_load(const float2* slot, const float2* tw
 }
 
 // Stage-1 outputs X[j1 + NB1 k2], k2 = 16 h + q, to the line in global memory.
+// The row's unscale and the pass scale are one factor: `up` is a power of two,
+// so up * scale is exact and every output is rounded once, as before.
 template <int N, int BL>
 __device__ __forceinline__ void tc2_s1_out(uint32_t acc, float2* line, const uint32_t* offA_s, int j1, int h, float up,
                                            float scale) {
     constexpr int NB1 = Tc2Geom<N, BL>::NB1;
+    const float f = up * scale;
     float y[32];
     tc_ld32(acc, y);
 #pragma unroll
-    for (int q = 0; q < 16; ++q)
-        st_stream(line + offA_s[j1 + NB1 * (16 * h + q)], scl(make_float2(y[q] * up, y[16 + q] * up), scale));
+    for (int q = 0; q < 16; ++q) st_stream(line + offA_s[j1 + NB1 * (16 * h + q)], make_float2(y[q] * f, y[16 + q] * f));
 }
 
 // The persistent kernel: each CTA allocates its tensor memory and loads the
