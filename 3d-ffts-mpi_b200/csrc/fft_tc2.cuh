@@ -12,15 +12,18 @@
 // fft_tc.cuh) has one thread; a radix-32 row has two: warps w and w + 4 reach
 // the same tensor-memory lanes, so thread half h writes the inputs of its half
 // of K (its 16 columns of each part) and reads its half of N.  Every thread
-// thus splits 16 complex values per stage.
+// thus splits 16 complex values per stage.  Rows of a stage fill 128-row
+// blocks of tensor memory (columns side by side): with one thread per row,
+// block k belongs to warps 4k .. 4k+3; with two, to warps 8k .. 8k+7, warp w
+// reaching lanes 32 (w mod 4) .. 32 (w mod 4) + 31.
 //
 // A pass has two GEMM stages, one twiddle multiply and one shared-memory
 // exchange per element.  Operands are split as in fft_tc.cuh (fp16: two parts,
 // rows scaled by a power of two; bf16: three parts); a radix-32 row's scale is
 // agreed between its two threads through shared memory.  Tiles (8 lines at
-// 512, 4 at 1024: 32 KB) arrive by the single-GPU TMA ring of fft_tmat.cuh (2
-// slots, transformed in place, no multicast); a tile's slot is refilled as
-// soon as its stage-1 operands are in tensor memory.
+// 512; 4 or 8 lines at 1024: 32 or 64 KB) arrive by the single-GPU TMA ring
+// of fft_tmat.cuh (2 slots, transformed in place, no multicast); a tile's slot
+// is refilled as soon as its stage-1 operands are in tensor memory.
 #pragma once
 
 #include "fft_tc.cuh"
